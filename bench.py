@@ -1,0 +1,278 @@
+"""Benchmark of the CUDA cloth step: sim steps/s on the floor-drape workload.
+
+python bench.py --gpus N --steps K --warmup W [--impl cuda|reference]
+                [--workload floor_drape|strip_pull] [--precision fp64|mixed]
+
+One process per GPU (torchrun for N > 1); every rank steps its own replica of
+the workload (a single sheet does not shard: "replicas only", weak scaling).
+Timing: per step, L2 is flushed (a 256 MiB write on the solver's stream), then
+the step is bracketed by CUDA events on the solver's stream; the reported
+time is the max over ranks. rank 0 prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+HBM_FALLBACK_GBS = 6650.0
+
+
+def measured_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            j = json.load(f)
+        return float(j["hbm_gbs"]), "measured"
+    except Exception:
+        return HBM_FALLBACK_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.dev)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def workload(name: str, steps_hint: int):
+    from closim_b200 import configs
+    if name == "floor_drape":
+        return configs.floor_drape()
+    if name == "strip_pull":
+        return configs.strip_pull()
+    raise SystemExit(f"unknown workload {name}")
+
+
+def cpu_baseline(cfg, budget_s: float, max_steps: int):
+    """The oracle (single-threaded C++ port of the reference CpuSolver) on a
+    bounded sample: the first steps of the same workload, up to budget_s."""
+    from tests.helpers import oracle_scene, oracle_step_kwargs
+    from closim_b200 import configs
+    sc = oracle_scene(cfg)
+    kw = oracle_step_kwargs(cfg)
+    t0 = time.perf_counter()
+    k = 0
+    while k < max_steps:
+        sc.set_pins(configs.pins_at(cfg, k))
+        sc.step(cfg["h"], **kw)
+        k += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    dt = time.perf_counter() - t0
+    return {"value": k / dt, "unit": "steps/s", "cores": 1, "kind": "port",
+            "sample": f"first {k} steps of {cfg['name']} ({dt:.1f} s, 1 thread)"}
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return 0
+    cfg = workload(args.workload, args.steps)
+    from oracle import oracle as O
+    O.lib()
+    per = []
+    for i in range(args.warmup + args.steps):
+        b = cpu_baseline(cfg, budget_s=max(5.0, 60.0 / max(1, args.warmup + args.steps)), max_steps=cfg["steps"])
+        if i >= args.warmup:
+            per.append(b["value"])
+    v = statistics.mean(per)
+    line = {"metric": "sim steps/s", "value": v, "unit": "steps/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": True, "impl": "reference", "scaling": "weak",
+            "dtype": "f64", "data": "synthetic (seeded)",
+            "config": {"workload": cfg["name"], "n": len(cfg["x"]) // 3, "h": cfg["h"]},
+            "cpu_baseline": {"value": v, "unit": "steps/s", "cores": 1, "kind": "port", "sample": b["sample"]},
+            "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "vs_baseline": None}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=60)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
+    ap.add_argument("--workload", default="floor_drape", choices=["floor_drape", "strip_pull"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank)
+
+    import torch
+    import torch.distributed as dist
+    import datetime
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    import closim_b200 as cb
+    from closim_b200 import configs
+    cfg = workload(args.workload, args.steps)
+    n = len(cfg["x"]) // 3
+    sc = configs.make_scene(cfg)
+    solver = cb.CudaSolver(args.precision, device=local, **cfg["options"])
+    solver.initialize(sc)
+    ext = torch.cuda.ExternalStream(solver.stream(), device=local)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{local}")  # 256 MiB > 126 MB L2
+
+    step_idx = [0]
+
+    def set_pins():
+        sc.pinned.clear()
+        sc.pinned.update(configs.pins_at(cfg, step_idx[0] % cfg["steps"]))
+        step_idx[0] += 1
+
+    for _ in range(args.warmup):
+        set_pins()
+        solver.advance(cfg["h"], 1)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+
+    # ---- device-resident timed region ----
+    sampler = ClockSampler(local)
+    sampler.start()
+    launches0 = solver.kernelLaunches()
+    solver.profile(True)
+    total_ms = 0.0
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    for _ in range(args.steps):
+        set_pins()
+        with torch.cuda.stream(ext):
+            flush.fill_(1.0)
+        ev0.record(ext)
+        solver.advance(cfg["h"], 1)
+        ev1.record(ext)
+        ev1.synchronize()
+        total_ms += ev0.elapsed_time(ev1)
+    torch.cuda.synchronize()
+    prof = solver.profileRead()
+    solver.profile(False)
+    launches = solver.kernelLaunches() - launches0
+    clocks = sampler.stop()
+
+    # ---- end to end through the public API: host state in, host state out ----
+    # scene arrays in pinned host memory (the copies each step read and write them)
+    px = torch.empty(n * 3, dtype=torch.float64).pin_memory()
+    pv = torch.empty(n * 3, dtype=torch.float64).pin_memory()
+    sc.positions = px.numpy()
+    sc.velocities = pv.numpy()
+    solver.syncFromScene = True
+    solver.pull()
+    e2e_ms = 0.0
+    e_steps = max(3, args.steps // 2)
+    for _ in range(e_steps):
+        set_pins()
+        ev0.record(ext)
+        solver.step(cfg["h"])
+        ev1.record(ext)
+        ev1.synchronize()
+        e2e_ms += ev0.elapsed_time(ev1)
+    h2d = 2 * n * 3 * 8 + len(sc.pinned) * (4 + 24)
+    d2h = 2 * n * 3 * 8
+
+    t = torch.tensor([total_ms, e2e_ms], dtype=torch.float64, device=f"cuda:{local}")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.barrier()
+    total_ms, e2e_ms = t.tolist()
+    ms_per_step = total_ms / args.steps
+    value = world * args.steps / (total_ms / 1000.0)
+    e2e_value = world * e_steps / (e2e_ms / 1000.0)
+
+    if rank == 0:
+        peak, peak_kind = measured_peak()
+        achieved = prof["bytes"] / prof["launches"] / (prof["ms_per_launch"] / 1000.0) / 1e9 if prof["launches"] else 0.0
+        line = {
+            "metric": "sim steps/s", "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
+            "data": "synthetic (seeded)", "impl": "cuda",
+            "config": {"workload": cfg["name"], "n": n, "m": len(cfg["idx"]) // 3, "h": cfg["h"],
+                       "precision": args.precision, "precond": cfg["options"]["precond"],
+                       "parallelism": f"replicas x{world}", "l2": "flushed between timed steps (256 MiB write)"},
+            "roofline": {"bound": "hbm", "kernel": "k_pcg", "achieved": achieved, "peak": peak,
+                         "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": None, "launches": prof["launches"], "ms_per_launch": prof["ms_per_launch"],
+                         "pcg_iters": prof["iters"], "alg_bytes_per_launch": prof["bytes"] / max(1, prof["launches"]),
+                         "share_of_step": prof["ms"] / total_ms if total_ms else None},
+            "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": launches,
+            "clocks": clocks,
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(cfg, budget_s=20.0, max_steps=cfg["steps"])
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,616 @@
+// FP64 path of the implicit-Euler Newton step (compiled with -fmad=false).
+//
+// One thread per element over SoA mesh constants writes element-local results;
+// one thread per vertex gathers them through the element-ordered CSR
+// incidence, so each vertex sum adds the same terms in the same order as the
+// reference's scatter (src/mesh/incidence.ts:1-7). The PCG solve runs as one
+// cooperative persistent kernel: grid-wide barriers separate its phases and
+// every reduction is a fixed-order two-level sum that all blocks evaluate
+// identically, so control decisions agree across the grid and runs repeat
+// bit for bit.
+#include <cstdio>
+
+#include "contact.cuh"
+#include "plain.cuh"
+
+namespace cs {
+
+__device__ __forceinline__ void load3(const double* x, int v, double o[3]) {
+  o[0] = x[v * 3]; o[1] = x[v * 3 + 1]; o[2] = x[v * 3 + 2];
+}
+
+// ---- predictor (newton.ts:41-50) -------------------------------------------
+__global__ void k_predict(Dev d) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.n) return;
+  const double h = d.h;
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    const double x0 = d.x[i * 3 + k];
+    d.x0[i * 3 + k] = x0;
+    const double y = x0 + h * d.v[i * 3 + k] + h * h * d.gravity[k];
+    d.yHat[i * 3 + k] = y;
+    d.x[i * 3 + k] = y;
+  }
+}
+
+__global__ void k_pins(Dev d, double* x) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= d.npins) return;
+  const int id = d.pinIds[k];
+  x[id * 3] = d.pinPos[k * 3];
+  x[id * 3 + 1] = d.pinPos[k * 3 + 1];
+  x[id * 3 + 2] = d.pinPos[k * 3 + 2];
+}
+
+// ---- gradient (fem.ts:15-54, newton.ts:113-130) -------------------------------
+__global__ void __launch_bounds__(kThreads) k_tri_grad(Dev d) {
+  __shared__ double sm[32];
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  double strain = 0;
+  if (t < d.m) {
+    const uint32_t i0 = d.idx[t * 3], i1 = d.idx[t * 3 + 1], i2 = d.idx[t * 3 + 2];
+    double p0[3], p1[3], p2[3];
+    load3(d.x, i0, p0); load3(d.x, i1, p1); load3(d.x, i2, p2);
+    const float4 iv = d.inv[t];
+    double e, g[9], E[3];
+    tri_grad<double>(p0, p1, p2, iv.x, iv.y, iv.z, iv.w, d.area[t], d.mat, e, g, E);
+#pragma unroll
+    for (int k = 0; k < 9; k++) d.elem[(size_t)t * 9 + k] = g[k];
+    strain = js_max(js_max(fabs(E[0]), fabs(E[1])), fabs(E[2]));
+  }
+  const double bm = block_max(strain, sm);
+  if (threadIdx.x == 0) d.part[0 * d.partStride + blockIdx.x] = bm;
+}
+
+__global__ void __launch_bounds__(kThreads) k_hinge_grad(Dev d) {
+  const int hh = blockIdx.x * blockDim.x + threadIdx.x;
+  if (hh >= d.hg) return;
+  const int4 hv = d.hinge[hh];
+  double q[12];
+  load3(d.x, hv.x, q); load3(d.x, hv.y, q + 3); load3(d.x, hv.z, q + 6); load3(d.x, hv.w, q + 9);
+  double out[12];
+  hinge_fd_grad(q, d.hmeta[hh * 3], d.hmeta[hh * 3 + 1], d.hmeta[hh * 3 + 2], d.kb, out);
+#pragma unroll
+  for (int k = 0; k < 12; k++) d.helem[(size_t)hh * 12 + k] = out[k];
+}
+
+// g = M (x - yHat) / h^2 + gradE (+ contact grad), pin filter, partial |g|^2.
+__global__ void __launch_bounds__(kThreads) k_gather_grad(Dev d) {
+  __shared__ double sm[32];
+  const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  double gg = 0;
+  if (v < d.n) {
+    double s[3] = {0, 0, 0};
+    for (uint32_t k = d.memOff[v]; k < d.memOff[v + 1]; k++) {
+      const uint32_t rec = d.memRec[k];
+      const double* e = d.elem + (size_t)(rec >> 2) * 9 + (rec & 3) * 3;
+      s[0] += e[0]; s[1] += e[1]; s[2] += e[2];
+    }
+    if (d.kb > 0)
+      for (uint32_t k = d.hinOff[v]; k < d.hinOff[v + 1]; k++) {
+        const uint32_t rec = d.hinRec[k];
+        const double* e = d.helem + (size_t)(rec >> 2) * 12 + (rec & 3) * 3;
+        s[0] += e[0]; s[1] += e[1]; s[2] += e[2];
+      }
+    const double M = d.mass[v];
+    const bool pin = d.pinned[v];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      const int i = v * 3 + k;
+      double gi = M * (d.x[i] - d.yHat[i]) * d.invH2 + s[k];
+      if (d.hasContact) gi += d.cgrad[i];
+      if (pin) gi = 0;
+      d.g[i] = gi;
+      gg += gi * gi;
+    }
+  }
+  const double bs = block_sum(gg, sm);
+  if (threadIdx.x == 0) d.part[1 * d.partStride + blockIdx.x] = bs;
+}
+
+// Final reduction of the gradient pass: sqrt(sum g^2), max strain.
+__global__ void k_grad_final(Dev d, int nbT, int nbV) {
+  if (threadIdx.x >= 32) return;
+  const double gs = warp_sum_partials(d.part + 1 * d.partStride, nbV);
+  const double ms = warp_max_partials(d.part + 0 * d.partStride, nbT);
+  if (threadIdx.x == 0) {
+    d.scal[S_GRADNORM] = sqrt(gs);
+    d.scal[S_MAXSTRAIN] = ms;
+  }
+}
+
+// ---- total energy (newton.ts:76-88; fem.ts:56-75) ------------------------------
+__global__ void __launch_bounds__(kThreads) k_energy(Dev d, const double* x) {
+  __shared__ double sm[32];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double ei = 0, et = 0, eh = 0;
+  if (i < d.n) {
+    const double m = d.mass[i];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      const double dd = x[i * 3 + k] - d.yHat[i * 3 + k];
+      ei += 0.5 * m * dd * dd / (d.h * d.h);
+    }
+  }
+  if (i < d.m) {
+    double p0[3], p1[3], p2[3];
+    load3(x, d.idx[i * 3], p0); load3(x, d.idx[i * 3 + 1], p1); load3(x, d.idx[i * 3 + 2], p2);
+    const float4 iv = d.inv[i];
+    et = tri_energy<double>(p0, p1, p2, iv.x, iv.y, iv.z, iv.w, d.area[i], d.mat);
+  }
+  if (i < d.hg && d.kb > 0) {
+    const int4 hv = d.hinge[i];
+    double q[12];
+    load3(x, hv.x, q); load3(x, hv.y, q + 3); load3(x, hv.z, q + 6); load3(x, hv.w, q + 9);
+    eh = hinge_energy4(q, d.hmeta[i * 3], d.hmeta[i * 3 + 1], d.hmeta[i * 3 + 2], d.kb);
+  }
+  const double bi = block_sum(ei, sm), bt = block_sum(et, sm), bh = block_sum(eh, sm);
+  if (threadIdx.x == 0) {
+    d.part[2 * d.partStride + blockIdx.x] = bi;
+    d.part[3 * d.partStride + blockIdx.x] = bt;
+    d.part[4 * d.partStride + blockIdx.x] = bh;
+  }
+}
+
+__global__ void k_energy_final(Dev d, int nb) {
+  if (threadIdx.x >= 32) return;
+  const double ei = warp_sum_partials(d.part + 2 * d.partStride, nb);
+  const double et = warp_sum_partials(d.part + 3 * d.partStride, nb);
+  const double eh = warp_sum_partials(d.part + 4 * d.partStride, nb);
+  const double em = d.hasContact ? d.scal[S_E_MERIT] : 0.0;
+  if (threadIdx.x == 0) {
+    d.scal[S_E_INERTIA] = ei;
+    d.scal[S_E_TRI] = et;
+    d.scal[S_E_HINGE] = eh;
+    d.scal[S_ENERGY_TRIAL] = ei + (et + eh) + em;
+  }
+}
+
+__global__ void k_diag_init(Dev d, double beta) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.n * 3) return;
+  d.diag[i] = (double)d.mass[i / 3] * d.invH2 + beta;
+}
+
+// ---- one-level additive Schwarz (schwarz.ts:154-309) ---------------------------
+// Factor: one warp per domain. Lane l owns the rows of member l and adds its
+// incident triangles' 9x9 rows in ascending triangle order (the reference's
+// per-entry accumulation order); the Cholesky is row-parallel with each entry
+// computed by one lane in the reference's sequential inner order.
+constexpr int kSchwarzWarps = 4;
+__global__ void __launch_bounds__(kSchwarzWarps * 32) k_schwarz_factor(Dev d) {
+  __shared__ double A[kSchwarzWarps][24 * 24];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int dom = blockIdx.x * kSchwarzWarps + wib;
+  if (dom >= d.D) return;
+  double* a = A[wib];
+  const int start = d.domStart[dom], dv = d.domStart[dom + 1] - start, dw = dv * 3;
+  for (int i = lane; i < 24 * 24; i += 32) a[i] = 0;
+  __syncwarp();
+  if (lane < dv) {
+    const int v = d.domVerts[start + lane];
+    for (int k = d.v2tOff[v]; k < d.v2tOff[v + 1]; k++) {
+      const int t = d.v2t[k];
+      const int cvs[3] = {(int)d.idx[t * 3], (int)d.idx[t * 3 + 1], (int)d.idx[t * 3 + 2]};
+      const int ci = cvs[0] == v ? 0 : cvs[1] == v ? 1 : 2;
+      double p0[3], p1[3], p2[3];
+      load3(d.x, cvs[0], p0); load3(d.x, cvs[1], p1); load3(d.x, cvs[2], p2);
+      const float4 iv = d.inv[t];
+      double h27[27];
+      tri_hessian9_rows<double>(p0, p1, p2, iv.x, iv.y, iv.z, iv.w, d.area[t], d.mat, ci * 3, ci * 3 + 3, h27);
+      for (int cj = 0; cj < 3; cj++) {
+        int lw = -1;
+        for (int q = 0; q < dv; q++)
+          if (d.domVerts[start + q] == cvs[cj]) { lw = q; break; }
+        if (lw < 0) continue;
+        for (int aa = 0; aa < 3; aa++)
+          for (int bb = 0; bb < 3; bb++) a[(lane * 3 + aa) * dw + (lw * 3 + bb)] += h27[aa * 9 + cj * 3 + bb];
+      }
+    }
+  }
+  __syncwarp();
+  if (lane < dw) {
+    const int v = d.domVerts[start + lane / 3];
+    a[lane * dw + lane] += d.diag[v * 3 + lane % 3];
+  }
+  __syncwarp();
+  for (int i = lane; i < dw; i += 32)
+    for (int j = i + 1; j < dw; j++) {
+      const double s = 0.5 * (a[i * dw + j] + a[j * dw + i]);
+      a[i * dw + j] = s;
+      a[j * dw + i] = s;
+    }
+  __syncwarp();
+  double scale = 0;
+  for (int i = 0; i < dw; i++) scale = js_max(scale, fabs(a[i * dw + i]));
+  const double tiny = 1e-20 * (1 + scale);
+  bool ok = true;
+  for (int k = 0; k < dw; k++) {
+    double diagk = 0;
+    if (lane == 0) {
+      double sum = a[k * dw + k];
+      for (int s = 0; s < k; s++) sum -= a[k * dw + s] * a[k * dw + s];
+      ok = sum > tiny;
+      if (ok) a[k * dw + k] = sqrt(sum);
+    }
+    ok = __shfl_sync(0xffffffffu, ok, 0);
+    __syncwarp();
+    if (!ok) break;
+    diagk = a[k * dw + k];
+    if (lane > k && lane < dw) {
+      double s2 = a[lane * dw + k];
+      for (int s = 0; s < k; s++) s2 -= a[lane * dw + s] * a[k * dw + s];
+      a[lane * dw + k] = s2 / diagk;
+    }
+    __syncwarp();
+  }
+  double* L = d.L + (size_t)dom * 576;
+  if (ok) {
+    for (int i = lane; i < dw; i += 32)
+      for (int j = 0; j < 24; j++) L[i * 24 + j] = j <= i && j < dw ? a[i * dw + j] : 0.0;
+  } else {
+    for (int i = lane; i < dw; i += 32) {
+      const int v = d.domVerts[start + i / 3];
+      const double dd = d.diag[v * 3 + i % 3];
+      for (int j = 0; j < 24; j++) L[i * 24 + j] = j == i ? (dd > 1e-12 ? 1 / dd : 0.0) : 0.0;
+    }
+  }
+  if (lane == 0) d.domFlag[dom] = ok ? 1 : 0;
+}
+
+// z = M^-1 r on one domain; returns sum r.z over its (pin-filtered) dofs.
+__device__ double schwarz_apply_domain(const Dev& d, int dom) {
+  const int start = d.domStart[dom], dv = d.domStart[dom + 1] - start, dw = dv * 3;
+  const double* L = d.L + (size_t)dom * 576;
+  double rhs[24], y[24], sol[24];
+  for (int l = 0; l < dv; l++) {
+    const int v = d.domVerts[start + l];
+    rhs[l * 3] = d.r[v * 3]; rhs[l * 3 + 1] = d.r[v * 3 + 1]; rhs[l * 3 + 2] = d.r[v * 3 + 2];
+  }
+  if (d.domFlag[dom]) {
+    for (int i = 0; i < dw; i++) {
+      double s = rhs[i];
+      for (int j = 0; j < i; j++) s -= L[i * 24 + j] * y[j];
+      y[i] = s / L[i * 24 + i];
+    }
+    for (int i = dw - 1; i >= 0; i--) {
+      double s = y[i];
+      for (int j = i + 1; j < dw; j++) s -= L[j * 24 + i] * sol[j];
+      sol[i] = s / L[i * 24 + i];
+    }
+  } else {
+    for (int i = 0; i < dw; i++) {
+      double s = 0;
+      for (int j = 0; j < dw; j++) s += L[i * 24 + j] * rhs[j];
+      sol[i] = s;
+    }
+  }
+  double rz = 0;
+  for (int l = 0; l < dv; l++) {
+    const int v = d.domVerts[start + l];
+    const bool pin = d.pinned[v];
+    for (int k = 0; k < 3; k++) {
+      const double zz = pin ? 0.0 : 0.0 + sol[l * 3 + k];
+      d.z[v * 3 + k] = zz;
+      rz += d.r[v * 3 + k] * zz;
+    }
+  }
+  return rz;
+}
+
+// ---- PCG as one cooperative kernel (pcg.ts:11-95 + newton.ts:148-179) ----------
+struct PcgArgs {
+  Dev d;
+  int maxIters;
+  double tol;
+};
+
+// Block partial -> row slot; after grid.sync every block reads the same total.
+__device__ __forceinline__ void put_partial(const Dev& d, int row, double v, double* sm) {
+  const double b = block_sum(v, sm);
+  if (threadIdx.x == 0) d.part[row * d.partStride + blockIdx.x] = b;
+}
+__device__ __forceinline__ double get_total(const Dev& d, int row, double* bc) {
+  if (threadIdx.x < 32) {
+    const double s = warp_sum_partials(d.part + row * d.partStride, gridDim.x);
+    if (threadIdx.x == 0) bc[0] = s;
+  }
+  __syncthreads();
+  const double r = bc[0];
+  __syncthreads();
+  return r;
+}
+__device__ __forceinline__ double get_max_nonan(const Dev& d, int row, double* bc) {
+  if (threadIdx.x < 32) {
+    const int lane = threadIdx.x;
+    double s = 0;
+    for (int i = lane; i < (int)gridDim.x; i += 32) {
+      const double v = d.part[row * d.partStride + i];
+      if (v > s) s = v;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      const double w = __shfl_xor_sync(0xffffffffu, s, o);
+      if (w > s) s = w;
+    }
+    if (lane == 0) bc[0] = s;
+  }
+  __syncthreads();
+  const double r = bc[0];
+  __syncthreads();
+  return r;
+}
+__device__ __forceinline__ double block_max_nonan(double v, double* sm) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int o = 16; o > 0; o >>= 1) {
+    const double w = __shfl_down_sync(0xffffffffu, v, o);
+    if (w > v) v = w;
+  }
+  __syncthreads();
+  if (lane == 0) sm[warp] = v;
+  __syncthreads();
+  double r = 0;
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < (int)(blockDim.x >> 5); i++)
+      if (sm[i] > r) r = sm[i];
+    sm[0] = r;
+  }
+  __syncthreads();
+  r = sm[0];
+  __syncthreads();
+  return r;
+}
+
+__global__ void __launch_bounds__(kThreads) k_pcg(PcgArgs A) {
+  cg::grid_group grid = cg::this_grid();
+  __shared__ double sm[32];
+  __shared__ double bc[2];
+  const Dev& d = A.d;
+  const int n3 = d.n * 3;
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+  const bool jacobi = d.precond == 0;
+  // Row use per iteration: 0 |p|^2, 1 pAp, 2 |r|^2, 3 r.z ; 4-6 init ; 4-5 post.
+  double rzp = 0, bbp = 0, rrp = 0;
+  for (int i = tid; i < n3; i += nth) {
+    const double bi = -d.g[i];
+    bbp += bi * bi;
+    const double ri = d.pinned[i / 3] ? 0.0 : bi;
+    d.r[i] = ri;
+    d.dx[i] = 0;
+    rrp += ri * ri;
+    if (jacobi) {
+      double zi = d.diag[i] > 1e-12 ? ri / d.diag[i] : ri;
+      if (d.pinned[i / 3]) zi = 0;
+      d.z[i] = zi;
+      d.p[i] = zi;
+      rzp += ri * zi;
+    }
+  }
+  put_partial(d, 5, bbp, sm);
+  put_partial(d, 6, rrp, sm);
+  if (jacobi) put_partial(d, 4, rzp, sm);
+  grid.sync();
+  if (!jacobi) {
+    rzp = 0;
+    for (int dom = tid; dom < d.D; dom += nth) rzp += schwarz_apply_domain(d, dom);
+    put_partial(d, 4, rzp, sm);
+    grid.sync();
+    for (int i = tid; i < n3; i += nth) d.p[i] = d.z[i];
+  }
+  double rz = get_total(d, 4, bc);
+  const double bNorm = sqrt(get_total(d, 5, bc));
+  const double absTol = js_max(A.tol * js_max(bNorm, 1e-12), 1e-12);
+  double residual = sqrt(get_total(d, 6, bc));
+  int iters = 0;
+  bool done = residual < absTol;
+  // |p|^2 for the first FD step size.
+  if (!done) {
+    double pp = 0;
+    for (int i = tid; i < n3; i += nth) pp += d.p[i] * d.p[i];
+    put_partial(d, 0, pp, sm);
+    grid.sync();
+  }
+  int k = 0;
+  for (; !done && k < A.maxIters; k++) {
+    // --- HVP: membraneHvp (fem.ts:108-130) + inertia + contact ---
+    const double pNorm = sqrt(get_total(d, 0, bc));
+    const double h = 1e-8 * (1 + pNorm);
+    for (int t = tid; t < d.m; t += nth) {
+      const uint32_t vi[3] = {d.idx[t * 3], d.idx[t * 3 + 1], d.idx[t * 3 + 2]};
+      double xp[9], xm[9];
+#pragma unroll
+      for (int c = 0; c < 3; c++)
+#pragma unroll
+        for (int q = 0; q < 3; q++) {
+          const double xx = d.x[vi[c] * 3 + q], pq = d.p[vi[c] * 3 + q];
+          xp[c * 3 + q] = xx + h * pq;
+          xm[c * 3 + q] = xx - h * pq;
+        }
+      const float4 iv = d.inv[t];
+      const double ar = d.area[t];
+      double e, gp[9], gm[9], E[3];
+      tri_grad<double>(xp, xp + 3, xp + 6, iv.x, iv.y, iv.z, iv.w, ar, d.mat, e, gp, E);
+      tri_grad<double>(xm, xm + 3, xm + 6, iv.x, iv.y, iv.z, iv.w, ar, d.mat, e, gm, E);
+      double* o = d.elem + (size_t)t * 18;
+#pragma unroll
+      for (int q = 0; q < 9; q++) { o[q] = gp[q]; o[9 + q] = gm[q]; }
+    }
+    if (d.hasContact) contact_hvp_coeffs(d, d.p, tid, nth);
+    grid.sync();
+    double pAp = 0;
+    for (int v = tid; v < d.n; v += nth) {
+      double sp[3] = {0, 0, 0}, sn[3] = {0, 0, 0};
+      for (uint32_t q = d.memOff[v]; q < d.memOff[v + 1]; q++) {
+        const uint32_t rec = d.memRec[q];
+        const double* e = d.elem + (size_t)(rec >> 2) * 18 + (rec & 3) * 3;
+        sp[0] += e[0]; sp[1] += e[1]; sp[2] += e[2];
+        sn[0] += e[9]; sn[1] += e[10]; sn[2] += e[11];
+      }
+      double ch[3] = {0, 0, 0};
+      if (d.hasContact) contact_hvp_gather(d, v, ch);
+      const double M = d.mass[v];
+      const bool pin = d.pinned[v];
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        const int i = v * 3 + c;
+        const double Hp = (sp[c] - sn[c]) / (2 * h);
+        double ap = M * d.p[i] * d.invH2 + Hp;
+        if (d.hasContact) ap += ch[c];
+        if (pin) ap = 0;
+        d.Ap[i] = ap;
+        pAp += d.p[i] * ap;
+      }
+    }
+    put_partial(d, 1, pAp, sm);
+    grid.sync();
+    const double pApT = get_total(d, 1, bc);
+    if (!(pApT > 1e-30)) { iters = k; done = true; break; }
+    const double alpha = rz / pApT;
+    double rr = 0, rzn = 0;
+    for (int i = tid; i < n3; i += nth) {
+      const bool pin = d.pinned[i / 3];
+      double xi = d.dx[i] + alpha * d.p[i];
+      double ri = d.r[i] - alpha * d.Ap[i];
+      if (pin) { xi = 0; ri = 0; }
+      d.dx[i] = xi;
+      d.r[i] = ri;
+      rr += ri * ri;
+      if (jacobi) {
+        double zi = d.diag[i] > 1e-12 ? ri / d.diag[i] : ri;
+        if (pin) zi = 0;
+        d.z[i] = zi;
+        rzn += ri * zi;
+      }
+    }
+    put_partial(d, 2, rr, sm);
+    if (jacobi) put_partial(d, 3, rzn, sm);
+    grid.sync();
+    residual = sqrt(get_total(d, 2, bc));
+    if (residual < absTol) { iters = k + 1; done = true; break; }
+    if (!jacobi) {
+      rzn = 0;
+      for (int dom = tid; dom < d.D; dom += nth) rzn += schwarz_apply_domain(d, dom);
+      put_partial(d, 3, rzn, sm);
+      grid.sync();
+    }
+    const double rzNew = get_total(d, 3, bc);
+    const double beta = rzNew / rz;
+    double pp = 0;
+    for (int i = tid; i < n3; i += nth) {
+      const double pi = d.z[i] + beta * d.p[i];
+      d.p[i] = pi;
+      pp += pi * pi;
+    }
+    rz = rzNew;
+    put_partial(d, 0, pp, sm);
+    grid.sync();
+  }
+  if (!done) iters = A.maxIters;
+  // --- descent safeguard + trust region (newton.ts:152-179) ---
+  grid.sync();
+  double gt = 0;
+  for (int i = tid; i < n3; i += nth) gt += d.g[i] * d.dx[i];
+  put_partial(d, 4, gt, sm);
+  grid.sync();
+  double gtdx = get_total(d, 4, bc);
+  bool fallback = false;
+  if (!isfinite(gtdx) || gtdx >= 0) {
+    fallback = true;
+    gt = 0;
+    for (int i = tid; i < n3; i += nth) {
+      const double di = -d.g[i] / d.diag[i];
+      d.dx[i] = di;
+      gt += d.g[i] * di;
+    }
+    put_partial(d, 5, gt, sm);
+    grid.sync();
+    gtdx = get_total(d, 5, bc);
+  }
+  double mx = 0;
+  for (int i = tid; i < n3; i += nth) {
+    const double a = fabs(d.dx[i]);
+    if (a > mx) mx = a;
+  }
+  const double bmx = block_max_nonan(mx, sm);
+  if (threadIdx.x == 0) d.part[6 * d.partStride + blockIdx.x] = bmx;
+  grid.sync();
+  const double maxDx = get_max_nonan(d, 6, bc);
+  const double TRUST = 0.002;
+  if (maxDx > TRUST) {
+    const double s = TRUST / maxDx;
+    for (int i = tid; i < n3; i += nth) d.dx[i] *= s;
+    gtdx *= s;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    d.scal[S_PCG_ITERS] = iters;
+    d.scal[S_PCG_RES] = residual;
+    d.scal[S_GTDX] = gtdx;
+    d.scal[S_FALLBACK] = fallback ? 1 : 0;
+    d.scal[S_MAXDX] = maxDx;
+  }
+}
+
+// ---- Armijo trial + velocity ----------------------------------------------------
+__global__ void k_trial(Dev d, double alpha) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.n * 3) return;
+  d.xt[i] = d.x[i] + alpha * d.dx[i];
+}
+
+__global__ void k_velocity(Dev d, double damp) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.n * 3) return;
+  d.v[i] = ((d.x[i] - d.x0[i]) / d.h) * damp;
+}
+
+// ---- launchers ------------------------------------------------------------------
+static inline int nblk(int n) { return (n + kThreads - 1) / kThreads; }
+
+void launch_predict(const Dev& d, cudaStream_t s) {
+  k_predict<<<nblk(d.n), kThreads, 0, s>>>(d);
+  launch_pins(d, d.x, s);
+}
+void launch_pins(const Dev& d, double* x, cudaStream_t s) {
+  if (d.npins > 0) k_pins<<<nblk(d.npins), kThreads, 0, s>>>(d, x);
+}
+void launch_grad(const Dev& d, cudaStream_t s) {
+  k_tri_grad<<<nblk(d.m), kThreads, 0, s>>>(d);
+  if (d.kb > 0 && d.hg > 0) k_hinge_grad<<<nblk(d.hg), kThreads, 0, s>>>(d);
+  k_gather_grad<<<nblk(d.n), kThreads, 0, s>>>(d);
+  k_grad_final<<<1, 32, 0, s>>>(d, nblk(d.m), nblk(d.n));
+}
+void launch_energy(const Dev& d, const double* x, cudaStream_t s) {
+  const int nb = nblk(std::max(std::max(d.n, d.m), d.hg));
+  k_energy<<<nb, kThreads, 0, s>>>(d, x);
+  k_energy_final<<<1, 32, 0, s>>>(d, nb);
+}
+void launch_diag_init(const Dev& d, double beta, cudaStream_t s) {
+  k_diag_init<<<nblk(d.n * 3), kThreads, 0, s>>>(d, beta);
+}
+void launch_schwarz_factor(const Dev& d, cudaStream_t s) {
+  k_schwarz_factor<<<(d.D + kSchwarzWarps - 1) / kSchwarzWarps, kSchwarzWarps * 32, 0, s>>>(d);
+}
+int pcg_grid_blocks(const Dev& d) {
+  int dev = 0, sms = 0, per = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pcg, kThreads, 0);
+  const int want = nblk(std::max(d.n * 3, d.m));
+  int cap = per * sms;
+  if (cap < 1) cap = 1;
+  return std::max(1, std::min(want, std::min(cap, d.partStride)));
+}
+int launch_pcg(const Dev& d, int maxIters, double tol, int gridBlocks, cudaStream_t s) {
+  PcgArgs a{d, maxIters, tol};
+  void* args[] = {&a};
+  return (int)cudaLaunchCooperativeKernel((void*)k_pcg, dim3(gridBlocks), dim3(kThreads), args, 0, s);
+}
+void launch_trial(const Dev& d, double alpha, cudaStream_t s) {
+  k_trial<<<nblk(d.n * 3), kThreads, 0, s>>>(d, alpha);
+  launch_pins(d, d.xt, s);
+}
+void launch_velocity(const Dev& d, double damp, cudaStream_t s) {
+  k_velocity<<<nblk(d.n * 3), kThreads, 0, s>>>(d, damp);
+}
+
+}  // namespace cs

@@ -1,0 +1,78 @@
+// Device-side data of one solver instance and the kernel launchers of the
+// FP64 path. All arrays live in HBM for the lifetime of the solver.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "elem.cuh"
+
+namespace cs {
+
+// Slots of the device scalar array (double).
+enum ScalarSlot {
+  S_GRADNORM = 0, S_MAXSTRAIN, S_ENERGY_TRIAL, S_GTDX, S_PCG_ITERS, S_PCG_RES, S_E_INERTIA,
+  S_E_TRI, S_E_HINGE, S_E_MERIT, S_FALLBACK, S_MAXDX, S_VALID, S_MINDIST, S_MINTOI, S_CCDFAIL,
+  S_BARRIER_E, S_FWORK, S_NSCALARS = 32
+};
+
+struct Contact;  // contact.cuh
+
+// Everything a kernel of the FP64 path needs, passed by value.
+struct Dev {
+  int n, m, hg, npins;
+  // mesh constants (Float32, as the reference stores them)
+  const uint32_t* idx;     // 3m
+  const float4* inv;       // m: Dm^-1 (a,b,c,d)
+  const float* area;       // m
+  const float* mass;       // n
+  const int4* hinge;       // hg: v0,v1,v2,v3
+  const double* hmeta;     // 3hg: restAngle, edgeLen, areaSum
+  // CSR incidence, element-ordered (record = elem << 2 | corner)
+  const uint32_t* memOff;  // n+1
+  const uint32_t* memRec;  // 3m
+  const uint32_t* hinOff;  // n+1
+  const uint32_t* hinRec;  // 4hg (distinct corners)
+  // pins
+  const uint8_t* pinned;   // n
+  const int* pinIds;       // npins
+  const double* pinPos;    // 3 npins
+  // state and work vectors (3n doubles each)
+  double *x, *v, *x0, *yHat, *g, *diag, *dx, *r, *z, *p, *Ap, *xt, *cgrad, *cHp;
+  double* elem;            // 18m element-local scratch
+  double* helem;           // 12hg
+  double* part;            // partial sums: NPART rows x maxBlocks
+  int partStride;
+  double* scal;            // S_NSCALARS
+  // material
+  Mat<double> mat;
+  double kb, h, invH2;
+  double gravity[3];
+  // one-level additive Schwarz (<= 8 vertices per domain)
+  int D;
+  const int* domStart;     // D+1
+  const int* domVerts;     // n (members, ascending per domain)
+  const int* v2tOff;       // n+1 vertex -> incident triangles (ascending)
+  const int* v2t;          // 3m
+  double* L;               // D x 576 (24x24 row-major), Cholesky or inverse diagonal
+  uint8_t* domFlag;        // D
+  int precond;             // 0 Jacobi, 1 Schwarz
+  Contact* contact;        // device pointer to contact data, or nullptr
+  int hasContact;
+};
+
+constexpr int kThreads = 256;
+constexpr int NPART = 8;
+
+// Launchers (plain.cu).
+void launch_predict(const Dev& d, cudaStream_t s);
+void launch_pins(const Dev& d, double* x, cudaStream_t s);
+void launch_grad(const Dev& d, cudaStream_t s);           // g, gradNorm, maxStrain
+void launch_energy(const Dev& d, const double* x, cudaStream_t s);  // S_ENERGY_TRIAL
+void launch_diag_init(const Dev& d, double beta, cudaStream_t s);
+void launch_schwarz_factor(const Dev& d, cudaStream_t s);
+int launch_pcg(const Dev& d, int maxIters, double tol, int gridBlocks, cudaStream_t s);
+void launch_trial(const Dev& d, double alpha, cudaStream_t s);   // xt = x + alpha dx, pins
+void launch_velocity(const Dev& d, double damp, cudaStream_t s);
+int pcg_grid_blocks(const Dev& d);
+
+}  // namespace cs

@@ -1,0 +1,154 @@
+/*
+ * closim_cuda.h - C ABI of the B200 CUDA cloth solver (libclosim_cuda.so).
+ *
+ * Drop-in replacement for the reference's ClothSolver backend
+ * (mohdabraralikhan/closim src/backend/solver.ts:5-13, implemented on the CPU
+ * by src/backend/cpu-solver.ts). A host binding (N-API addon, ctypes, ...)
+ * wraps one cs_solver per ClothScene. Plain pointers and sizes only.
+ *
+ * Frame: y-up, as the reference (gravity defaults to {0,-9.81,0}, the floor is
+ * a y = const plane).
+ *
+ * Errors: every call returns CS_OK (0) or a CS_E_* code; cs_last_error()
+ * returns a message. A handle is synchronous and single-threaded; separate
+ * handles are independent.
+ */
+#ifndef CLOSIM_CUDA_H
+#define CLOSIM_CUDA_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  CS_OK = 0,
+  CS_E_UNINIT = 1,     /* "CpuSolver not initialized" (cpu-solver.ts:16,21,26,41,46) */
+  CS_E_NONFINITE = 2,  /* "non-finite gradient - blow up; reduce dt/stiffness" (newton.ts:129) */
+  CS_E_CAPACITY = 3,   /* a device buffer was too small; the call was not applied */
+  CS_E_CUDA = 4,       /* CUDA runtime error */
+  CS_E_ARG = 5         /* invalid argument */
+};
+
+enum { CS_PRECISION_FP64 = 0, CS_PRECISION_MIXED = 1 };
+enum { CS_PRECOND_JACOBI = 0, CS_PRECOND_SCHWARZ = 1 };
+
+/* ClothMaterial (src/physics/types.ts:1-12). */
+typedef struct cs_material {
+  double areal_density;   /* kg/m^2, lumped mass only */
+  double thickness;       /* m, scales the elastic energy */
+  double stretch_warp;    /* C00 */
+  double stretch_weft;    /* C11 */
+  double stretch_coupling;/* C01 */
+  double shear;           /* G */
+  double bend_warp;
+  double bend_weft;
+  double damping;         /* 0..0.1 velocity damping */
+} cs_material;
+
+/* ContactParams (src/collision/types.ts:27-47). */
+typedef struct cs_contact_params {
+  double dhat;            /* barrier activation distance, m */
+  double kappa;           /* barrier energy scale, J */
+  double dmin;            /* minimum admissible distance, m */
+  double mu;              /* Coulomb coefficient */
+  double eps;             /* friction regularization, m */
+} cs_contact_params;
+
+/* Preprocessed ClothMeshData (src/mesh/mesh.ts:3-14). */
+typedef struct cs_mesh {
+  int32_t n, m, hg;           /* vertices, triangles, hinges */
+  const uint32_t* indices;    /* 3m */
+  const float* rest;          /* 3n rest positions (Schwarz domain seeding) */
+  const float* inv_dm;        /* 4m: a,b,c,d */
+  const float* area;          /* m */
+  const float* mass;          /* n lumped */
+  const int32_t* hinge;       /* 4hg: v0,v1 (shared edge), v2, v3 */
+  const double* hinge_meta;   /* 3hg: restAngle, edgeLen, areaSum */
+} cs_mesh;
+
+/* StepperOptions (src/solver/newton.ts:20-25) + preconditioner choice. */
+typedef struct cs_stepper_options {
+  int32_t newton_iters;   /* default 10 */
+  int32_t pcg_max_iters;  /* default 60 */
+  int32_t ls_iters;       /* default 10 */
+  int32_t precond;        /* CS_PRECOND_* (Schwarz domains: target 8, min 1) */
+  double grad_tol;        /* default 1e-5 */
+} cs_stepper_options;
+
+/* StepStats (src/solver/newton.ts:10-18) + ContactDiagnostics
+ * (src/collision/types.ts:49-62) + counters of this implementation. */
+typedef struct cs_step_stats {
+  int32_t newton_iters;       /* the configured budget, as the reference reports */
+  int32_t pcg_iters;          /* summed over Newton iterations */
+  double grad_norm, energy, max_strain;
+  int32_t converged;
+  int32_t has_contact;
+  double candidate_pairs, active_pairs, vt_pairs, ee_pairs, floor_pairs;
+  double min_distance, min_toi, barrier_energy, friction_work;
+  double rejected_line_search_steps, ccd_failures;
+  int32_t newton_iters_used;  /* iterations actually run */
+  int32_t armijo_trials;      /* line-search trials run */
+} cs_step_stats;
+
+typedef struct cs_solver cs_solver;
+
+/* Creates a solver on CUDA device `device` (precision: CS_PRECISION_*). */
+cs_solver* cs_create(int precision, int device);
+void cs_destroy(cs_solver* s);
+const char* cs_last_error(cs_solver* s);
+
+/* ClothSolver.initialize(scene) (solver.ts:6): uploads mesh, material,
+ * gravity, positions x (3n f64) and velocities v (3n f64; NULL = zero). */
+int cs_initialize(cs_solver* s, const cs_mesh* mesh, const cs_material* mat,
+                  const double gravity[3], const double* x, const double* v);
+/* scene.contact = new ContactSystem(params, indices) + setFloor + setStaticMesh
+ * (contact-assembly.ts:63-73). params NULL disables contact. */
+int cs_set_contact(cs_solver* s, const cs_contact_params* params, int floor_on, double floor_y,
+                   const float* static_pos, int32_t ns, const uint32_t* static_idx, int32_t ms);
+int cs_set_stepper_options(cs_solver* s, const cs_stepper_options* opts);
+/* ClothSolver.setMaterial (solver.ts:8). */
+int cs_set_material(cs_solver* s, const cs_material* mat);
+/* Replaces the pin map (scene.pinned, solver.ts:9-10): k ids and 3k positions. */
+int cs_set_pins(cs_solver* s, int32_t k, const int32_t* ids, const double* pos);
+/* ClothSolver.step(dt) (solver.ts:7; cpu-solver.ts:15-18). */
+int cs_step(cs_solver* s, double dt);
+/* getPositions / getVelocities (solver.ts:11-12): copy 3n f64 out. */
+int cs_get_positions(cs_solver* s, double* out);
+int cs_get_velocities(cs_solver* s, double* out);
+/* Overwrites positions and/or velocities (either may be NULL). */
+int cs_set_state(cs_solver* s, const double* x, const double* v);
+/* CpuSolver.lastStats (cpu-solver.ts:6). */
+int cs_last_stats(cs_solver* s, cs_step_stats* out);
+
+/* ---- device-resident helpers (no reference counterpart needed by a drop-in) ---- */
+/* Runs `nsteps` steps back to back without copying state to the host. */
+int cs_step_n(cs_solver* s, double dt, int32_t nsteps);
+/* Synchronizes the solver's stream; returns CS_E_CUDA on a pending error. */
+int cs_sync(cs_solver* s);
+/* Number of this library's kernel launches since creation. */
+int64_t cs_kernel_launches(cs_solver* s);
+/* The solver's CUDA stream (cudaStream_t), for recording events around calls. */
+void* cs_stream(cs_solver* s);
+/* Per-launch timing of the linear-solve kernel (the dominant kernel): when
+ * enabled, each launch is bracketed by CUDA events on the solver's stream.
+ * cs_profile_read fills out[5]: total ms, launches, algorithmic bytes, PCG
+ * iterations, and the flush-free mean ms per launch. */
+int cs_profile(cs_solver* s, int enable);
+int cs_profile_read(cs_solver* s, double* out5);
+
+/* ---- mesh preprocessing (src/mesh/mesh.ts:17-126), host side ---- */
+/* buildGrid(nx, ny, w, h): pos 3n f32, uv 2n f32, idx 6*nx*ny u32. */
+int cs_build_grid(int32_t nx, int32_t ny, double w, double h, float* pos, float* uv, uint32_t* idx);
+/* preprocess(positions, uv, indices, density): inv_dm 4m, area m, mass n; the
+ * hinge count is returned through *hg and hinge / hinge_meta receive 4hg / 3hg
+ * values. Any output pointer may be NULL (a first call with NULLs sizes hg). */
+int cs_preprocess(int32_t n, int32_t m, const float* pos, const float* uv, const uint32_t* idx,
+                  double density, float* inv_dm, float* area, float* mass, int32_t* hg,
+                  int32_t* hinge, double* hinge_meta);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CLOSIM_CUDA_H */

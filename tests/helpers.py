@@ -76,3 +76,30 @@ def pin_column(x, pred):
         if pred(x[i * 3], x[i * 3 + 1], x[i * 3 + 2], i):
             pins[i] = (x[i * 3], x[i * 3 + 1], x[i * 3 + 2])
     return pins
+
+
+def oracle_scene(cfg):
+    """Oracle scene (CpuSolver equivalent) from a closim_b200.configs workload dict."""
+    mesh = O.Mesh(cfg["pos"], cfg["uv"], cfg["idx"], cfg["density"])
+    m = cfg["material"]
+    mat = dict(arealDensity=m["arealDensityKgM2"], thickness=m["thickness"], C00=m["stretchWarp"],
+               C11=m["stretchWeft"], C01=m["stretchCoupling"], G=m["shear"], bendWarp=m["bendWarp"],
+               bendWeft=m["bendWeft"], damping=m["damping"])
+    sc = O.Scene(mesh, mat, gravity=cfg["gravity"], x=cfg["x"], v=cfg["v"])
+    c = cfg["contact"]
+    if c is not None:
+        cs = O.ContactSystem(dict(dHat=c["dHatM"], kappa=c["kappaJ"], dMin=c["dMinM"], mu=c["frictionMu"],
+                                  eps=c["frictionEpsM"]), mesh.indices)
+        if c.get("floorY") is not None:
+            cs.set_floor(c["floorY"])
+        if c.get("staticPos") is not None:
+            cs.set_static_mesh(c["staticPos"], c["staticIdx"])
+        sc.set_contact(cs)
+        sc._cs = cs
+    return sc
+
+
+def oracle_step_kwargs(cfg):
+    o = cfg["options"]
+    return dict(newton_iters=o["newtonIters"], pcg_max_iters=o["pcgMaxIters"], grad_tol=o["gradTol"],
+                ls_iters=o["lineSearchIters"], precond=o["precond"])
