@@ -1,0 +1,446 @@
+// LBVH broadphase kernels (FP64 path file: compiled with -fmad=false).
+//
+// The pipeline follows the reference's FP32 mirror (gpu-broadphase.ts:193-386):
+// swept AABB + centroid per triangle, 30-bit centroid Morton key, (key, triId)
+// order (a stable radix sort of the key over triangle order), Karras 2012
+// hierarchy with the sorted-position tiebreak, refit, per-leaf traversal.
+// The refit here is bottom-up with one atomic arrival counter per node (the
+// second child to arrive merges and climbs; no thread ever waits).
+//
+// Exactness for the FP64 path: internal nodes carry outward-rounded f32 boxes
+// of the exact f64 swept boxes, and every leaf hit is re-tested with the f64
+// boxes, so the emitted pair set equals the reference CPU BVH's set (all
+// non-adjacent triangle pairs whose padded swept boxes overlap, inclusive),
+// independent of tree shape (src/collision/bvh.ts:79-124).
+#include "broadphase.cuh"
+#include "common.cuh"
+
+namespace cs {
+
+constexpr int kBT = 256;
+static inline int nb(int n) { return (n + kBT - 1) / kBT; }
+
+__device__ __forceinline__ float rd(double v) { return __double2float_rd(v); }
+__device__ __forceinline__ float ru(double v) { return __double2float_ru(v); }
+
+// ---- boxes (aabb.ts:9-31 in f64; gpu-broadphase.ts:54-93 in FP32) ----------------
+__global__ void k_boxes(BvhBufs b, const double* x0, const double* x1, double pad) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= b.m) return;
+  const int ids[3] = {(int)b.idx[t * 3], (int)b.idx[t * 3 + 1], (int)b.idx[t * 3 + 2]};
+  double mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+  float fmn[3] = {INFINITY, INFINITY, INFINITY}, fmx[3] = {-INFINITY, -INFINITY, -INFINITY};
+  for (int q = 0; q < 3; q++) {
+    const int v = ids[q];
+    for (int w = 0; w < 2; w++) {
+      const double* x = w == 0 ? x0 : x1;
+      for (int k = 0; k < 3; k++) {
+        const double c = x[v * 3 + k];
+        if (c < mn[k]) mn[k] = c;
+        if (c > mx[k]) mx[k] = c;
+        const float cf = (float)c;
+        if (cf < fmn[k]) fmn[k] = cf;
+        if (cf > fmx[k]) fmx[k] = cf;
+      }
+    }
+  }
+  const float pf = (float)pad;
+  for (int k = 0; k < 3; k++) {
+    const double lo = mn[k] - pad, hi = mx[k] + pad;
+    b.box64[t * 6 + k] = lo;
+    b.box64[t * 6 + 3 + k] = hi;
+    b.boxc[t * 6 + k] = rd(lo);
+    b.boxc[t * 6 + 3 + k] = ru(hi);
+    b.boxr[t * 6 + k] = __fsub_rn(fmn[k], pf);
+    b.boxr[t * 6 + 3 + k] = __fadd_rn(fmx[k], pf);
+    float s = 0.f;
+    for (int q = 0; q < 3; q++) {
+      s = __fadd_rn(s, (float)x0[ids[q] * 3 + k]);
+      s = __fadd_rn(s, (float)x1[ids[q] * 3 + k]);
+    }
+    b.cent[t * 3 + k] = __fdiv_rn(s, 6.f);
+  }
+}
+
+// Centroid bounds (min/max are exact, so one block's fixed loop suffices).
+__global__ void __launch_bounds__(1024) k_scene_bounds(BvhBufs b) {
+  __shared__ float sm[6][1024];
+  float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+  for (int t = threadIdx.x; t < b.m; t += blockDim.x)
+    for (int k = 0; k < 3; k++) {
+      const float c = b.cent[t * 3 + k];
+      if (c < mn[k]) mn[k] = c;
+      if (c > mx[k]) mx[k] = c;
+    }
+  for (int k = 0; k < 3; k++) { sm[k][threadIdx.x] = mn[k]; sm[3 + k][threadIdx.x] = mx[k]; }
+  __syncthreads();
+  for (int off = 512; off > 0; off >>= 1) {
+    if ((int)threadIdx.x < off)
+      for (int k = 0; k < 3; k++) {
+        const float a = sm[k][threadIdx.x + off], c = sm[3 + k][threadIdx.x + off];
+        if (a < sm[k][threadIdx.x]) sm[k][threadIdx.x] = a;
+        if (c > sm[3 + k][threadIdx.x]) sm[3 + k][threadIdx.x] = c;
+      }
+    __syncthreads();
+  }
+  if (threadIdx.x < 6) b.scene[threadIdx.x] = sm[threadIdx.x][0];
+}
+
+__device__ __forceinline__ uint32_t expand10(uint32_t v) {
+  uint32_t x = v & 1023u;
+  x = (x | (x << 16)) & 0x030000ffu;
+  x = (x | (x << 8)) & 0x0300f00fu;
+  x = (x | (x << 4)) & 0x030c30c3u;
+  x = (x | (x << 2)) & 0x09249249u;
+  return x;
+}
+
+// gpu-broadphase.ts:105-117 mortonKeyOf: span = max(f32 span, 1e-9 as a double),
+// n = fround(fround(c - min) / span) clamped to [0,1], q = floor(n * 1023).
+__global__ void k_morton(BvhBufs b) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= b.m) return;
+  uint32_t q[3];
+  for (int k = 0; k < 3; k++) {
+    const float smin = b.scene[k], smax = b.scene[3 + k];
+    double span = (double)__fsub_rn(smax, smin);
+    if (!(span > 1e-9)) span = span != span ? span : 1e-9;
+    const float dc = __fsub_rn(b.cent[t * 3 + k], smin);
+    const float nf = __double2float_rn((double)dc / span);
+    double nn = (double)nf;
+    nn = js_min(1.0, js_max(0.0, nn));
+    q[k] = (uint32_t)floor(nn * 1023.0);
+  }
+  b.k0[t].w[0] = (expand10(q[0]) << 2) | (expand10(q[1]) << 1) | expand10(q[2]);
+  b.p0[t] = (uint32_t)t;
+}
+
+__device__ __forceinline__ int delta_pos(const Key<1>* keys, int p, int q, int n) {
+  if (q < 0 || q >= n) return -1;
+  const uint32_t kp = keys[p].w[0], kq = keys[q].w[0];
+  if (kp != kq) return __clz(kp ^ kq);
+  return 32 + __clz((uint32_t)(p ^ q));
+}
+
+// gpu-broadphase.ts:253-299: range + split per internal node (power-of-two strides).
+__global__ void k_karras(BvhBufs b, const Key<1>* sk) {
+  const int m = b.m;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m - 1) return;
+  const int dNext = delta_pos(sk, i, i + 1, m);
+  const int dPrev = delta_pos(sk, i, i - 1, m);
+  int d = 1, dMin = dPrev;
+  if (dPrev > dNext) { d = -1; dMin = dNext; }
+  long lMax = 2;
+  while (delta_pos(sk, i, (int)(i + d * lMax), m) > dMin) {
+    lMax *= 2;
+    if (lMax > m) break;
+  }
+  long l = 0, t = lMax / 2;
+  while (t > 0) {
+    if (delta_pos(sk, i, (int)(i + d * (l + t)), m) > dMin) l += t;
+    t /= 2;
+  }
+  const int j = (int)(i + d * l);
+  const int lo = min(i, j), hi = max(i, j);
+  const int dNode = delta_pos(sk, lo, hi, m);
+  int split = lo, stride = 1;
+  while (stride * 2 <= hi - lo) stride *= 2;
+  while (stride > 0) {
+    const int mid = split + stride;
+    if (mid < hi && delta_pos(sk, lo, mid, m) > dNode) split = mid;
+    stride /= 2;
+  }
+  const int L = split == lo ? m - 1 + lo : split;
+  const int R = split + 1 == hi ? m - 1 + split + 1 : split + 1;
+  b.left[i] = L;
+  b.right[i] = R;
+  b.parent[L] = i;
+  b.parent[R] = i;
+  if (lo == 0 && hi == m - 1) *b.root = i;
+}
+
+__global__ void k_node_init(BvhBufs b) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nn = 2 * b.m - 1;
+  if (i >= nn) return;
+  if (i < b.m - 1) {
+    // Unreached internal nodes stay infinite, which keeps traversal conservative.
+    for (int k = 0; k < 3; k++) { b.nbox[i * 6 + k] = -INFINITY; b.nbox[i * 6 + 3 + k] = INFINITY; }
+  }
+  b.visit[i] = 0;
+  b.parent[i] = -1;
+  b.depth[i] = 1;
+}
+
+// Leaf boxes, then climb: the second child to arrive at a node merges both
+// children and continues. Bounded by the node count.
+__global__ void k_refit(BvhBufs b, const uint32_t* sp, bool mirror) {
+  const int m = b.m;
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= m) return;
+  const int slot = m - 1 + s;
+  const uint32_t tri = sp[s];
+  const float* src = mirror ? b.boxr : b.boxc;
+  for (int k = 0; k < 6; k++) b.nbox[slot * 6 + k] = src[tri * 6 + k];
+  b.depth[slot] = 1;
+  __threadfence();
+  int node = b.parent[slot];
+  for (int guard = 0; node >= 0 && guard < 2 * m; guard++) {
+    const uint32_t prev = atomicAdd(&b.visit[node], 1u);
+    if (prev == 0) return;
+    __threadfence();
+    const int L = b.left[node], R = b.right[node];
+    for (int k = 0; k < 3; k++) {
+      const float a = ((volatile float*)b.nbox)[L * 6 + k], c = ((volatile float*)b.nbox)[R * 6 + k];
+      b.nbox[node * 6 + k] = fminf(a, c);
+      const float a2 = ((volatile float*)b.nbox)[L * 6 + 3 + k], c2 = ((volatile float*)b.nbox)[R * 6 + 3 + k];
+      b.nbox[node * 6 + 3 + k] = fmaxf(a2, c2);
+    }
+    const int dL = ((volatile int*)b.depth)[L], dR = ((volatile int*)b.depth)[R];
+    b.depth[node] = max(dL, dR) + 1;
+    __threadfence();
+    node = b.parent[node];
+  }
+}
+
+__device__ __forceinline__ bool ov6(const float* a, const float* c) {
+  return a[0] <= c[3] && a[3] >= c[0] && a[1] <= c[4] && a[4] >= c[1] && a[2] <= c[5] && a[5] >= c[2];
+}
+__device__ __forceinline__ bool ov6d(const double* a, const double* c) {
+  return a[0] <= c[3] && a[3] >= c[0] && a[1] <= c[4] && a[4] >= c[1] && a[2] <= c[5] && a[5] >= c[2];
+}
+__device__ __forceinline__ bool share_vertex(const uint32_t* idx, int a, int c) {
+  const uint32_t A0 = idx[a * 3], A1 = idx[a * 3 + 1], A2 = idx[a * 3 + 2];
+  const uint32_t B0 = idx[c * 3], B1 = idx[c * 3 + 1], B2 = idx[c * 3 + 2];
+  return A0 == B0 || A0 == B1 || A0 == B2 || A1 == B0 || A1 == B1 || A1 == B2 || A2 == B0 || A2 == B1 || A2 == B2;
+}
+
+constexpr int kStack = 64;
+
+// Self traversal per sorted leaf s (gpu-broadphase.ts:321-357): children of
+// each popped node are tested against the query leaf's box; leaves with a
+// larger triangle id that share no vertex are pairs. emit = false counts only.
+template <bool EMIT>
+__global__ void k_self(BvhBufs b, const uint32_t* sp, bool mirror) {
+  const int m = b.m;
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= m) return;
+  const int q = (int)sp[s];
+  const float* qb = b.nbox + (size_t)(m - 1 + s) * 6;
+  float qbox[6];
+  for (int k = 0; k < 6; k++) qbox[k] = qb[k];
+  const double* q64 = b.box64 + (size_t)q * 6;
+  uint32_t count = 0;
+  uint32_t out = EMIT ? b.cnt[s] : 0;
+  int stack[kStack];
+  int sp_ = 0;
+  stack[sp_++] = *b.root;
+  while (sp_ > 0) {
+    const int node = stack[--sp_];
+    const int ch[2] = {b.left[node], b.right[node]};
+    for (int c = 0; c < 2; c++) {
+      const int child = ch[c];
+      if (child < 0 || !ov6(qbox, b.nbox + (size_t)child * 6)) continue;
+      if (child >= m - 1) {
+        const int tL = (int)sp[child - (m - 1)];
+        if (tL > q && !share_vertex(b.idx, q, tL) && (mirror || ov6d(q64, b.box64 + (size_t)tL * 6))) {
+          if (EMIT) b.pairs[out++] = make_int2(q, tL);
+          count++;
+        }
+      } else {
+        if (sp_ >= kStack) { atomicOr(b.flags, 1); return; }
+        stack[sp_++] = child;
+      }
+    }
+  }
+  if (!EMIT) b.cnt[s] = count;
+}
+
+// Static triangles against the cloth hierarchy (contact-assembly.ts:96-140):
+// box = f32 static vertices in f64 +- pad (static, not swept).
+__device__ __forceinline__ void static_box(const BvhBufs& b, int st, double pad, double* o) {
+  double mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+  for (int q = 0; q < 3; q++) {
+    const uint32_t v = b.sidx[st * 3 + q];
+    for (int k = 0; k < 3; k++) {
+      const double c = b.spos[v * 3 + k];
+      mn[k] = js_min(mn[k], c);
+      mx[k] = js_max(mx[k], c);
+    }
+  }
+  for (int k = 0; k < 3; k++) { o[k] = mn[k] - pad; o[3 + k] = mx[k] + pad; }
+}
+
+template <bool EMIT>
+__global__ void k_static(BvhBufs b, const uint32_t* sp, double pad, int2* outp) {
+  const int st = blockIdx.x * blockDim.x + threadIdx.x;
+  if (st >= b.ms) return;
+  const int m = b.m;
+  double s64[6];
+  static_box(b, st, pad, s64);
+  float sb[6];
+  for (int k = 0; k < 3; k++) { sb[k] = __double2float_rd(s64[k]); sb[3 + k] = __double2float_ru(s64[3 + k]); }
+  uint32_t count = 0;
+  uint32_t out = EMIT ? b.cnt[st] : 0;
+  int stack[kStack];
+  int sp_ = 0;
+  if (m == 1) {
+    if (ov6d(b.box64, s64)) {
+      if (EMIT) outp[out++] = make_int2(0, st);
+      count++;
+    }
+  } else {
+    stack[sp_++] = *b.root;
+    // the root itself is tested too (queryBvhAll tests every popped node)
+    if (!ov6(sb, b.nbox + (size_t)(*b.root) * 6)) sp_ = 0;
+  }
+  while (sp_ > 0) {
+    const int node = stack[--sp_];
+    const int ch[2] = {b.left[node], b.right[node]};
+    for (int c = 0; c < 2; c++) {
+      const int child = ch[c];
+      if (child < 0 || !ov6(sb, b.nbox + (size_t)child * 6)) continue;
+      if (child >= m - 1) {
+        const int tL = (int)sp[child - (m - 1)];
+        if (ov6d(b.box64 + (size_t)tL * 6, s64)) {
+          if (EMIT) outp[out++] = make_int2(tL, st);
+          count++;
+        }
+      } else {
+        if (sp_ >= kStack) { atomicOr(b.flags, 1); return; }
+        stack[sp_++] = child;
+      }
+    }
+  }
+  if (!EMIT) b.cnt[st] = count;
+}
+
+void scan_counts(uint32_t* cnt, int n, uint32_t* total, cudaStream_t s, int64_t* launches) {
+  k_scan_exclusive<<<1, 1024, 0, s>>>(cnt, n, total);
+  if (launches) *launches += 1;
+}
+
+void bvh_build(BvhBufs& b, const double* x0, const double* x1, double pad, bool mirror, cudaStream_t s,
+               int64_t* launches) {
+  const int m = b.m;
+  k_boxes<<<nb(m), kBT, 0, s>>>(b, x0, x1, pad);
+  k_scene_bounds<<<1, 1024, 0, s>>>(b);
+  k_morton<<<nb(m), kBT, 0, s>>>(b);
+  *launches += 3;
+  const bool flip = radix_sort<1>(b.k0, b.p0, b.k1, b.p1, m, 30, b.hist, s, launches);
+  const Key<1>* sk = flip ? b.k1 : b.k0;
+  const uint32_t* sp = flip ? b.p1 : b.p0;
+  if (flip) {  // keep the sorted result in (k0, p0)
+    cudaMemcpyAsync(b.k0, sk, (size_t)m * sizeof(Key<1>), cudaMemcpyDeviceToDevice, s);
+    cudaMemcpyAsync(b.p0, sp, (size_t)m * 4, cudaMemcpyDeviceToDevice, s);
+  }
+  k_node_init<<<nb(2 * m - 1), kBT, 0, s>>>(b);
+  *launches += 1;
+  cudaMemsetAsync(b.root, 0, sizeof(int), s);
+  if (m > 1) {
+    k_karras<<<nb(m - 1), kBT, 0, s>>>(b, b.k0);
+    *launches += 1;
+  }
+  k_refit<<<nb(m), kBT, 0, s>>>(b, b.p0, mirror);
+  *launches += 1;
+}
+
+void bvh_count_self(BvhBufs& b, bool mirror, cudaStream_t s, int64_t* launches) {
+  if (b.m < 2) {
+    cudaMemsetAsync(b.cnt, 0, (size_t)(b.m + 1) * 4, s);
+    return;
+  }
+  k_self<false><<<nb(b.m), kBT, 0, s>>>(b, b.p0, mirror);
+  *launches += 1;
+}
+void bvh_emit_self(BvhBufs& b, bool mirror, cudaStream_t s, int64_t* launches) {
+  if (b.m < 2) return;
+  k_self<true><<<nb(b.m), kBT, 0, s>>>(b, b.p0, mirror);
+  *launches += 1;
+}
+void bvh_count_static(BvhBufs& b, double pad, cudaStream_t s, int64_t* launches) {
+  if (b.ms <= 0) return;
+  k_static<false><<<nb(b.ms), kBT, 0, s>>>(b, b.p0, pad, nullptr);
+  *launches += 1;
+}
+void bvh_emit_static(BvhBufs& b, double pad, int2* out, cudaStream_t s, int64_t* launches) {
+  if (b.ms <= 0) return;
+  k_static<true><<<nb(b.ms), kBT, 0, s>>>(b, b.p0, pad, out);
+  *launches += 1;
+}
+
+// ---- candidates (contact-assembly.ts:87-121, self-collision.ts:23-41) -----------
+__device__ __forceinline__ void put_cand(int* rec, Key<4>* keys, uint32_t* pay, int slot, int kind, int p, int a,
+                                         int bb, int c, int d, int ns) {
+  int* r = rec + (size_t)slot * 6;
+  r[0] = kind; r[1] = p; r[2] = a; r[3] = bb; r[4] = c; r[5] = d;
+  // ids shifted by ns + 2 so static ids -(i+2), -2 and -1 order below cloth ids; 24 bits each
+  const uint64_t off = (uint64_t)(ns + 2);
+  const uint64_t P = (uint64_t)((int64_t)p + off), A = (uint64_t)((int64_t)a + off), B = (uint64_t)((int64_t)bb + off);
+  const uint64_t Cc = (uint64_t)((int64_t)c + off), D = (uint64_t)((int64_t)d + off);
+  const uint64_t hi = ((uint64_t)kind << 56) | (P << 32) | (A << 8) | (B >> 16);
+  const uint64_t lo = ((B & 0xffffull) << 48) | (Cc << 24) | D;
+  keys[slot].w[0] = (uint32_t)(hi >> 32);
+  keys[slot].w[1] = (uint32_t)hi;
+  keys[slot].w[2] = (uint32_t)(lo >> 32);
+  keys[slot].w[3] = (uint32_t)lo;
+  pay[slot] = (uint32_t)slot;
+}
+
+__global__ void k_expand_self(CandBufs c, const uint32_t* idx, const int2* pairs, int np, int ns) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= np) return;
+  const int tA = pairs[i].x, tB = pairs[i].y;
+  const int A[3] = {(int)idx[tA * 3], (int)idx[tA * 3 + 1], (int)idx[tA * 3 + 2]};
+  const int B[3] = {(int)idx[tB * 3], (int)idx[tB * 3 + 1], (int)idx[tB * 3 + 2]};
+  int slot = i * 15;
+  for (int k = 0; k < 3; k++) put_cand(c.rec, c.k0, c.p0, slot++, 0, A[k], B[0], B[1], B[2], -1, ns);
+  for (int k = 0; k < 3; k++) put_cand(c.rec, c.k0, c.p0, slot++, 0, B[k], A[0], A[1], A[2], -1, ns);
+  const int TE[3][2] = {{0, 1}, {1, 2}, {2, 0}};
+  for (int ea = 0; ea < 3; ea++)
+    for (int eb = 0; eb < 3; eb++) {
+      const int a = A[TE[ea][0]], bb = A[TE[ea][1]], cc = B[TE[eb][0]], d = B[TE[eb][1]];
+      if (a == cc || a == d || bb == cc || bb == d) put_cand(c.rec, c.k0, c.p0, slot++, 3, 0, 0, 0, 0, 0, ns);
+      else put_cand(c.rec, c.k0, c.p0, slot++, 1, -1, a, bb, cc, d, ns);
+    }
+}
+
+__global__ void k_expand_static(CandBufs c, const uint32_t* idx, const uint32_t* sidx, const int2* pairs, int np,
+                                int base, int ns) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= np) return;
+  const int ct = pairs[i].x, st = pairs[i].y;
+  const int A[3] = {(int)idx[ct * 3], (int)idx[ct * 3 + 1], (int)idx[ct * 3 + 2]};
+  const int B[3] = {(int)sidx[st * 3], (int)sidx[st * 3 + 1], (int)sidx[st * 3 + 2]};
+  int slot = base + i * 12;
+  for (int k = 0; k < 3; k++) put_cand(c.rec, c.k0, c.p0, slot++, 0, A[k], -(B[0] + 2), -(B[1] + 2), -(B[2] + 2), -2, ns);
+  const int E[3][2] = {{0, 1}, {1, 2}, {2, 0}};
+  for (int e = 0; e < 3; e++)
+    for (int f = 0; f < 3; f++)
+      put_cand(c.rec, c.k0, c.p0, slot++, 1, -1, A[E[e][0]], A[E[e][1]], -(B[E[f][0]] + 2), -(B[E[f][1]] + 2), ns);
+}
+
+__global__ void k_gather_cand(const int* rec, const uint32_t* order, int n, int* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int* r = rec + (size_t)order[i] * 6;
+  int* o = out + (size_t)i * 6;
+  for (int k = 0; k < 6; k++) o[k] = r[k];
+}
+
+void make_candidates(CandBufs& c, const uint32_t* idx, const uint32_t* sidx, int ns, const int2* selfPairs, int nSelf,
+                     const int2* staticPairs, int nStatic, cudaStream_t s, int64_t* launches) {
+  const int n = nSelf * 15 + nStatic * 12;
+  if (n == 0) return;
+  if (nSelf) { k_expand_self<<<nb(nSelf), kBT, 0, s>>>(c, idx, selfPairs, nSelf, ns); *launches += 1; }
+  if (nStatic) {
+    k_expand_static<<<nb(nStatic), kBT, 0, s>>>(c, idx, sidx, staticPairs, nStatic, nSelf * 15, ns);
+    *launches += 1;
+  }
+  const bool flip = radix_sort<4>(c.k0, c.p0, c.k1, c.p1, n, 122, c.hist, s, launches);
+  k_gather_cand<<<nb(n), kBT, 0, s>>>(c.rec, flip ? c.p1 : c.p0, n, c.srt);
+  *launches += 1;
+}
+
+}  // namespace cs

@@ -1,35 +1,107 @@
-// Contact data shared by the FP64 kernels: the frozen active set and the
-// per-vertex gather structures of the barrier HVP.
+// Device functions of the frozen-contact model used inside the FP64 kernels
+// (reference src/collision/contact-assembly.ts:222-414).
 #pragma once
+#include "contact_math.cuh"
 #include "plain.cuh"
 
 namespace cs {
 
-// One frozen contact (contact-assembly.ts:22-30): kind 0 VT, 1 EE, 2 floor.
-struct Frozen {
-  int kind, p, a, b, c, d;
-  double w0, w1, w2, w3, nx, ny, nz;
-};
-
-struct Contact {
-  double dHat, kappa, dMin, mu, eps, floorY;
-  int hasFloor;
-  int nActive;           // active records
-  Frozen* active;        // cap
-  double* dd;            // per-contact HVP coefficient (coeff * J v)
-  // vertex -> (contact << 2 | slot) records in contact order
-  const uint32_t* cOff;  // n+1
-  const uint32_t* cRec;
-};
-
-// Per-contact HVP coefficient (contact-assembly.ts:371-387).
-__device__ __forceinline__ void contact_hvp_coeffs(const Dev& d, const double* v, int tid, int nth) {
-  (void)d; (void)v; (void)tid; (void)nth;
+__device__ __forceinline__ void cpos(const Contact& c, const double* x, int v, double o[3]) {
+  if (v >= 0) { o[0] = x[v * 3]; o[1] = x[v * 3 + 1]; o[2] = x[v * 3 + 2]; return; }
+  const int i = -v - 2;
+  o[0] = c.spos[i * 3]; o[1] = c.spos[i * 3 + 1]; o[2] = c.spos[i * 3 + 2];
 }
 
-// Per-vertex sum of the contact HVP contributions (contact-assembly.ts:388-391).
+// frozenDist (contact-assembly.ts:222-258): n . r(x) with lagged weights.
+__device__ __forceinline__ double frozen_dist(const Contact& c, const double* x, const Frozen& f) {
+  if (f.kind == 2) return x[f.p * 3 + 1] - c.floorY;
+  if (f.kind == 0) {
+    double A[3], B[3], C[3];
+    cpos(c, x, f.a, A); cpos(c, x, f.b, B); cpos(c, x, f.c, C);
+    const double qx = f.w0 * A[0] + f.w1 * B[0] + f.w2 * C[0];
+    const double qy = f.w0 * A[1] + f.w1 * B[1] + f.w2 * C[1];
+    const double qz = f.w0 * A[2] + f.w1 * B[2] + f.w2 * C[2];
+    const double ddx = x[f.p * 3] - qx, ddy = x[f.p * 3 + 1] - qy, ddz = x[f.p * 3 + 2] - qz;
+    return f.nx * ddx + f.ny * ddy + f.nz * ddz;
+  }
+  double A[3], B[3], C[3], D[3];
+  cpos(c, x, f.a, A); cpos(c, x, f.b, B); cpos(c, x, f.c, C); cpos(c, x, f.d, D);
+  const double rx = f.w0 * A[0] + f.w1 * B[0] + f.w2 * C[0] + f.w3 * D[0];
+  const double ry = f.w0 * A[1] + f.w1 * B[1] + f.w2 * C[1] + f.w3 * D[1];
+  const double rz = f.w0 * A[2] + f.w1 * B[2] + f.w2 * C[2] + f.w3 * D[2];
+  return f.nx * rx + f.ny * ry + f.nz * rz;
+}
+
+// distJvp (contact-assembly.ts:394-414).
+__device__ __forceinline__ double dist_jvp(const Frozen& f, const double* v) {
+  if (f.kind == 2) return v[f.p * 3 + 1];
+  if (f.kind == 0) {
+    double j = f.nx * v[f.p * 3] + f.ny * v[f.p * 3 + 1] + f.nz * v[f.p * 3 + 2];
+    const double ws[3] = {f.w0, f.w1, f.w2};
+    const int vs[3] = {f.a, f.b, f.c};
+    for (int k = 0; k < 3; k++) {
+      if (vs[k] < 0) continue;
+      j -= ws[k] * (f.nx * v[vs[k] * 3] + f.ny * v[vs[k] * 3 + 1] + f.nz * v[vs[k] * 3 + 2]);
+    }
+    return j;
+  }
+  const double ws[4] = {f.w0, f.w1, f.w2, f.w3};
+  const int vs[4] = {f.a, f.b, f.c, f.d};
+  double j = 0;
+  for (int k = 0; k < 4; k++) {
+    if (vs[k] < 0) continue;
+    j += ws[k] * (f.nx * v[vs[k] * 3] + f.ny * v[vs[k] * 3 + 1] + f.nz * v[vs[k] * 3 + 2]);
+  }
+  return j;
+}
+
+// addDistGrad contribution of one stencil slot (contact-assembly.ts:288-315).
+__device__ __forceinline__ void dist_grad_slot(const Frozen& f, int slot, double g, double o[3]) {
+  if (f.kind == 2) { o[1] += g; return; }
+  if (f.kind == 0) {
+    if (slot == 0) { o[0] += g * f.nx; o[1] += g * f.ny; o[2] += g * f.nz; return; }
+    const double w = slot == 1 ? f.w0 : slot == 2 ? f.w1 : f.w2;
+    o[0] += -g * w * f.nx; o[1] += -g * w * f.ny; o[2] += -g * w * f.nz;
+    return;
+  }
+  const double w = slot == 0 ? f.w0 : slot == 1 ? f.w1 : slot == 2 ? f.w2 : f.w3;
+  o[0] += g * w * f.nx; o[1] += g * w * f.ny; o[2] += g * w * f.nz;
+}
+
+// addFrictionForce contribution of one slot (contact-assembly.ts:318-341).
+__device__ __forceinline__ void friction_slot(const Frozen& f, int slot, const double* ff, double o[3]) {
+  if (f.kind == 2 || (f.kind == 0 && slot == 0)) { o[0] += ff[0]; o[1] += ff[1]; o[2] += ff[2]; return; }
+  if (f.kind == 0) {
+    const double w = slot == 1 ? f.w0 : slot == 2 ? f.w1 : f.w2;
+    o[0] += -ff[0] * w; o[1] += -ff[1] * w; o[2] += -ff[2] * w;
+    return;
+  }
+  const double w = slot == 0 ? f.w0 : slot == 1 ? f.w1 : slot == 2 ? -f.w2 : -f.w3;
+  o[0] += ff[0] * w; o[1] += ff[1] * w; o[2] += ff[2] * w;
+}
+
+// Per-contact HVP coefficient dd = kappa max(b'', 0) * (J v) (contact-assembly.ts:371-387).
+__device__ __forceinline__ void contact_hvp_coeffs(const Dev& d, const double* v, int tid, int nth) {
+  const Contact& c = d.c;
+  for (int i = tid; i < c.nActive; i += nth) {
+    const Frozen f = c.active[i];
+    const double dist = js_max(frozen_dist(c, d.x, f), 1e-12);
+    double dd = 0;
+    if (dist < c.dHat) dd = barrier_curvature(dist, c.dHat, c.kappa) * dist_jvp(f, v);
+    c.dd[i] = dd;
+  }
+}
+
+// Per-vertex sum of the contact HVP, contacts in order (contact-assembly.ts:388-391).
 __device__ __forceinline__ void contact_hvp_gather(const Dev& d, int vtx, double out[3]) {
-  (void)d; (void)vtx; out[0] = out[1] = out[2] = 0;
+  const Contact& c = d.c;
+  out[0] = out[1] = out[2] = 0;
+  for (uint32_t k = c.cOff[vtx]; k < c.cOff[vtx + 1]; k++) {
+    const uint32_t rec = c.cRec[k];
+    const double g = c.dd[rec >> 2];
+    if (g == 0) continue;
+    dist_grad_slot(c.active[rec >> 2], rec & 3, g, out);
+  }
 }
 
 }  // namespace cs

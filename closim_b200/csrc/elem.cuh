@@ -8,6 +8,7 @@
 //   9x9 block src/physics/membrane-blocks.ts:21-98
 #pragma once
 #include "common.cuh"
+#include "jsmath.cuh"
 
 namespace cs {
 
@@ -194,7 +195,8 @@ __device__ __forceinline__ T dihedral4(const T* q) {
   const T l1 = js_hypot3(n1x, n1y, n1z) + T(1e-30);
   const T l2 = js_hypot3(n2x, n2y, n2z) + T(1e-30);
   const T cosT = js_min(T(1), js_max(T(-1), (n1x * n2x + n1y * n2y + n1z * n2z) / (l1 * l2)));
-  return acos(cosT);
+  if constexpr (sizeof(T) == 8) return js_acos(cosT);
+  else return acosf(cosT);
 }
 
 // W = 0.5 k (theta - theta0)^2 edgeLen^2 / max(areaSum, 1e-12).

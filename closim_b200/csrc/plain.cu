@@ -19,6 +19,21 @@ __device__ __forceinline__ void load3(const double* x, int v, double o[3]) {
   o[0] = x[v * 3]; o[1] = x[v * 3 + 1]; o[2] = x[v * 3 + 2];
 }
 
+// s0 + t[0] + t[1] + ... evaluated left to right by one thread: the
+// reference's `for (i...) s += t[i]` accumulation, rounding for rounding.
+__device__ __forceinline__ double seq_chain(const double* t, int n, double s = 0.0) {
+  int i = 0;
+  for (; i + 4 <= n; i += 4) {
+    const double a0 = t[i], a1 = t[i + 1], a2 = t[i + 2], a3 = t[i + 3];
+    s = s + a0;
+    s = s + a1;
+    s = s + a2;
+    s = s + a3;
+  }
+  for (; i < n; i++) s = s + t[i];
+  return s;
+}
+
 // ---- predictor (newton.ts:41-50) -------------------------------------------
 __global__ void k_predict(Dev d) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -77,9 +92,7 @@ __global__ void __launch_bounds__(kThreads) k_hinge_grad(Dev d) {
 
 // g = M (x - yHat) / h^2 + gradE (+ contact grad), pin filter, partial |g|^2.
 __global__ void __launch_bounds__(kThreads) k_gather_grad(Dev d) {
-  __shared__ double sm[32];
   const int v = blockIdx.x * blockDim.x + threadIdx.x;
-  double gg = 0;
   if (v < d.n) {
     double s[3] = {0, 0, 0};
     for (uint32_t k = d.memOff[v]; k < d.memOff[v + 1]; k++) {
@@ -102,68 +115,67 @@ __global__ void __launch_bounds__(kThreads) k_gather_grad(Dev d) {
       if (d.hasContact) gi += d.cgrad[i];
       if (pin) gi = 0;
       d.g[i] = gi;
-      gg += gi * gi;
+      d.T0[i] = gi * gi;
     }
   }
-  const double bs = block_sum(gg, sm);
-  if (threadIdx.x == 0) d.part[1 * d.partStride + blockIdx.x] = bs;
 }
 
-// Final reduction of the gradient pass: sqrt(sum g^2), max strain.
-__global__ void k_grad_final(Dev d, int nbT, int nbV) {
+// Final reduction of the gradient pass: sqrt(sum g^2) in index order
+// (newton.ts:128), max strain (order-free).
+__global__ void k_grad_final(Dev d, int nbT) {
   if (threadIdx.x >= 32) return;
-  const double gs = warp_sum_partials(d.part + 1 * d.partStride, nbV);
   const double ms = warp_max_partials(d.part + 0 * d.partStride, nbT);
   if (threadIdx.x == 0) {
-    d.scal[S_GRADNORM] = sqrt(gs);
+    d.scal[S_GRADNORM] = sqrt(seq_chain(d.T0, d.n * 3));
     d.scal[S_MAXSTRAIN] = ms;
   }
 }
 
 // ---- total energy (newton.ts:76-88; fem.ts:56-75) ------------------------------
+// Per-element energy terms: inertia 0.5 m d^2 / h^2 per dof into T0, triangle
+// energies then hinge energies into T1 (the order internalEnergyOnly adds them).
 __global__ void __launch_bounds__(kThreads) k_energy(Dev d, const double* x) {
-  __shared__ double sm[32];
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  double ei = 0, et = 0, eh = 0;
   if (i < d.n) {
     const double m = d.mass[i];
 #pragma unroll
     for (int k = 0; k < 3; k++) {
       const double dd = x[i * 3 + k] - d.yHat[i * 3 + k];
-      ei += 0.5 * m * dd * dd / (d.h * d.h);
+      d.T0[i * 3 + k] = 0.5 * m * dd * dd / (d.h * d.h);
     }
   }
   if (i < d.m) {
     double p0[3], p1[3], p2[3];
     load3(x, d.idx[i * 3], p0); load3(x, d.idx[i * 3 + 1], p1); load3(x, d.idx[i * 3 + 2], p2);
     const float4 iv = d.inv[i];
-    et = tri_energy<double>(p0, p1, p2, iv.x, iv.y, iv.z, iv.w, d.area[i], d.mat);
+    d.T1[i] = tri_energy<double>(p0, p1, p2, iv.x, iv.y, iv.z, iv.w, d.area[i], d.mat);
   }
   if (i < d.hg && d.kb > 0) {
     const int4 hv = d.hinge[i];
     double q[12];
     load3(x, hv.x, q); load3(x, hv.y, q + 3); load3(x, hv.z, q + 6); load3(x, hv.w, q + 9);
-    eh = hinge_energy4(q, d.hmeta[i * 3], d.hmeta[i * 3 + 1], d.hmeta[i * 3 + 2], d.kb);
-  }
-  const double bi = block_sum(ei, sm), bt = block_sum(et, sm), bh = block_sum(eh, sm);
-  if (threadIdx.x == 0) {
-    d.part[2 * d.partStride + blockIdx.x] = bi;
-    d.part[3 * d.partStride + blockIdx.x] = bt;
-    d.part[4 * d.partStride + blockIdx.x] = bh;
+    d.T1[d.m + i] = hinge_energy4(q, d.hmeta[i * 3], d.hmeta[i * 3 + 1], d.hmeta[i * 3 + 2], d.kb);
   }
 }
 
-__global__ void k_energy_final(Dev d, int nb) {
-  if (threadIdx.x >= 32) return;
-  const double ei = warp_sum_partials(d.part + 2 * d.partStride, nb);
-  const double et = warp_sum_partials(d.part + 3 * d.partStride, nb);
-  const double eh = warp_sum_partials(d.part + 4 * d.partStride, nb);
-  const double em = d.hasContact ? d.scal[S_E_MERIT] : 0.0;
+// totalEnergy (newton.ts:76-88): ((sum inertia) + internal) + merit, each sum a
+// left-to-right chain; the three chains run on three warps.
+__global__ void k_energy_final(Dev d, int nMerit) {
+  __shared__ double part[3];
+  const int w = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0) {
+    if (w == 0) part[0] = seq_chain(d.T0, d.n * 3);
+    if (w == 1) part[1] = seq_chain(d.T1, d.m + (d.kb > 0 ? d.hg : 0));
+    if (w == 2) part[2] = d.hasContact ? seq_chain(d.Tc, nMerit) : 0.0;
+  }
+  __syncthreads();
   if (threadIdx.x == 0) {
-    d.scal[S_E_INERTIA] = ei;
-    d.scal[S_E_TRI] = et;
-    d.scal[S_E_HINGE] = eh;
-    d.scal[S_ENERGY_TRIAL] = ei + (et + eh) + em;
+    d.scal[S_E_INERTIA] = part[0];
+    d.scal[S_E_TRI] = part[1];
+    d.scal[S_E_MERIT] = part[2];
+    double e = part[0] + part[1];
+    if (d.hasContact) e += part[2];
+    d.scal[S_ENERGY_TRIAL] = e;
   }
 }
 
@@ -286,17 +298,16 @@ __device__ double schwarz_apply_domain(const Dev& d, int dom) {
       sol[i] = s;
     }
   }
-  double rz = 0;
   for (int l = 0; l < dv; l++) {
     const int v = d.domVerts[start + l];
     const bool pin = d.pinned[v];
     for (int k = 0; k < 3; k++) {
       const double zz = pin ? 0.0 : 0.0 + sol[l * 3 + k];
       d.z[v * 3 + k] = zz;
-      rz += d.r[v * 3 + k] * zz;
+      d.T2[v * 3 + k] = d.r[v * 3 + k] * zz;
     }
   }
-  return rz;
+  return 0.0;
 }
 
 // ---- PCG as one cooperative kernel (pcg.ts:11-95 + newton.ts:148-179) ----------
@@ -361,6 +372,17 @@ __device__ __forceinline__ double block_max_nonan(double v, double* sm) {
   return r;
 }
 
+// One thread per chain computes the chained sums after a grid barrier;
+// results land in scal[S_CH0 + w]. Up to 4 chains, one per warp of block 0.
+__device__ __forceinline__ void run_chains(const Dev& d, int nch, const double* a0, const double* a1,
+                                           const double* a2, int n) {
+  if (blockIdx.x == 0 && (threadIdx.x & 31) == 0) {
+    const int w = threadIdx.x >> 5;
+    const double* a = w == 0 ? a0 : w == 1 ? a1 : a2;
+    if (w < nch) d.scal[S_CH0 + w] = seq_chain(a, n);
+  }
+}
+
 __global__ void __launch_bounds__(kThreads) k_pcg(PcgArgs A) {
   cg::grid_group grid = cg::this_grid();
   __shared__ double sm[32];
@@ -369,51 +391,47 @@ __global__ void __launch_bounds__(kThreads) k_pcg(PcgArgs A) {
   const int n3 = d.n * 3;
   const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
   const bool jacobi = d.precond == 0;
-  // Row use per iteration: 0 |p|^2, 1 pAp, 2 |r|^2, 3 r.z ; 4-6 init ; 4-5 post.
-  double rzp = 0, bbp = 0, rrp = 0;
+  // ---- init: r = filter(b), z = M^-1 r, p = z (pcg.ts:27-55) ----
   for (int i = tid; i < n3; i += nth) {
     const double bi = -d.g[i];
-    bbp += bi * bi;
+    d.T0[i] = bi * bi;
     const double ri = d.pinned[i / 3] ? 0.0 : bi;
     d.r[i] = ri;
     d.dx[i] = 0;
-    rrp += ri * ri;
+    d.T1[i] = ri * ri;
     if (jacobi) {
       double zi = d.diag[i] > 1e-12 ? ri / d.diag[i] : ri;
       if (d.pinned[i / 3]) zi = 0;
       d.z[i] = zi;
       d.p[i] = zi;
-      rzp += ri * zi;
+      d.T2[i] = ri * zi;
     }
   }
-  put_partial(d, 5, bbp, sm);
-  put_partial(d, 6, rrp, sm);
-  if (jacobi) put_partial(d, 4, rzp, sm);
   grid.sync();
   if (!jacobi) {
-    rzp = 0;
-    for (int dom = tid; dom < d.D; dom += nth) rzp += schwarz_apply_domain(d, dom);
-    put_partial(d, 4, rzp, sm);
+    for (int dom = tid; dom < d.D; dom += nth) schwarz_apply_domain(d, dom);
     grid.sync();
     for (int i = tid; i < n3; i += nth) d.p[i] = d.z[i];
   }
-  double rz = get_total(d, 4, bc);
-  const double bNorm = sqrt(get_total(d, 5, bc));
+  // chains: rz (T2), |b|^2 (T0), |r|^2 (T1)
+  run_chains(d, 3, d.T2, d.T0, d.T1, n3);
+  grid.sync();
+  double rz = d.scal[S_CH0];
+  const double bNorm = sqrt(d.scal[S_CH1]);
   const double absTol = js_max(A.tol * js_max(bNorm, 1e-12), 1e-12);
-  double residual = sqrt(get_total(d, 6, bc));
+  double residual = sqrt(d.scal[S_CH2]);
   int iters = 0;
   bool done = residual < absTol;
-  // |p|^2 for the first FD step size.
   if (!done) {
-    double pp = 0;
-    for (int i = tid; i < n3; i += nth) pp += d.p[i] * d.p[i];
-    put_partial(d, 0, pp, sm);
+    for (int i = tid; i < n3; i += nth) d.T3[i] = d.p[i] * d.p[i];
+    grid.sync();
+    if (blockIdx.x == 0 && threadIdx.x == 0) d.scal[S_CH3] = seq_chain(d.T3, n3);
     grid.sync();
   }
   int k = 0;
   for (; !done && k < A.maxIters; k++) {
-    // --- HVP: membraneHvp (fem.ts:108-130) + inertia + contact ---
-    const double pNorm = sqrt(get_total(d, 0, bc));
+    // ---- Ap = M/h^2 p + membraneHvp (fem.ts:108-130) + contact HVP ----
+    const double pNorm = sqrt(d.scal[S_CH3]);
     const double h = 1e-8 * (1 + pNorm);
     for (int t = tid; t < d.m; t += nth) {
       const uint32_t vi[3] = {d.idx[t * 3], d.idx[t * 3 + 1], d.idx[t * 3 + 2]};
@@ -437,7 +455,6 @@ __global__ void __launch_bounds__(kThreads) k_pcg(PcgArgs A) {
     }
     if (d.hasContact) contact_hvp_coeffs(d, d.p, tid, nth);
     grid.sync();
-    double pAp = 0;
     for (int v = tid; v < d.n; v += nth) {
       double sp[3] = {0, 0, 0}, sn[3] = {0, 0, 0};
       for (uint32_t q = d.memOff[v]; q < d.memOff[v + 1]; q++) {
@@ -458,15 +475,15 @@ __global__ void __launch_bounds__(kThreads) k_pcg(PcgArgs A) {
         if (d.hasContact) ap += ch[c];
         if (pin) ap = 0;
         d.Ap[i] = ap;
-        pAp += d.p[i] * ap;
+        d.T0[i] = d.p[i] * ap;
       }
     }
-    put_partial(d, 1, pAp, sm);
     grid.sync();
-    const double pApT = get_total(d, 1, bc);
-    if (!(pApT > 1e-30)) { iters = k; done = true; break; }
-    const double alpha = rz / pApT;
-    double rr = 0, rzn = 0;
+    if (blockIdx.x == 0 && threadIdx.x == 0) d.scal[S_CH1] = seq_chain(d.T0, n3);
+    grid.sync();
+    const double pAp = d.scal[S_CH1];
+    if (!(pAp > 1e-30)) { iters = k; done = true; break; }
+    const double alpha = rz / pAp;
     for (int i = tid; i < n3; i += nth) {
       const bool pin = d.pinned[i / 3];
       double xi = d.dx[i] + alpha * d.p[i];
@@ -474,57 +491,57 @@ __global__ void __launch_bounds__(kThreads) k_pcg(PcgArgs A) {
       if (pin) { xi = 0; ri = 0; }
       d.dx[i] = xi;
       d.r[i] = ri;
-      rr += ri * ri;
+      d.T1[i] = ri * ri;
       if (jacobi) {
         double zi = d.diag[i] > 1e-12 ? ri / d.diag[i] : ri;
         if (pin) zi = 0;
         d.z[i] = zi;
-        rzn += ri * zi;
+        d.T2[i] = ri * zi;
       }
     }
-    put_partial(d, 2, rr, sm);
-    if (jacobi) put_partial(d, 3, rzn, sm);
     grid.sync();
-    residual = sqrt(get_total(d, 2, bc));
+    run_chains(d, jacobi ? 2 : 1, d.T1, d.T2, d.T2, n3);  // |r|^2 -> CH0, r.z -> CH1
+    grid.sync();
+    residual = sqrt(d.scal[S_CH0]);
     if (residual < absTol) { iters = k + 1; done = true; break; }
     if (!jacobi) {
-      rzn = 0;
-      for (int dom = tid; dom < d.D; dom += nth) rzn += schwarz_apply_domain(d, dom);
-      put_partial(d, 3, rzn, sm);
+      for (int dom = tid; dom < d.D; dom += nth) schwarz_apply_domain(d, dom);
+      grid.sync();
+      if (blockIdx.x == 0 && threadIdx.x == 0) d.scal[S_CH1] = seq_chain(d.T2, n3);
       grid.sync();
     }
-    const double rzNew = get_total(d, 3, bc);
+    const double rzNew = d.scal[S_CH1];
     const double beta = rzNew / rz;
-    double pp = 0;
     for (int i = tid; i < n3; i += nth) {
       const double pi = d.z[i] + beta * d.p[i];
       d.p[i] = pi;
-      pp += pi * pi;
+      d.T3[i] = pi * pi;
     }
     rz = rzNew;
-    put_partial(d, 0, pp, sm);
+    grid.sync();
+    if (blockIdx.x == 0 && threadIdx.x == 0) d.scal[S_CH3] = seq_chain(d.T3, n3);
     grid.sync();
   }
   if (!done) iters = A.maxIters;
-  // --- descent safeguard + trust region (newton.ts:152-179) ---
+  // ---- descent safeguard + trust region (newton.ts:152-179) ----
   grid.sync();
-  double gt = 0;
-  for (int i = tid; i < n3; i += nth) gt += d.g[i] * d.dx[i];
-  put_partial(d, 4, gt, sm);
+  for (int i = tid; i < n3; i += nth) d.T0[i] = d.g[i] * d.dx[i];
   grid.sync();
-  double gtdx = get_total(d, 4, bc);
+  if (blockIdx.x == 0 && threadIdx.x == 0) d.scal[S_CH2] = seq_chain(d.T0, n3);
+  grid.sync();
+  double gtdx = d.scal[S_CH2];
   bool fallback = false;
   if (!isfinite(gtdx) || gtdx >= 0) {
     fallback = true;
-    gt = 0;
     for (int i = tid; i < n3; i += nth) {
       const double di = -d.g[i] / d.diag[i];
       d.dx[i] = di;
-      gt += d.g[i] * di;
+      d.T1[i] = d.g[i] * di;
     }
-    put_partial(d, 5, gt, sm);
     grid.sync();
-    gtdx = get_total(d, 5, bc);
+    if (blockIdx.x == 0 && threadIdx.x == 0) d.scal[S_CH3] = seq_chain(d.T1, n3);
+    grid.sync();
+    gtdx = d.scal[S_CH3];
   }
   double mx = 0;
   for (int i = tid; i < n3; i += nth) {
@@ -577,12 +594,12 @@ void launch_grad(const Dev& d, cudaStream_t s) {
   k_tri_grad<<<nblk(d.m), kThreads, 0, s>>>(d);
   if (d.kb > 0 && d.hg > 0) k_hinge_grad<<<nblk(d.hg), kThreads, 0, s>>>(d);
   k_gather_grad<<<nblk(d.n), kThreads, 0, s>>>(d);
-  k_grad_final<<<1, 32, 0, s>>>(d, nblk(d.m), nblk(d.n));
+  k_grad_final<<<1, 32, 0, s>>>(d, nblk(d.m));
 }
 void launch_energy(const Dev& d, const double* x, cudaStream_t s) {
   const int nb = nblk(std::max(std::max(d.n, d.m), d.hg));
   k_energy<<<nb, kThreads, 0, s>>>(d, x);
-  k_energy_final<<<1, 32, 0, s>>>(d, nb);
+  k_energy_final<<<1, 96, 0, s>>>(d, d.hasContact ? d.c.nActive : 0);
 }
 void launch_diag_init(const Dev& d, double beta, cudaStream_t s) {
   k_diag_init<<<nblk(d.n * 3), kThreads, 0, s>>>(d, beta);

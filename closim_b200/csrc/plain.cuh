@@ -12,10 +12,29 @@ namespace cs {
 enum ScalarSlot {
   S_GRADNORM = 0, S_MAXSTRAIN, S_ENERGY_TRIAL, S_GTDX, S_PCG_ITERS, S_PCG_RES, S_E_INERTIA,
   S_E_TRI, S_E_HINGE, S_E_MERIT, S_FALLBACK, S_MAXDX, S_VALID, S_MINDIST, S_MINTOI, S_CCDFAIL,
-  S_BARRIER_E, S_FWORK, S_NSCALARS = 32
+  S_BARRIER_E, S_FWORK, S_CH0 = 24, S_CH1, S_CH2, S_CH3, S_NSCALARS = 32
 };
 
-struct Contact;  // contact.cuh
+// One frozen contact (contact-assembly.ts:22-30): kind 0 VT, 1 EE, 2 floor.
+// Ids < 0 other than -1 are static vertices -(i + 2).
+struct Frozen {
+  int kind, p, a, b, c, d;
+  double w0, w1, w2, w3, nx, ny, nz;
+};
+
+// Frozen active set and its per-vertex gather structure, as seen by kernels.
+struct Contact {
+  double dHat, kappa, dMin, mu, eps, floorY;
+  int hasFloor;
+  int ns;                  // static vertices
+  const float* spos;       // 3 ns
+  int nActive;             // active records (VT/EE first, then floor)
+  const Frozen* active;
+  double* dd;              // per-contact scalar (HVP coefficient, diag curvature, ...)
+  double* cg;              // 4 per contact: barrier dE/dd, friction force args (-f)
+  const uint32_t* cOff;    // n+1: vertex -> records (contact << 2 | slot), contact order
+  const uint32_t* cRec;
+};
 
 // Everything a kernel of the FP64 path needs, passed by value.
 struct Dev {
@@ -42,6 +61,10 @@ struct Dev {
   double* helem;           // 12hg
   double* part;            // partial sums: NPART rows x maxBlocks
   int partStride;
+  // Per-element terms of the reductions. The FP64 path adds them one by one in
+  // index order (the reference's sequential loops), one thread per chain.
+  double *T0, *T1, *T2, *T3; // max(3n, m + hg) each
+  double* Tc;              // per-contact terms (contact capacity)
   double* scal;            // S_NSCALARS
   // material
   Mat<double> mat;
@@ -56,8 +79,8 @@ struct Dev {
   double* L;               // D x 576 (24x24 row-major), Cholesky or inverse diagonal
   uint8_t* domFlag;        // D
   int precond;             // 0 Jacobi, 1 Schwarz
-  Contact* contact;        // device pointer to contact data, or nullptr
   int hasContact;
+  Contact c;               // valid when hasContact
 };
 
 constexpr int kThreads = 256;

@@ -1,0 +1,139 @@
+// Stable LSD radix sort of (key, payload) records on the device, hand-written.
+//
+// Keys are KW 32-bit words, most significant word first (word 0); each pass
+// sorts one 8-bit digit: a per-tile histogram, one exclusive scan over
+// (digit, tile), then a stable scatter in which each tile ranks its elements
+// with warp match + per-warp digit counters. Passes run from the least
+// significant digit up, so equal keys keep their input order (a stable sort,
+// which is what makes the (key, index) orders of the reference reproducible).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace cs {
+
+constexpr int kSortThreads = 256;
+constexpr int kSortItems = 8;                        // rows per tile
+constexpr int kSortTile = kSortThreads * kSortItems;  // 2048 elements
+
+template <int KW>
+struct Key {
+  uint32_t w[KW];
+};
+
+template <int KW>
+__device__ __forceinline__ uint32_t digit_of(const Key<KW>& k, int pass) {
+  // pass 0 = least significant byte of the last word
+  const int word = KW - 1 - pass / 4;
+  return (k.w[word] >> ((pass % 4) * 8)) & 0xffu;
+}
+
+template <int KW>
+__global__ void __launch_bounds__(kSortThreads) k_radix_hist(const Key<KW>* keys, int n, int pass, uint32_t* hist,
+                                                             int ntiles) {
+  __shared__ uint32_t h[256];
+  h[threadIdx.x] = 0;
+  __syncthreads();
+  const int base = blockIdx.x * kSortTile;
+  for (int r = 0; r < kSortItems; r++) {
+    const int i = base + r * kSortThreads + threadIdx.x;
+    if (i < n) atomicAdd(&h[digit_of(keys[i], pass)], 1u);
+  }
+  __syncthreads();
+  hist[threadIdx.x * ntiles + blockIdx.x] = h[threadIdx.x];
+}
+
+// Exclusive scan of `n` u32 in place by one block (chunked, running carry).
+__global__ void __launch_bounds__(1024) k_scan_exclusive(uint32_t* a, int n, uint32_t* total) {
+  __shared__ uint32_t s[1024];
+  __shared__ uint32_t carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (int base = 0; base < n; base += 1024) {
+    const int i = base + threadIdx.x;
+    const uint32_t v = i < n ? a[i] : 0;
+    s[threadIdx.x] = v;
+    __syncthreads();
+    for (int off = 1; off < 1024; off <<= 1) {
+      const uint32_t t = threadIdx.x >= off ? s[threadIdx.x - off] : 0;
+      __syncthreads();
+      s[threadIdx.x] += t;
+      __syncthreads();
+    }
+    if (i < n) a[i] = carry + s[threadIdx.x] - v;
+    __syncthreads();
+    if (threadIdx.x == 1023) carry += s[1023];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0 && total) *total = carry;
+}
+
+template <int KW>
+__global__ void __launch_bounds__(kSortThreads) k_radix_scatter(const Key<KW>* kin, const uint32_t* pin, Key<KW>* kout,
+                                                                uint32_t* pout, int n, int pass, const uint32_t* offs,
+                                                                int ntiles) {
+  __shared__ uint32_t running[256];
+  __shared__ uint32_t wcount[kSortThreads / 32][256];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  running[threadIdx.x] = offs[threadIdx.x * ntiles + blockIdx.x];
+  for (int w = 0; w < kSortThreads / 32; w++) wcount[w][threadIdx.x] = 0;
+  __syncthreads();
+  const int base = blockIdx.x * kSortTile;
+  const uint32_t lt = (1u << lane) - 1u;
+  for (int r = 0; r < kSortItems; r++) {
+    const int i = base + r * kSortThreads + threadIdx.x;
+    const bool valid = i < n;
+    Key<KW> k;
+    uint32_t pl = 0;
+    int dg = -1;
+    if (valid) {
+      k = kin[i];
+      pl = pin[i];
+      dg = (int)digit_of(k, pass);
+    }
+    const uint32_t peers = __match_any_sync(0xffffffffu, dg);
+    const uint32_t rank = __popc(peers & lt);
+    if (valid && rank == 0) wcount[warp][dg] = __popc(peers);
+    __syncthreads();
+    if (valid) {
+      uint32_t off = running[dg] + rank;
+      for (int w = 0; w < warp; w++) off += wcount[w][dg];
+      kout[off] = k;
+      pout[off] = pl;
+    }
+    __syncthreads();
+    uint32_t tot = 0;
+    for (int w = 0; w < kSortThreads / 32; w++) {
+      tot += wcount[w][threadIdx.x];
+      wcount[w][threadIdx.x] = 0;
+    }
+    running[threadIdx.x] += tot;
+    __syncthreads();
+  }
+}
+
+// Sorts n records by key over the low `bits` bits of the key (counted from the
+// least significant end). Ping-pongs between (k0,p0) and (k1,p1); returns true
+// when the result ended in (k1,p1). hist must hold 256 * ceil(n / 2048) + 1 u32.
+template <int KW>
+bool radix_sort(Key<KW>* k0, uint32_t* p0, Key<KW>* k1, uint32_t* p1, int n, int bits, uint32_t* hist,
+                cudaStream_t s, int64_t* launches) {
+  if (n <= 1) return false;
+  const int ntiles = (n + kSortTile - 1) / kSortTile;
+  const int passes = (bits + 7) / 8;
+  bool flip = false;
+  for (int pass = 0; pass < passes; pass++) {
+    const Key<KW>* ki = flip ? k1 : k0;
+    const uint32_t* pi = flip ? p1 : p0;
+    Key<KW>* ko = flip ? k0 : k1;
+    uint32_t* po = flip ? p0 : p1;
+    k_radix_hist<KW><<<ntiles, kSortThreads, 0, s>>>(ki, n, pass, hist, ntiles);
+    k_scan_exclusive<<<1, 1024, 0, s>>>(hist, 256 * ntiles, nullptr);
+    k_radix_scatter<KW><<<ntiles, kSortThreads, 0, s>>>(ki, pi, ko, po, n, pass, hist, ntiles);
+    if (launches) *launches += 3;
+    flip = !flip;
+  }
+  return flip;
+}
+
+}  // namespace cs

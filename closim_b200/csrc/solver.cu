@@ -87,6 +87,7 @@ class Solver {
   DBuf<int> pinIdsD, domStart, domVerts, v2tOff, v2t;
   DBuf<double> pinPosD;
   DBuf<double> vx, vv, vx0, vyHat, vg, vdiag, vdx, vr, vz, vp, vAp, vxt, vcgrad, vcHp, elem, helem, part, scal, L;
+  DBuf<double> T0, T1, T2, T3, Tc;
   DBuf<uint8_t> domFlag;
   double* hscal = nullptr;  // pinned host mirror of scal
   int pcgBlocks = 1;
@@ -193,6 +194,9 @@ class Solver {
       b->alloc(n3);
     CK(cudaMemsetAsync(vcgrad.p, 0, n3 * 8, stream));
     CK(cudaMemsetAsync(vcHp.p, 0, n3 * 8, stream));
+    const size_t tcap = std::max(n3, (size_t)cm.m + (size_t)cm.hg);
+    for (DBuf<double>* b : {&T0, &T1, &T2, &T3}) b->alloc(tcap);
+    Tc.alloc(1);
     elem.alloc(std::max<size_t>((size_t)cm.m * 18, 1));
     helem.alloc(std::max<size_t>((size_t)cm.hg * 12, 1));
     const int partStride = (int)((std::max(std::max(n3, (size_t)cm.m), (size_t)cm.hg) + kThreads - 1) / kThreads) + 1;
@@ -214,6 +218,7 @@ class Solver {
     d.elem = elem.p; d.helem = helem.p; d.part = part.p; d.partStride = partStride; d.scal = scal.p;
     d.D = mesh.D; d.domStart = domStart.p; d.domVerts = domVerts.p; d.v2tOff = v2tOff.p; d.v2t = v2t.p;
     d.L = L.p; d.domFlag = domFlag.p;
+    d.T0 = T0.p; d.T1 = T1.p; d.T2 = T2.p; d.T3 = T3.p; d.Tc = Tc.p;
     set_material(m);
     for (int k = 0; k < 3; k++) d.gravity[k] = gravity[k];
     pcgBlocks = pcg_grid_blocks(d);

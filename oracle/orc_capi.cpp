@@ -336,3 +336,10 @@ void orc_lbvh_arrays(void* h, float* aabb, float* centroid, uint32_t* morton, ui
 }
 
 }  // extern "C"
+
+#include "jsmath.hpp"
+extern "C" {
+double orc_js_acos(double x) { return orc::js_acos(x); }
+double orc_js_log(double x) { return orc::js_log(x); }
+double orc_js_cbrt(double x) { return orc::js_cbrt(x); }
+}

@@ -4,6 +4,7 @@
 #include <array>
 
 #include "orc.hpp"
+#include "jsmath.hpp"
 
 namespace orc {
 
@@ -120,17 +121,17 @@ std::vector<double> solve_cubic01(double a3, double a2, double a1, double a0) {
   const double shift = A / 3;
   if (disc > eps) {
     const double sd = std::sqrt(disc);
-    const double u = std::cbrt(-q / 2 + sd);
-    const double v = std::cbrt(-q / 2 - sd);
+    const double u = js_cbrt(-q / 2 + sd);
+    const double v = js_cbrt(-q / 2 - sd);
     roots.push_back(u + v - shift);
   } else if (std::fabs(disc) <= eps) {
-    const double u = std::cbrt(-q / 2);
+    const double u = js_cbrt(-q / 2);
     roots.push_back(2 * u - shift);
     roots.push_back(-u - shift);
   } else {
     const double r = std::sqrt(-(p * p * p) / 27);
-    const double phi = std::acos(js_min(1, js_max(-1, -q / (2 * r))));
-    const double s = 2 * std::cbrt(r);
+    const double phi = js_acos(js_min(1, js_max(-1, -q / (2 * r))));
+    const double s = 2 * js_cbrt(r);
     const double PI = 3.141592653589793;
     roots.push_back(s * std::cos(phi / 3) - shift);
     roots.push_back(s * std::cos((phi + 2 * PI) / 3) - shift);
@@ -286,13 +287,13 @@ double barrier_value(double d, double dHat) {
   if (d >= dHat) return 0;
   const double dc = js_max(d, 1e-12);
   const double t = dc - dHat;
-  return -t * t * std::log(dc / dHat);
+  return -t * t * js_log(dc / dHat);
 }
 double barrier_grad_scalar(double d, double dHat, double kappa, double w) {
   if (d >= dHat) return 0;
   const double dc = js_max(d, 1e-12);
   const double t = dc - dHat;
-  const double db = -2 * t * std::log(dc / dHat) - (t * t) / dc;
+  const double db = -2 * t * js_log(dc / dHat) - (t * t) / dc;
   return kappa * w * db;
 }
 double barrier_normal_force(double d, double dHat, double kappa, double w) {
@@ -759,7 +760,7 @@ void ContactSystem::apply_hvp(const double* x, const double* v, double* out, int
     const Frozen& c = active[i];
     const double d = js_max(frozen_dist(x, c), 1e-12);
     if (d >= dHat) { dd[i] = 0; continue; }
-    const double L = std::log(d / dHat);
+    const double L = js_log(d / dHat);
     const double u = d - dHat;
     const double b2 = -(2 * L + (4 * u) / d - (u * u) / (d * d));
     const double coeff = kappa * js_max(b2, 0);
@@ -789,7 +790,7 @@ void ContactSystem::add_diag_estimate(double* dg, const double* x) {
   for (const Frozen& c : active) {
     const double d = js_max(frozen_dist(x, c), 1e-12);
     if (d >= dHat) continue;
-    const double L = std::log(d / dHat);
+    const double L = js_log(d / dHat);
     const double u = d - dHat;
     const double b2 = js_max(-(2 * L + (4 * u) / d - (u * u) / (d * d)), 0);
     const double k = kappa * b2;

@@ -10,6 +10,7 @@
 #include <unordered_map>
 
 #include "orc.hpp"
+#include "jsmath.hpp"
 
 namespace orc {
 
@@ -55,7 +56,7 @@ double dihedral(const T* x, int v0, int v1, int v2, int v3) {
   double l1 = js_hypot3(n1x, n1y, n1z) + 1e-30;
   double l2 = js_hypot3(n2x, n2y, n2z) + 1e-30;
   double cosT = js_min(1, js_max(-1, (n1x * n2x + n1y * n2y + n1z * n2z) / (l1 * l2)));
-  return std::acos(cosT);
+  return js_acos(cosT);
 }
 template double dihedral<float>(const float*, int, int, int, int);
 template double dihedral<double>(const double*, int, int, int, int);
