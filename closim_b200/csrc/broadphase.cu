@@ -236,7 +236,9 @@ __global__ void k_self(BvhBufs b, const uint32_t* sp, bool mirror) {
   int stack[kStack];
   int sp_ = 0;
   stack[sp_++] = *b.root;
+  long guard = 0;
   while (sp_ > 0) {
+    if (++guard > 4l * m + 8) { atomicOr(b.flags, 2); return; }
     const int node = stack[--sp_];
     const int ch[2] = {b.left[node], b.right[node]};
     for (int c = 0; c < 2; c++) {
@@ -295,7 +297,9 @@ __global__ void k_static(BvhBufs b, const uint32_t* sp, double pad, int2* outp) 
     // the root itself is tested too (queryBvhAll tests every popped node)
     if (!ov6(sb, b.nbox + (size_t)(*b.root) * 6)) sp_ = 0;
   }
+  long guard = 0;
   while (sp_ > 0) {
+    if (++guard > 4l * m + 8) { atomicOr(b.flags, 2); return; }
     const int node = stack[--sp_];
     const int ch[2] = {b.left[node], b.right[node]};
     for (int c = 0; c < 2; c++) {

@@ -1,19 +1,953 @@
-// ContactSystem on the device (reference src/collision/contact-assembly.ts).
+// ContactSystem on the device (reference src/collision/contact-assembly.ts),
+// FP64 path (compiled with -fmad=false).
+//
+// Per Newton iteration the frozen active set is rebuilt from the broadphase
+// candidates (sorted by (kind, p, a, b, c, d), contact-assembly.ts:118) and the
+// floor vertices; per-contact kernels evaluate the barrier, lagged friction,
+// frozen HVP and diagonal terms, and per-vertex kernels gather them through a
+// vertex -> (contact, slot) CSR built by a stable sort, so every vertex adds its
+// contact terms in active-list order as the reference's scatter does. Chained
+// sums (barrier energy, friction work, merit energy) are evaluated left to
+// right by one thread.
+#include <climits>
+
+#include "broadphase.cuh"
 #include "contact.cuh"
 #include "contact_host.hpp"
+#include "solver.hpp"
 
 namespace cs {
 
-void set_contact(Solver&, const cs_contact_params* p, int, double, const float*, int, const uint32_t*, int) {
-  if (p) throw std::invalid_argument("contact is not available in this build");
+constexpr int kCT = 256;
+static inline int cnb(long n) { return (int)((n + kCT - 1) / kCT); }
+
+struct CView {  // kernel view of the contact host buffers
+  Contact c;
+  int nCand, nFloor, n;
+  const double* x0;  // xStep
+  const int* srt;
+  uint32_t* cflag;
+  uint32_t* fflag;
+  double* cmin;
+  double* ctoi;
+  double* vtmp;
+  double* vtmp2;
+  Frozen* active;
+  double* dd;
+  double* cg;
+  double* tc;
+  double* tf;
+  double* lagFloor;
+  uint8_t* lagFloorOk;
+  const Key<6>* lagKeys;
+  const double4* lagVals;
+  int lagCount;
+  int* cint;
+  DevDiag* diag;
+};
+
+__device__ __forceinline__ double seq_sum(const double* t, int n) {
+  double s = 0.0;
+  for (int i = 0; i < n; i++) s = s + t[i];
+  return s;
 }
-void ContactHost::begin_step_and_bisect(Solver&) {}
-void ContactHost::update_active_set(Solver&, double*) {}
-void ContactHost::merit_energy(Solver&, const double*) {}
-void ContactHost::gradient_terms(Solver&) {}
-bool ContactHost::check_trial(Solver&, const double*) { return true; }
-void ContactHost::commit(Solver&, const double*) {}
-void ContactHost::kill_approach_velocity(Solver&) {}
-void ContactHost::fill_stats(Solver&, cs_step_stats&) {}
+
+__global__ void k_lerp(double* out, const double* x0, const double* x, double t, int n3) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n3) out[i] = x0[i] + t * (x[i] - x0[i]);
+}
+
+// ---- active set (contact-assembly.ts:164-220) -------------------------------------
+__device__ __forceinline__ void cand_closest(const CView& v, const double* x, const int* r, Closest& cp) {
+  double P[3], A[3], B[3], C[3];
+  if (r[0] == 0) {
+    cpos(v.c, x, r[1], P); cpos(v.c, x, r[2], A); cpos(v.c, x, r[3], B); cpos(v.c, x, r[4], C);
+    cp = closest_vt(P, A, B, C);
+  } else {
+    cpos(v.c, x, r[2], A); cpos(v.c, x, r[3], B); cpos(v.c, x, r[4], C); cpos(v.c, x, r[5], P);
+    cp = closest_ee(A, B, C, P);
+  }
+}
+
+__global__ void k_cand_flags(CView v, const double* x, int C) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= C) return;
+  const int* r = v.srt + (size_t)i * 6;
+  if (r[0] == 3) { v.cflag[i] = 0; v.cmin[i] = INFINITY; return; }
+  Closest cp;
+  cand_closest(v, x, r, cp);
+  const bool act = !(cp.dist >= v.c.dHat || cp.dist < 1e-12);
+  v.cflag[i] = act ? 1u : 0u;
+  v.cmin[i] = cp.dist;
+  if (act && r[0] == 0) atomicAdd(&v.cint[CI_NVT], 1);
+}
+
+__global__ void k_floor_flags(CView v, const double* x) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= v.n) return;
+  if (!v.c.hasFloor) { v.fflag[i] = 0; v.vtmp[i] = INFINITY; return; }
+  const double d = x[i * 3 + 1] - v.c.floorY;
+  v.vtmp[i] = d;
+  v.fflag[i] = d >= v.c.dHat ? 0u : 1u;
+}
+
+__global__ void k_cand_compact(CView v, const double* x, int C) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= C) return;
+  const int* r = v.srt + (size_t)i * 6;
+  if (r[0] == 3) return;
+  Closest cp;
+  cand_closest(v, x, r, cp);
+  if (cp.dist >= v.c.dHat || cp.dist < 1e-12) return;
+  Frozen f;
+  f.kind = r[0]; f.p = r[1]; f.a = r[2]; f.b = r[3]; f.c = r[4]; f.d = r[5];
+  f.nx = cp.rx / cp.dist; f.ny = cp.ry / cp.dist; f.nz = cp.rz / cp.dist;
+  if (r[0] == 0) {
+    f.d = -1;
+    f.w1 = cp.s; f.w2 = cp.t; f.w0 = 1 - cp.s - cp.t; f.w3 = 0;
+  } else {
+    f.p = -1;
+    f.w0 = 1 - cp.s; f.w1 = cp.s; f.w2 = -(1 - cp.t); f.w3 = -cp.t;
+  }
+  v.active[v.cflag[i]] = f;
+}
+
+__global__ void k_floor_compact(CView v, const double* x) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= v.n || !v.c.hasFloor) return;
+  const double d = x[i * 3 + 1] - v.c.floorY;
+  if (d >= v.c.dHat) return;
+  Frozen f;
+  f.kind = 2; f.p = i; f.a = f.b = f.c = f.d = -1;
+  f.w0 = f.w1 = f.w2 = f.w3 = 0;
+  f.nx = 0; f.ny = 1; f.nz = 0;
+  v.active[v.nCand + v.fflag[i]] = f;
+}
+
+// Minimum ignoring NaN (the reference's `if (d < minD) minD = d`) over two arrays.
+__device__ double block_min2(const double* a, int na, const double* b, int nb) {
+  __shared__ double sm[1024];
+  double m = INFINITY;
+  for (int i = threadIdx.x; i < na; i += blockDim.x) if (a[i] < m) m = a[i];
+  for (int i = threadIdx.x; i < nb; i += blockDim.x) if (b[i] < m) m = b[i];
+  sm[threadIdx.x] = m;
+  __syncthreads();
+  for (int off = blockDim.x / 2; off > 0; off >>= 1) {
+    if ((int)threadIdx.x < off && sm[threadIdx.x + off] < sm[threadIdx.x]) sm[threadIdx.x] = sm[threadIdx.x + off];
+    __syncthreads();
+  }
+  const double r = sm[0];
+  __syncthreads();
+  return r;
+}
+
+__global__ void __launch_bounds__(1024) k_active_min(CView v, int C, int nf) {
+  const double m = block_min2(v.cmin, C, v.vtmp, nf);
+  if (threadIdx.x == 0 && m < v.diag->minDistance) v.diag->minDistance = m;
+}
+
+// CSR records: one per (contact, slot) whose vertex is a cloth vertex.
+__global__ void k_csr_records(CView v, Key<1>* k, uint32_t* p, int na) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= na * 4) return;
+  const int c = i >> 2, slot = i & 3;
+  const Frozen f = v.active[c];
+  int vert = -1;
+  if (f.kind == 2) vert = slot == 0 ? f.p : -1;
+  else if (f.kind == 0) vert = slot == 0 ? f.p : slot == 1 ? f.a : slot == 2 ? f.b : f.c;
+  else vert = slot == 0 ? f.a : slot == 1 ? f.b : slot == 2 ? f.c : f.d;
+  k[i].w[0] = vert >= 0 ? (uint32_t)vert : 0xffffffffu;
+  p[i] = (uint32_t)i;
+}
+
+__global__ void k_csr_offsets(const Key<1>* k, int nrec, uint32_t* off, int n) {
+  const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v > n) return;
+  int lo = 0, hi = nrec;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (k[mid].w[0] < (uint32_t)v) lo = mid + 1;
+    else hi = mid;
+  }
+  off[v] = (uint32_t)lo;
+}
+
+// ---- barrier + lagged friction (contact-assembly.ts:262-285) -----------------------
+__device__ __forceinline__ void lag_key(const Frozen& f, int ns, Key<6>& k) {
+  const uint32_t off = (uint32_t)(ns + 2);
+  k.w[0] = (uint32_t)f.kind;
+  if (f.kind == 0) {
+    int t0 = f.a, t1 = f.b, t2 = f.c, tmp;
+    if (t1 < t0) { tmp = t0; t0 = t1; t1 = tmp; }
+    if (t2 < t1) { tmp = t1; t1 = t2; t2 = tmp; }
+    if (t1 < t0) { tmp = t0; t0 = t1; t1 = tmp; }
+    k.w[1] = (uint32_t)f.p + off; k.w[2] = (uint32_t)t0 + off; k.w[3] = (uint32_t)t1 + off;
+    k.w[4] = (uint32_t)t2 + off;
+  } else {
+    int e1a = min(f.a, f.b), e1b = max(f.a, f.b), e2a = min(f.c, f.d), e2b = max(f.c, f.d);
+    if (e2a < e1a || (e2a == e1a && e2b < e1b)) {
+      int t = e1a; e1a = e2a; e2a = t;
+      t = e1b; e1b = e2b; e2b = t;
+    }
+    k.w[1] = (uint32_t)e1a + off; k.w[2] = (uint32_t)e1b + off; k.w[3] = (uint32_t)e2a + off;
+    k.w[4] = (uint32_t)e2b + off;
+  }
+  k.w[5] = 0;
+}
+
+// Latest committed (n, lambdaN) for a VT/EE key; false when never committed.
+__device__ __forceinline__ bool lag_find(const CView& v, const Key<6>& k, double4& out) {
+  int lo = 0, hi = v.lagCount;  // first entry whose key words exceed k (seq ignored)
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    const Key<6>& e = v.lagKeys[mid];
+    bool le = true;
+    for (int w = 0; w < 5; w++) {
+      if (e.w[w] != k.w[w]) { le = e.w[w] < k.w[w]; break; }
+    }
+    if (le) lo = mid + 1;
+    else hi = mid;
+  }
+  if (lo == 0) return false;
+  const Key<6>& e = v.lagKeys[lo - 1];
+  for (int w = 0; w < 5; w++)
+    if (e.w[w] != k.w[w]) return false;
+  out = v.lagVals[lo - 1];
+  return true;
+}
+
+__device__ __forceinline__ void relative_slip(const CView& v, const double* x, const Frozen& f, double u[3]) {
+  auto D = [&](int q, double o[3]) {
+    if (q < 0) { o[0] = o[1] = o[2] = 0; return; }
+    o[0] = x[q * 3] - v.x0[q * 3]; o[1] = x[q * 3 + 1] - v.x0[q * 3 + 1]; o[2] = x[q * 3 + 2] - v.x0[q * 3 + 2];
+  };
+  if (f.kind == 2) { D(f.p, u); return; }
+  if (f.kind == 0) {
+    // the third triangle vertex reads D(c.d), a negative id (reference behaviour)
+    double dp[3], da[3], db[3], dc[3];
+    D(f.p, dp); D(f.a, da); D(f.b, db); D(f.d, dc);
+    for (int i = 0; i < 3; i++) u[i] = dp[i] - (f.w0 * da[i] + f.w1 * db[i] + f.w2 * dc[i]);
+    return;
+  }
+  double da[3], db[3], dc[3], dd[3];
+  D(f.a, da); D(f.b, db); D(f.c, dc); D(f.d, dd);
+  for (int i = 0; i < 3; i++) u[i] = f.w0 * da[i] + f.w1 * db[i] + f.w2 * dc[i] + f.w3 * dd[i];
+}
+
+// Per contact: active flag (dd), barrier dE/dd and friction args (cg), the
+// energy and friction-work chain terms (tc, tf).
+__global__ void k_contact_prep(CView v, const double* x, int na) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= na) return;
+  const Frozen f = v.active[i];
+  const Contact& c = v.c;
+  const double d = js_max(frozen_dist(c, x, f), 1e-12);
+  if (d >= c.dHat) {
+    v.dd[i] = 0; v.tc[i] = 0; v.tf[i] = 0;
+    return;
+  }
+  v.dd[i] = 1;
+  v.tc[i] = c.kappa * barrier_value(d, c.dHat);
+  const double g = barrier_grad_scalar(d, c.dHat, c.kappa, 1);
+  double nx = f.nx, ny = f.ny, nz = f.nz, lam;
+  bool has = false;
+  double4 lv;
+  if (f.kind == 2) {
+    if (v.lagFloorOk[f.p]) { has = true; lv = make_double4(0, 1, 0, v.lagFloor[f.p]); }
+  } else {
+    Key<6> k;
+    lag_key(f, c.ns, k);
+    has = lag_find(v, k, lv);
+  }
+  if (has) { nx = lv.x; ny = lv.y; nz = lv.z; lam = lv.w; }
+  else lam = barrier_normal_force(d, c.dHat, c.kappa, 1);
+  double u[3], fr[3];
+  relative_slip(v, x, f, u);
+  coulomb_force(u, nx, ny, nz, lam, c.mu, c.eps, fr);
+  v.cg[i * 4] = g;
+  v.cg[i * 4 + 1] = -fr[0];
+  v.cg[i * 4 + 2] = -fr[1];
+  v.cg[i * 4 + 3] = -fr[2];
+  v.tf[i] = fr[0] * u[0] + fr[1] * u[1] + fr[2] * u[2];
+}
+
+__global__ void k_contact_chains(CView v, int na) {
+  if (threadIdx.x == 0) v.diag->barrierEnergy = seq_sum(v.tc, na);
+  if (threadIdx.x == 32) v.diag->frictionWork = v.diag->frictionWork + seq_sum(v.tf, na);
+}
+
+__global__ void k_contact_grad_gather(CView v, double* cgrad) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= v.n) return;
+  double o[3] = {0, 0, 0};
+  for (uint32_t k = v.c.cOff[q]; k < v.c.cOff[q + 1]; k++) {
+    const uint32_t rec = v.c.cRec[k];
+    const int ci = rec >> 2, slot = rec & 3;
+    if (v.dd[ci] == 0) continue;
+    const Frozen f = v.active[ci];
+    dist_grad_slot(f, slot, v.cg[ci * 4], o);
+    friction_slot(f, slot, v.cg + ci * 4 + 1, o);
+  }
+  cgrad[q * 3] = o[0]; cgrad[q * 3 + 1] = o[1]; cgrad[q * 3 + 2] = o[2];
+}
+
+// addDiagEstimate (contact-assembly.ts:436-471): dd = kappa max(b'', 0).
+__global__ void k_contact_curv(CView v, const double* x, int na) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= na) return;
+  const double d = js_max(frozen_dist(v.c, x, v.active[i]), 1e-12);
+  v.dd[i] = d >= v.c.dHat ? 0.0 : barrier_curvature(d, v.c.dHat, v.c.kappa);
+}
+
+__global__ void k_contact_diag_gather(CView v, double* diag) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= v.n) return;
+  double o[3] = {diag[q * 3], diag[q * 3 + 1], diag[q * 3 + 2]};
+  for (uint32_t k = v.c.cOff[q]; k < v.c.cOff[q + 1]; k++) {
+    const uint32_t rec = v.c.cRec[k];
+    const int ci = rec >> 2, slot = rec & 3;
+    const double kk = v.dd[ci];
+    if (kk == 0) continue;
+    const Frozen f = v.active[ci];
+    if (f.kind == 2) { o[1] += kk; continue; }
+    const double n2[3] = {f.nx * f.nx, f.ny * f.ny, f.nz * f.nz};
+    if (f.kind == 0 && slot == 0) {
+      for (int a = 0; a < 3; a++) o[a] += kk * n2[a];
+      continue;
+    }
+    const double w = f.kind == 0 ? (slot == 1 ? f.w0 : slot == 2 ? f.w1 : f.w2)
+                                 : (slot == 0 ? f.w0 : slot == 1 ? f.w1 : slot == 2 ? f.w2 : f.w3);
+    for (int a = 0; a < 3; a++) o[a] += kk * w * w * n2[a];
+  }
+  diag[q * 3] = o[0]; diag[q * 3 + 1] = o[1]; diag[q * 3 + 2] = o[2];
+}
+
+// meritEnergy terms (contact-assembly.ts:419-428).
+__global__ void k_contact_merit(CView v, const double* x, int na) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= na) return;
+  const double d = js_max(frozen_dist(v.c, x, v.active[i]), 1e-12);
+  v.tc[i] = d >= v.c.dHat ? 0.0 : v.c.kappa * barrier_value(d, v.c.dHat);
+}
+
+// commit (contact-assembly.ts:475-485): floor multipliers in a per-vertex
+// table; VT/EE entries appended to the lag table (key, commit sequence).
+__global__ void k_contact_commit(CView v, const double* x, int na, Key<6>* lk, uint32_t* lp, double4* lval,
+                                 int base, int commitNo) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= na) return;
+  const Frozen f = v.active[i];
+  const double d = js_max(frozen_dist(v.c, x, f), 1e-12);
+  const bool ok = d < v.c.dHat;
+  const double lam = ok ? barrier_normal_force(d, v.c.dHat, v.c.kappa, 1) : 0.0;
+  if (f.kind == 2) {
+    if (ok) { v.lagFloor[f.p] = lam; v.lagFloorOk[f.p] = 1; }
+    return;
+  }
+  if (i >= v.nCand) return;
+  const int e = base + i;
+  Key<6> k;
+  if (ok) {
+    lag_key(f, v.c.ns, k);
+    k.w[5] = ((uint32_t)commitNo << 24) | (uint32_t)i;
+  } else {
+    for (int w = 0; w < 6; w++) k.w[w] = 0xffffffffu;
+  }
+  lk[e] = k;
+  lp[e] = (uint32_t)e;
+  lval[e] = make_double4(f.nx, f.ny, f.nz, lam);
+}
+
+__global__ void k_iota(uint32_t* p, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) p[i] = (uint32_t)i;
+}
+
+__global__ void k_gather_vals(const double4* src, const uint32_t* order, int n, double4* dst) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) dst[i] = src[order[i]];
+}
+
+// ---- trial validation (contact-assembly.ts:489-553) ----------------------------------
+__global__ void k_trial_reset(int* cint) {
+  cint[CI_FIRSTNF] = INT_MAX;
+  cint[CI_FIRSTBAD] = INT_MAX;
+  cint[CI_FLOORBAD] = 0;
+  cint[CI_VALID] = 0;
+}
+
+__global__ void k_trial_cand(CView v, const double* xt, int C, double dMin) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= C) return;
+  const int* r = v.srt + (size_t)i * 6;
+  v.cflag[i] = 0;
+  v.ctoi[i] = INFINITY;
+  if (r[0] == 3) { v.cmin[i] = INFINITY; return; }
+  Closest cp;
+  cand_closest(v, xt, r, cp);
+  v.cmin[i] = cp.dist;
+  if (!isfinite(cp.dist)) atomicMin(&v.cint[CI_FIRSTNF], i);
+  int ids[4];
+  if (r[0] == 0) {
+    if (r[1] < 0 && r[2] < 0) return;
+    ids[0] = r[1]; ids[1] = r[2]; ids[2] = r[3]; ids[3] = r[4];
+  } else {
+    if (r[2] < 0 && r[3] < 0 && r[4] < 0 && r[5] < 0) return;
+    ids[0] = r[2]; ids[1] = r[3]; ids[2] = r[4]; ids[3] = r[5];
+  }
+  double P0[12], P1[12];
+  for (int k = 0; k < 4; k++) {
+    cpos(v.c, v.x0, ids[k], P0 + k * 3);
+    cpos(v.c, xt, ids[k], P1 + k * 3);
+  }
+  const double toi = r[0] == 0 ? vt_ccd(P0, P1, dMin) : ee_ccd(P0, P1, dMin);
+  v.ctoi[i] = toi;
+  uint32_t st = 0;
+  if (isnan(toi)) st = 2;
+  else if (toi > 0 && toi < 1 - 1e-9) st = 1;
+  v.cflag[i] = st;
+  if (st) atomicMin(&v.cint[CI_FIRSTBAD], i);
+}
+
+__global__ void k_trial_floor(CView v, const double* xt, double dMin) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= v.n) return;
+  v.vtmp2[q] = INFINITY;
+  if (!v.c.hasFloor) { v.vtmp[q] = INFINITY; return; }
+  const double dd = xt[q * 3 + 1] - v.c.floorY;
+  v.vtmp[q] = dd;
+  const double y0 = v.x0[q * 3 + 1] - v.c.floorY;
+  const double yT = xt[q * 3 + 1] - v.c.floorY;
+  if (y0 - fabs(yT - y0) > dMin) return;
+  if (y0 > dMin && yT <= dMin && y0 > yT) {
+    const double toi = (y0 - dMin) / (y0 - yT);
+    v.vtmp2[q] = toi;
+    if (toi < 1 - 1e-9) atomicOr(&v.cint[CI_FLOORBAD], 1);
+  }
+}
+
+__global__ void __launch_bounds__(1024) k_trial_final(CView v, int C, double dMin) {
+  const double minDist = block_min2(v.cmin, C, v.vtmp, v.n);
+  const double minTOI = block_min2(v.ctoi, C, v.vtmp2, v.n);
+  if (threadIdx.x != 0) return;
+  int valid = 0;
+  DevDiag* dg = v.diag;
+  if (v.cint[CI_FIRSTNF] != INT_MAX) {
+    dg->ccdFailures += 1;
+  } else if (minDist <= dMin) {
+  } else if (v.cint[CI_FIRSTBAD] != INT_MAX) {
+    if (v.cflag[v.cint[CI_FIRSTBAD]] == 2) dg->ccdFailures += 1;
+  } else if (v.cint[CI_FLOORBAD]) {
+  } else {
+    valid = 1;
+    if (minDist < dg->minDistance) dg->minDistance = minDist;
+    if (minTOI < dg->minTOI) dg->minTOI = minTOI;
+  }
+  dg->trialMinDist = minDist;
+  dg->trialMinTOI = minTOI;
+  v.cint[CI_VALID] = valid;
+}
+
+// ---- restitution-0 filter (newton.ts:238-303) -----------------------------------------
+// VT/EE impulses in list order by one thread (each sees the earlier updates).
+__global__ void k_kill_vtee(CView v, double* vel, int nve) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  for (int i = 0; i < nve; i++) {
+    const Frozen c = v.active[i];
+    if (c.kind == 0) {
+      const double vp[3] = {vel[c.p * 3], vel[c.p * 3 + 1], vel[c.p * 3 + 2]};
+      double tx = 0, ty = 0, tz = 0;
+      const double ws[3] = {c.w0, c.w1, c.w2};
+      const int vs[3] = {c.a, c.b, c.c};
+      for (int k = 0; k < 3; k++) {
+        if (vs[k] < 0) continue;
+        tx += ws[k] * vel[vs[k] * 3];
+        ty += ws[k] * vel[vs[k] * 3 + 1];
+        tz += ws[k] * vel[vs[k] * 3 + 2];
+      }
+      const double rel = (vp[0] - tx) * c.nx + (vp[1] - ty) * c.ny + (vp[2] - tz) * c.nz;
+      if (rel < 0) {
+        const double j = -0.5 * rel;
+        vel[c.p * 3] += j * c.nx;
+        vel[c.p * 3 + 1] += j * c.ny;
+        vel[c.p * 3 + 2] += j * c.nz;
+        for (int k = 0; k < 3; k++) {
+          if (vs[k] < 0) continue;
+          vel[vs[k] * 3] -= j * ws[k] * c.nx;
+          vel[vs[k] * 3 + 1] -= j * ws[k] * c.ny;
+          vel[vs[k] * 3 + 2] -= j * ws[k] * c.nz;
+        }
+      }
+      continue;
+    }
+    double A[3] = {0, 0, 0}, B[3] = {0, 0, 0};
+    {
+      double xa[3] = {0, 0, 0}, xb[3] = {0, 0, 0};
+      if (c.a >= 0) for (int k = 0; k < 3; k++) xa[k] = vel[c.a * 3 + k];
+      if (c.b >= 0) for (int k = 0; k < 3; k++) xb[k] = vel[c.b * 3 + k];
+      for (int k = 0; k < 3; k++) A[k] = (xa[k] + xb[k]) / 2;
+      double xc[3] = {0, 0, 0}, xd[3] = {0, 0, 0};
+      if (c.c >= 0) for (int k = 0; k < 3; k++) xc[k] = vel[c.c * 3 + k];
+      if (c.d >= 0) for (int k = 0; k < 3; k++) xd[k] = vel[c.d * 3 + k];
+      for (int k = 0; k < 3; k++) B[k] = (xc[k] + xd[k]) / 2;
+    }
+    const double rel = (A[0] - B[0]) * c.nx + (A[1] - B[1]) * c.ny + (A[2] - B[2]) * c.nz;
+    if (rel < 0) {
+      const double j = -0.25 * rel;
+      const int up[2] = {c.a, c.b}, dn[2] = {c.c, c.d};
+      for (int q = 0; q < 2; q++) {
+        if (up[q] < 0) continue;
+        vel[up[q] * 3] += j * c.nx; vel[up[q] * 3 + 1] += j * c.ny; vel[up[q] * 3 + 2] += j * c.nz;
+      }
+      for (int q = 0; q < 2; q++) {
+        if (dn[q] < 0) continue;
+        vel[dn[q] * 3] -= j * c.nx; vel[dn[q] * 3 + 1] -= j * c.ny; vel[dn[q] * 3 + 2] -= j * c.nz;
+      }
+    }
+  }
+}
+
+__global__ void k_kill_floor(CView v, double* vel, int base, int nf) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nf) return;
+  const int p = v.active[base + i].p;
+  if (vel[p * 3 + 1] < 0) vel[p * 3 + 1] = 0;
+}
+
+// ---- host side --------------------------------------------------------------------------
+template <class T>
+static void dalloc(T*& p, size_t n) {
+  if (p) cudaFree(p);
+  p = nullptr;
+  if (n) CK(cudaMalloc(&p, n * sizeof(T)));
+}
+template <class T>
+static void dfree(T*& p) {
+  if (p) cudaFree(p);
+  p = nullptr;
+}
+
+static CView view(ContactHost& h, Solver& s) {
+  CView v;
+  v.c = s.d.c;
+  v.nCand = h.nCand;
+  v.nFloor = h.nFloor;
+  v.n = h.n;
+  v.x0 = s.d.x0;
+  v.srt = h.cand.srt;
+  v.cflag = h.cflag;
+  v.fflag = h.fflag;
+  v.cmin = h.cmin;
+  v.ctoi = h.ctoi;
+  v.vtmp = h.probe + 3 * (size_t)h.n;
+  v.vtmp2 = h.probe + 4 * (size_t)h.n;
+  v.active = h.active;
+  v.dd = h.dd;
+  v.cg = h.cg;
+  v.tc = h.tc;
+  v.tf = h.tf;
+  v.lagFloor = h.lagFloor;
+  v.lagFloorOk = h.lagFloorOk;
+  v.lagKeys = h.lk0;
+  v.lagVals = h.lsorted;
+  v.lagCount = h.lagCount;
+  v.cint = h.cint;
+  v.diag = h.diag;
+  return v;
+}
+
+ContactHost::~ContactHost() {
+  for (void** q : {(void**)&spos, (void**)&sidx, (void**)&bvh.box64, (void**)&bvh.boxc, (void**)&bvh.boxr,
+                   (void**)&bvh.cent, (void**)&bvh.scene, (void**)&bvh.k0, (void**)&bvh.k1, (void**)&bvh.p0,
+                   (void**)&bvh.p1, (void**)&bvh.hist, (void**)&bvh.left, (void**)&bvh.right, (void**)&bvh.parent,
+                   (void**)&bvh.depth, (void**)&bvh.nbox, (void**)&bvh.visit, (void**)&bvh.root, (void**)&bvh.cnt,
+                   (void**)&bvh.pairs, (void**)&scnt, (void**)&spairs, (void**)&cand.rec, (void**)&cand.srt,
+                   (void**)&cand.k0, (void**)&cand.k1, (void**)&cand.p0, (void**)&cand.p1, (void**)&cand.hist,
+                   (void**)&cflag, (void**)&fflag, (void**)&cmin, (void**)&ctoi, (void**)&active, (void**)&dd,
+                   (void**)&cg, (void**)&tc, (void**)&tf, (void**)&rk0, (void**)&rk1, (void**)&rp0, (void**)&rp1,
+                   (void**)&rhist, (void**)&cOff, (void**)&lagFloor, (void**)&lagFloorOk, (void**)&lk0,
+                   (void**)&lk1, (void**)&lp0, (void**)&lp1, (void**)&lhist, (void**)&lval, (void**)&lsorted,
+                   (void**)&probe, (void**)&diag, (void**)&cint})
+    if (*q) cudaFree(*q);
+  if (hint) cudaFreeHost(hint);
+  if (hdiag) cudaFreeHost(hdiag);
+}
+
+void ContactHost::init(Solver& s, const cs_contact_params* prm, int floor_on, double floor_y, const float* sp,
+                       int nsv, const uint32_t* si, int msv) {
+  p = *prm;
+  hasFloor = floor_on != 0;
+  floorY = floor_y;
+  n = s.mesh.n;
+  m = s.mesh.m;
+  ns = nsv;
+  ms = msv;
+  if ((long)n + ns + 2 >= (1l << 24)) throw std::invalid_argument("too many vertices for the candidate key");
+  if (ms > 0) {
+    for (int i = 0; i < 3 * ms; i++)
+      if ((int)si[i] >= ns) throw std::invalid_argument("static index out of range");
+    dalloc(spos, 3 * (size_t)ns);
+    dalloc(sidx, 3 * (size_t)ms);
+    CK(cudaMemcpy(spos, sp, 12 * (size_t)ns, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(sidx, si, 12 * (size_t)ms, cudaMemcpyHostToDevice));
+  }
+  bvh.m = m;
+  bvh.ns = ns;
+  bvh.ms = ms;
+  bvh.idx = s.idx.p;
+  bvh.spos = spos;
+  bvh.sidx = sidx;
+  const size_t nn = std::max(1, 2 * m - 1);
+  dalloc(bvh.box64, 6 * (size_t)m);
+  dalloc(bvh.boxc, 6 * (size_t)m);
+  dalloc(bvh.boxr, 6 * (size_t)m);
+  dalloc(bvh.cent, 3 * (size_t)m);
+  dalloc(bvh.scene, 6);
+  dalloc(bvh.k0, (size_t)m);
+  dalloc(bvh.k1, (size_t)m);
+  dalloc(bvh.p0, (size_t)m);
+  dalloc(bvh.p1, (size_t)m);
+  dalloc(bvh.hist, 256 * (size_t)((m + kSortTile - 1) / kSortTile) + 1);
+  dalloc(bvh.left, nn);
+  dalloc(bvh.right, nn);
+  dalloc(bvh.parent, nn);
+  dalloc(bvh.depth, nn);
+  dalloc(bvh.nbox, 6 * nn);
+  dalloc(bvh.visit, nn);
+  dalloc(bvh.root, 1);
+  dalloc(bvh.cnt, (size_t)m + 1);
+  dalloc(scnt, (size_t)std::max(ms, 1) + 1);
+  dalloc(fflag, (size_t)n + 1);
+  dalloc(cOff, (size_t)n + 1);
+  dalloc(lagFloor, (size_t)n);
+  dalloc(lagFloorOk, (size_t)n);
+  dalloc(probe, 5 * (size_t)n);
+  dalloc(diag, 1);
+  dalloc(cint, CI_N);
+  CK(cudaMallocHost(&hint, CI_N * sizeof(int)));
+  CK(cudaMallocHost(&hdiag, sizeof(DevDiag)));
+  ensure_pairs(1024, 64);
+  ensure_cands(1024);
+  ensure_active(s, std::max(1024, n + 64));
+  ensure_lag(1024);
+  bvh.flags = cint + CI_OVERFLOW;
+  bind(s);
+}
+
+void ContactHost::ensure_pairs(size_t np, size_t nsp) {
+  if (np > pairCap) { pairCap = np + np / 2 + 64; dalloc(bvh.pairs, pairCap); }
+  if (nsp > spairCap) { spairCap = nsp + nsp / 2 + 64; dalloc(spairs, spairCap); }
+}
+void ContactHost::ensure_cands(size_t nc) {
+  if ((int)nc <= cand.cap) return;
+  const size_t c = nc + nc / 2 + 256;
+  cand.cap = (int)c;
+  dalloc(cand.rec, 6 * c);
+  dalloc(cand.srt, 6 * c);
+  dalloc(cand.k0, c);
+  dalloc(cand.k1, c);
+  dalloc(cand.p0, c);
+  dalloc(cand.p1, c);
+  dalloc(cand.hist, 256 * ((c + kSortTile - 1) / kSortTile) + 1);
+  dalloc(cflag, c + 1);
+  dalloc(cmin, c);
+  dalloc(ctoi, c);
+}
+void ContactHost::ensure_active(Solver& s, size_t na) {
+  if (na <= actCap) return;
+  const size_t c = na + na / 2 + 256;
+  actCap = c;
+  dalloc(active, c);
+  dalloc(dd, c);
+  dalloc(cg, 4 * c);
+  dalloc(tc, c);
+  dalloc(tf, c);
+  dalloc(rk0, 4 * c);
+  dalloc(rk1, 4 * c);
+  dalloc(rp0, 4 * c);
+  dalloc(rp1, 4 * c);
+  dalloc(rhist, 256 * ((4 * c + kSortTile - 1) / kSortTile) + 1);
+  (void)s;
+}
+void ContactHost::ensure_lag(size_t nl) {
+  if (nl <= lagCap) return;
+  const size_t c = nl + nl / 2 + 256;
+  // keep existing sorted entries
+  Key<6>* ok = nullptr;
+  double4* ov = nullptr;
+  if (lagCount > 0) {
+    CK(cudaMalloc(&ok, lagCount * sizeof(Key<6>)));
+    CK(cudaMalloc(&ov, lagCount * sizeof(double4)));
+    CK(cudaMemcpy(ok, lk0, lagCount * sizeof(Key<6>), cudaMemcpyDeviceToDevice));
+    CK(cudaMemcpy(ov, lsorted, lagCount * sizeof(double4), cudaMemcpyDeviceToDevice));
+  }
+  lagCap = c;
+  dalloc(lk0, c);
+  dalloc(lk1, c);
+  dalloc(lp0, c);
+  dalloc(lp1, c);
+  dalloc(lhist, 256 * ((c + kSortTile - 1) / kSortTile) + 1);
+  dalloc(lval, c);
+  dalloc(lsorted, c);
+  if (lagCount > 0) {
+    CK(cudaMemcpy(lk0, ok, lagCount * sizeof(Key<6>), cudaMemcpyDeviceToDevice));
+    CK(cudaMemcpy(lsorted, ov, lagCount * sizeof(double4), cudaMemcpyDeviceToDevice));
+    cudaFree(ok);
+    cudaFree(ov);
+  }
+}
+
+void ContactHost::bind(Solver& s) {
+  Contact& c = s.d.c;
+  c.dHat = p.dhat; c.kappa = p.kappa; c.dMin = p.dmin; c.mu = p.mu; c.eps = p.eps;
+  c.floorY = floorY;
+  c.hasFloor = hasFloor ? 1 : 0;
+  c.ns = ns;
+  c.spos = spos;
+  c.nActive = nCand + nFloor;
+  c.active = active;
+  c.dd = dd;
+  c.cg = cg;
+  c.cOff = cOff;
+  c.cRec = rp0;
+  s.d.Tc = tc;
+  s.d.hasContact = 1;
+}
+
+void ContactHost::read_ints(Solver& s) {
+  CK(cudaMemcpyAsync(hint, cint, CI_N * sizeof(int), cudaMemcpyDeviceToHost, s.stream));
+  CK(cudaStreamSynchronize(s.stream));
+}
+
+int ContactHost::build_candidates(Solver& s, const double* x, double pad) {
+  cudaStream_t st = s.stream;
+  int64_t& lc = launch_counter();
+  CK(cudaMemsetAsync(cint, 0, CI_N * sizeof(int), st));
+  bvh_build(bvh, s.d.x0, x, pad, false, st, &lc);
+  bvh_count_self(bvh, false, st, &lc);
+  scan_counts(bvh.cnt, m, (uint32_t*)(cint + CI_SELF), st, &lc);
+  BvhBufs sb = bvh;
+  sb.cnt = scnt;
+  if (ms > 0) {
+    bvh_count_static(sb, pad, st, &lc);
+    scan_counts(scnt, ms, (uint32_t*)(cint + CI_STATIC), st, &lc);
+  }
+  read_ints(s);
+  if (hint[CI_OVERFLOW]) throw CapacityError("broadphase traversal aborted (stack deeper than 64 or malformed tree)");
+  const int P = hint[CI_SELF], S = ms > 0 ? hint[CI_STATIC] : 0;
+  ensure_pairs(P, S);
+  if (P > 0) bvh_emit_self(bvh, false, st, &lc);
+  if (S > 0) {
+    sb.pairs = bvh.pairs;
+    bvh_emit_static(sb, pad, spairs, st, &lc);
+  }
+  const long C = 15l * P + 12l * S;
+  if (C > INT_MAX / 8) throw CapacityError("too many contact candidates");
+  ensure_cands(C);
+  make_candidates(cand, s.idx.p, sidx, ns, bvh.pairs, P, spairs, S, st, &lc);
+  return (int)C;
+}
+
+void ContactHost::update_active_set(Solver& s, double* x) {
+  cudaStream_t st = s.stream;
+  int64_t& lc = launch_counter();
+  const int C = build_candidates(s, x, p.dhat);
+  candidatePairs = C;
+  CK(cudaMemsetAsync(cint + CI_NVT, 0, sizeof(int), st));
+  CView v = view(*this, s);
+  if (C > 0) {
+    k_cand_flags<<<cnb(C), kCT, 0, st>>>(v, x, C);
+    lc++;
+  }
+  k_floor_flags<<<cnb(n), kCT, 0, st>>>(v, x);
+  k_active_min<<<1, 1024, 0, st>>>(v, C, n);
+  lc += 2;
+  if (C > 0) scan_counts(cflag, C, (uint32_t*)(cint + CI_NCAND), st, &lc);
+  else CK(cudaMemsetAsync(cint + CI_NCAND, 0, sizeof(int), st));
+  scan_counts(fflag, n, (uint32_t*)(cint + CI_NFLOOR), st, &lc);
+  read_ints(s);
+  nCand = hint[CI_NCAND];
+  nFloor = hint[CI_NFLOOR];
+  nVT = hint[CI_NVT];
+  const int na = nCand + nFloor;
+  ensure_active(s, na);
+  v = view(*this, s);
+  if (C > 0) {
+    k_cand_compact<<<cnb(C), kCT, 0, st>>>(v, x, C);
+    lc++;
+  }
+  k_floor_compact<<<cnb(n), kCT, 0, st>>>(v, x);
+  lc++;
+  activePairs = na;
+  vtPairs = nVT;
+  eePairs = nCand - nVT;
+  floorPairs = nFloor;
+  // vertex -> (contact, slot) CSR in contact order
+  if (na > 0) {
+    k_csr_records<<<cnb(4l * na), kCT, 0, st>>>(v, rk0, rp0, na);
+    lc++;
+    const bool flip = radix_sort<1>(rk0, rp0, rk1, rp1, 4 * na, 32, rhist, st, &lc);
+    if (flip) {
+      CK(cudaMemcpyAsync(rk0, rk1, 4 * (size_t)na * sizeof(Key<1>), cudaMemcpyDeviceToDevice, st));
+      CK(cudaMemcpyAsync(rp0, rp1, 4 * (size_t)na * 4, cudaMemcpyDeviceToDevice, st));
+    }
+    k_csr_offsets<<<cnb(n + 1), kCT, 0, st>>>(rk0, 4 * na, cOff, n);
+    lc++;
+  } else {
+    CK(cudaMemsetAsync(cOff, 0, ((size_t)n + 1) * 4, st));
+  }
+  bind(s);
+}
+
+void ContactHost::gradient_terms(Solver& s) {
+  cudaStream_t st = s.stream;
+  int64_t& lc = launch_counter();
+  update_active_set(s, s.d.x);
+  const int na = nCand + nFloor;
+  CView v = view(*this, s);
+  if (na > 0) {
+    k_contact_prep<<<cnb(na), kCT, 0, st>>>(v, s.d.x, na);
+    k_contact_chains<<<1, 64, 0, st>>>(v, na);
+    lc += 2;
+  } else {
+    k_contact_chains<<<1, 64, 0, st>>>(v, 0);
+    lc++;
+  }
+  k_contact_grad_gather<<<cnb(n), kCT, 0, st>>>(v, s.d.cgrad);
+  lc++;
+  if (na > 0) {
+    k_contact_curv<<<cnb(na), kCT, 0, st>>>(v, s.d.x, na);
+    k_contact_diag_gather<<<cnb(n), kCT, 0, st>>>(v, s.d.diag);
+    lc += 2;
+  }
+}
+
+void ContactHost::merit_energy(Solver& s, const double* x) {
+  const int na = nCand + nFloor;
+  if (na <= 0) return;
+  CView v = view(*this, s);
+  k_contact_merit<<<cnb(na), kCT, 0, s.stream>>>(v, x, na);
+  launch_counter()++;
+}
+
+bool ContactHost::check_trial(Solver& s, const double* xt) {
+  cudaStream_t st = s.stream;
+  int64_t& lc = launch_counter();
+  const int C = build_candidates(s, xt, p.dmin);
+  candidatePairs = C;
+  k_trial_reset<<<1, 1, 0, st>>>(cint);
+  CView v = view(*this, s);
+  if (C > 0) {
+    k_trial_cand<<<cnb(C), kCT, 0, st>>>(v, xt, C, p.dmin);
+    lc++;
+  }
+  k_trial_floor<<<cnb(n), kCT, 0, st>>>(v, xt, p.dmin);
+  k_trial_final<<<1, 1024, 0, st>>>(v, C, p.dmin);
+  lc += 3;
+  read_ints(s);
+  return hint[CI_VALID] != 0;
+}
+
+void ContactHost::commit(Solver& s, const double* x) {
+  cudaStream_t st = s.stream;
+  int64_t& lc = launch_counter();
+  const int na = nCand + nFloor;
+  if (na <= 0) return;
+  ensure_lag((size_t)lagCount + nCand + 1);
+  if (nCand > 0 && lagCount > 0) {
+    // the sorted prefix becomes entries 0..lagCount-1 with their values in place
+    CK(cudaMemcpyAsync(lval, lsorted, (size_t)lagCount * sizeof(double4), cudaMemcpyDeviceToDevice, st));
+    k_iota<<<cnb(lagCount), kCT, 0, st>>>(lp0, lagCount);
+    lc++;
+  }
+  CView v = view(*this, s);
+  k_contact_commit<<<cnb(na), kCT, 0, st>>>(v, x, na, lk0, lp0, lval, lagCount, commitNo);
+  lc++;
+  commitNo++;
+  if (nCand > 0) {
+    const int total = lagCount + nCand;
+    const bool flip = radix_sort<6>(lk0, lp0, lk1, lp1, total, 192, lhist, st, &lc);
+    const uint32_t* sp = flip ? lp1 : lp0;
+    k_gather_vals<<<cnb(total), kCT, 0, st>>>(lval, sp, total, lsorted);
+    lc++;
+    if (flip) CK(cudaMemcpyAsync(lk0, lk1, (size_t)total * sizeof(Key<6>), cudaMemcpyDeviceToDevice, st));
+    lagCount = total;
+  }
+}
+
+void ContactHost::kill_approach_velocity(Solver& s) {
+  update_active_set(s, s.d.x);
+  CView v = view(*this, s);
+  if (nCand > 0) {
+    k_kill_vtee<<<1, 1, 0, s.stream>>>(v, s.d.v, nCand);
+    launch_counter()++;
+  }
+  if (nFloor > 0) {
+    k_kill_floor<<<cnb(nFloor), kCT, 0, s.stream>>>(v, s.d.v, nCand, nFloor);
+    launch_counter()++;
+  }
+}
+
+void ContactHost::begin_step_and_bisect(Solver& s) {
+  cudaStream_t st = s.stream;
+  DevDiag z{};
+  z.minDistance = INFINITY;
+  z.minTOI = INFINITY;
+  CK(cudaMemcpyAsync(diag, &z, sizeof z, cudaMemcpyHostToDevice, st));
+  CK(cudaMemsetAsync(lagFloorOk, 0, (size_t)n, st));
+  lagCount = 0;
+  commitNo = 0;
+  rejections = 0;
+  candidatePairs = activePairs = vtPairs = eePairs = floorPairs = 0;
+  nCand = nFloor = nVT = 0;
+  bind(s);
+  CK(cudaStreamSynchronize(st));  // z is a host temporary
+  if (check_trial(s, s.d.x)) return;
+  double lo = 0, hi = 1;
+  const int n3 = 3 * n;
+  for (int b = 0; b < 8; b++) {
+    const double mid = 0.5 * (lo + hi);
+    k_lerp<<<cnb(n3), kCT, 0, st>>>(probe, s.d.x0, s.d.x, mid, n3);
+    launch_counter()++;
+    launch_pins(s.d, probe, st);
+    if (check_trial(s, probe)) lo = mid;
+    else hi = mid;
+    if (hi - lo < 1e-4) break;
+  }
+  k_lerp<<<cnb(n3), kCT, 0, st>>>(s.d.x, s.d.x0, s.d.x, lo, n3);
+  launch_counter()++;
+  launch_pins(s.d, s.d.x, st);
+}
+
+void ContactHost::fill_stats(Solver& s, cs_step_stats& out) {
+  CK(cudaMemcpyAsync(hdiag, diag, sizeof(DevDiag), cudaMemcpyDeviceToHost, s.stream));
+  CK(cudaStreamSynchronize(s.stream));
+  out.candidate_pairs = candidatePairs;
+  out.active_pairs = activePairs;
+  out.vt_pairs = vtPairs;
+  out.ee_pairs = eePairs;
+  out.floor_pairs = floorPairs;
+  out.min_distance = hdiag->minDistance;
+  out.min_toi = hdiag->minTOI;
+  out.barrier_energy = hdiag->barrierEnergy;
+  out.friction_work = hdiag->frictionWork;
+  out.rejected_line_search_steps = rejections;
+  out.ccd_failures = hdiag->ccdFailures;
+}
+
+void set_contact(Solver& s, const cs_contact_params* p, int floor_on, double floor_y, const float* sp, int ns,
+                 const uint32_t* si, int ms) {
+  if (!p) {
+    s.contact.reset();
+    s.d.hasContact = 0;
+    return;
+  }
+  if (!(p->dhat > 0) || !(p->dmin >= 0) || !(p->kappa >= 0) || !(p->eps > 0) || !(p->mu >= 0))
+    throw std::invalid_argument("bad contact parameters");
+  if ((ns > 0) != (ms > 0) || (ms > 0 && (!sp || !si))) throw std::invalid_argument("bad static mesh");
+  auto c = std::make_unique<ContactHost>();
+  c->init(s, p, floor_on, floor_y, sp, ns, si, ms);
+  s.contact = std::move(c);
+}
 
 }  // namespace cs

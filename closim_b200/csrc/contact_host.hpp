@@ -2,9 +2,15 @@
 // device buffers of the frozen active set, broadphase and CCD, and the calls
 // the Newton step makes into them.
 #pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
 #include <stdexcept>
+#include <vector>
 
 #include "../../include/closim_cuda.h"
+#include "broadphase.cuh"
+#include "plain.cuh"
 
 namespace cs {
 
@@ -14,9 +20,69 @@ struct CapacityError : std::runtime_error {
   using std::runtime_error::runtime_error;
 };
 
+// Device-resident contact diagnostics (ContactDiagnostics, types.ts:49-62).
+struct DevDiag {
+  double minDistance, minTOI, barrierEnergy, frictionWork, ccdFailures;
+  double trialMinDist, trialMinTOI;
+  double pad;
+};
+
+// Device counters read back by the host (int32).
+enum CInt { CI_SELF = 0, CI_STATIC, CI_OVERFLOW, CI_NCAND, CI_NFLOOR, CI_NVT, CI_VALID, CI_FIRSTNF, CI_FIRSTBAD,
+            CI_FLOORBAD, CI_N = 16 };
+
 class ContactHost {
  public:
+  cs_contact_params p{};
+  bool hasFloor = false;
+  double floorY = 0;
+  int n = 0, m = 0, ns = 0, ms = 0;
   double rejections = 0;
+  double candidatePairs = 0, activePairs = 0, vtPairs = 0, eePairs = 0, floorPairs = 0;
+  int nCand = 0, nFloor = 0, nVT = 0;  // current frozen set layout
+  int commitNo = 0, lagCount = 0;
+
+  // static mesh
+  float* spos = nullptr;
+  uint32_t* sidx = nullptr;
+  // broadphase
+  BvhBufs bvh;
+  uint32_t* scnt = nullptr;    // ms + 1
+  int2* spairs = nullptr;
+  size_t pairCap = 0, spairCap = 0;
+  CandBufs cand;
+  uint32_t* cflag = nullptr;   // per-candidate flag / offset (cand cap + 1)
+  uint32_t* fflag = nullptr;   // per-vertex floor flag / offset (n + 1)
+  double* cmin = nullptr;      // per-candidate distance (cand cap)
+  double* ctoi = nullptr;      // per-candidate toi
+  // frozen set
+  size_t actCap = 0;
+  Frozen* active = nullptr;
+  double* dd = nullptr;
+  double* cg = nullptr;        // 4 per contact
+  double* tc = nullptr;        // per-contact chain terms (merit)
+  double* tf = nullptr;        // per-contact chain terms (friction work)
+  Key<1>* rk0 = nullptr; Key<1>* rk1 = nullptr;
+  uint32_t* rp0 = nullptr; uint32_t* rp1 = nullptr; uint32_t* rhist = nullptr;
+  uint32_t* cOff = nullptr;    // n + 1
+  // lagged normals / multipliers
+  double* lagFloor = nullptr;  // n
+  uint8_t* lagFloorOk = nullptr;
+  size_t lagCap = 0;
+  Key<6>* lk0 = nullptr; Key<6>* lk1 = nullptr;
+  uint32_t* lp0 = nullptr; uint32_t* lp1 = nullptr; uint32_t* lhist = nullptr;
+  double4* lval = nullptr;     // appended values, indexed by payload
+  double4* lsorted = nullptr;  // values in sorted key order
+  // probes
+  double* probe = nullptr;
+  DevDiag* diag = nullptr;
+  int* cint = nullptr;
+  int* hint = nullptr;         // pinned mirror of cint
+  DevDiag* hdiag = nullptr;    // pinned mirror of diag
+
+  ~ContactHost();
+  void init(Solver& s, const cs_contact_params* prm, int floor_on, double floor_y, const float* sp, int nsv,
+            const uint32_t* si, int msv);
   void begin_step_and_bisect(Solver& s);
   void update_active_set(Solver& s, double* x);
   void merit_energy(Solver& s, const double* x);
@@ -25,6 +91,15 @@ class ContactHost {
   void commit(Solver& s, const double* x);
   void kill_approach_velocity(Solver& s);
   void fill_stats(Solver& s, cs_step_stats& st);
+  // broadphase stage only: candidate count for a segment xStep -> x with pad
+  int build_candidates(Solver& s, const double* x, double pad);
+  void bind(Solver& s);  // refresh the Contact view inside the solver's Dev
+ private:
+  void read_ints(Solver& s);
+  void ensure_pairs(size_t np, size_t nsp);
+  void ensure_cands(size_t nc);
+  void ensure_active(Solver& s, size_t na);
+  void ensure_lag(size_t nl);
 };
 
 void set_contact(Solver& s, const cs_contact_params* p, int floor_on, double floor_y, const float* sp, int ns,

@@ -44,7 +44,7 @@ __global__ void __launch_bounds__(kSortThreads) k_radix_hist(const Key<KW>* keys
 }
 
 // Exclusive scan of `n` u32 in place by one block (chunked, running carry).
-__global__ void __launch_bounds__(1024) k_scan_exclusive(uint32_t* a, int n, uint32_t* total) {
+static __global__ void __launch_bounds__(1024) k_scan_exclusive(uint32_t* a, int n, uint32_t* total) {
   __shared__ uint32_t s[1024];
   __shared__ uint32_t carry;
   if (threadIdx.x == 0) carry = 0;

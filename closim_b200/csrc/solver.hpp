@@ -1,0 +1,379 @@
+// The CUDA cloth solver instance: device buffers, set-up and the host
+// orchestration of one implicit-Euler step (shared by solver.cu and contact.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/closim_cuda.h"
+#include "contact_host.hpp"
+#include "plain.cuh"
+#include "setup.hpp"
+
+namespace cs {
+
+inline int64_t& launch_counter() {
+  static int64_t c = 0;
+  return c;
+}
+
+struct CudaError : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+#define CK(x)                                                                                    \
+  do {                                                                                           \
+    cudaError_t e_ = (x);                                                                        \
+    if (e_ != cudaSuccess) throw CudaError(std::string(#x) + ": " + cudaGetErrorString(e_));   \
+  } while (0)
+
+template <class T>
+struct DBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  void alloc(size_t k) {
+    free();
+    n = k;
+    if (k) CK(cudaMalloc(&p, k * sizeof(T)));
+  }
+  void upload(const T* h, size_t k, cudaStream_t s) {
+    if (k > n) alloc(k);
+    if (k) CK(cudaMemcpyAsync(p, h, k * sizeof(T), cudaMemcpyHostToDevice, s));
+  }
+  void free() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  ~DBuf() { free(); }
+};
+
+struct NonFinite : std::runtime_error {
+  NonFinite() : std::runtime_error("non-finite gradient — blow up; reduce dt/stiffness") {}
+};
+
+class Solver {
+ public:
+  int precision = CS_PRECISION_FP64;
+  int device = 0;
+  bool ready = false;
+  cudaStream_t stream = nullptr;
+  HostMesh mesh;
+  cs_material mat{};
+  double gravity[3] = {0, -9.81, 0};
+  cs_stepper_options opts{10, 60, 10, CS_PRECOND_JACOBI, 1e-5};
+  cs_step_stats stats{};
+  bool haveStats = false;
+  std::vector<int> pinIds;
+  std::vector<double> pinPos;
+  std::unique_ptr<ContactHost> contact;
+
+  // device buffers
+  DBuf<uint32_t> idx, memOff, memRec, hinOff, hinRec;
+  DBuf<float4> inv;
+  DBuf<float> area, mass;
+  DBuf<int4> hinge;
+  DBuf<double> hmeta;
+  DBuf<uint8_t> pinned;
+  DBuf<int> pinIdsD, domStart, domVerts, v2tOff, v2t;
+  DBuf<double> pinPosD;
+  DBuf<double> vx, vv, vx0, vyHat, vg, vdiag, vdx, vr, vz, vp, vAp, vxt, vcgrad, vcHp, elem, helem, part, scal, L;
+  DBuf<double> T0, T1, T2, T3, Tc;
+  DBuf<uint8_t> domFlag;
+  double* hscal = nullptr;  // pinned host mirror of scal
+  int pcgBlocks = 1;
+  Dev d{};
+  // profiling of the linear-solve kernel
+  bool prof = false;
+  cudaEvent_t pev0 = nullptr, pev1 = nullptr;
+  double profMs = 0, profLaunches = 0, profBytes = 0, profIters = 0;
+  bool profPending = false;
+
+  // Algorithmic bytes of one k_pcg launch that ran `iters` iterations: per
+  // iteration the FD HVP reads x, p (2 x 24 B per vertex), Dm^-1, area and 3
+  // indices per triangle (32 B), writes and re-reads 18 element doubles
+  // (2 x 144 B per triangle), reads mass (4 B) and writes Ap (24 B); the vector
+  // update reads p, Ap, x, r, diag and writes x, r, z, p (9 x 24 B per vertex);
+  // Schwarz adds one read of its 24x24 factors (4608 B per domain).
+  double pcg_bytes(int iters) const {
+    const double n = mesh.n, m = mesh.m;
+    double hvp = 2 * 24 * n + 32 * m + 2 * 144 * m + 4 * n + 24 * n;
+    double vec = 9 * 24 * n + (d.precond == 1 ? 4608.0 * mesh.D : 0.0);
+    double init = 6 * 24 * n;
+    double post = 4 * 24 * n;
+    return init + iters * (hvp + vec) + post;
+  }
+  void prof_collect(int iters) {
+    if (!profPending) return;
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, pev0, pev1));
+    profMs += ms;
+    profLaunches += 1;
+    profBytes += pcg_bytes(iters);
+    profIters += iters;
+    profPending = false;
+  }
+
+  ~Solver() {
+    if (pev0) cudaEventDestroy(pev0);
+    if (pev1) cudaEventDestroy(pev1);
+    if (hscal) cudaFreeHost(hscal);
+    if (stream) cudaStreamDestroy(stream);
+  }
+
+  void create(int prec, int dev) {
+    precision = prec;
+    device = dev;
+    CK(cudaSetDevice(dev));
+    CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    CK(cudaMallocHost(&hscal, S_NSCALARS * sizeof(double)));
+    CK(cudaEventCreate(&pev0));
+    CK(cudaEventCreate(&pev1));
+  }
+
+  void set_material(const cs_material& m) {
+    mat = m;
+    d.mat = Mat<double>{m.stretch_warp, m.stretch_weft, m.stretch_coupling, m.shear, m.thickness};
+    d.kb = 0.5 * (m.bend_warp + m.bend_weft);
+  }
+
+  void initialize(const cs_mesh& cm, const cs_material& m, const double* g, const double* x, const double* v) {
+    CK(cudaSetDevice(device));
+    if (cm.n <= 0 || cm.m <= 0 || cm.hg < 0) throw std::invalid_argument("bad mesh sizes");
+    if (!cm.indices || !cm.rest || !cm.inv_dm || !cm.area || !cm.mass || (cm.hg > 0 && (!cm.hinge || !cm.hinge_meta)))
+      throw std::invalid_argument("null mesh array");
+    mesh = HostMesh();
+    mesh.n = cm.n; mesh.m = cm.m; mesh.hg = cm.hg;
+    mesh.idx.assign(cm.indices, cm.indices + 3 * (size_t)cm.m);
+    for (uint32_t q : mesh.idx)
+      if ((int)q >= cm.n) throw std::invalid_argument("triangle index out of range");
+    mesh.rest.assign(cm.rest, cm.rest + 3 * (size_t)cm.n);
+    mesh.inv.assign(cm.inv_dm, cm.inv_dm + 4 * (size_t)cm.m);
+    mesh.area.assign(cm.area, cm.area + cm.m);
+    mesh.mass.assign(cm.mass, cm.mass + cm.n);
+    mesh.hinge.assign(cm.hinge, cm.hinge + 4 * (size_t)cm.hg);
+    for (int q : mesh.hinge)
+      if (q < 0 || q >= cm.n) throw std::invalid_argument("hinge index out of range");
+    mesh.hmeta.assign(cm.hinge_meta, cm.hinge_meta + 3 * (size_t)cm.hg);
+    build_topology(mesh);
+    build_schwarz(mesh, 8, 1);
+    if (mesh.maxDomain > 8) throw std::runtime_error("Schwarz domain larger than 8 vertices");
+    for (int k = 0; k < 3; k++) gravity[k] = g ? g[k] : (k == 1 ? -9.81 : 0.0);
+    set_material(m);
+    const size_t n3 = 3 * (size_t)cm.n;
+    idx.upload(mesh.idx.data(), mesh.idx.size(), stream);
+    inv.alloc(cm.m);
+    if (cm.m) CK(cudaMemcpyAsync(inv.p, mesh.inv.data(), (size_t)cm.m * 16, cudaMemcpyHostToDevice, stream));
+    area.upload(mesh.area.data(), cm.m, stream);
+    mass.upload(mesh.mass.data(), cm.n, stream);
+    hinge.alloc(std::max(cm.hg, 1));
+    if (cm.hg) CK(cudaMemcpyAsync(hinge.p, mesh.hinge.data(), (size_t)cm.hg * 16, cudaMemcpyHostToDevice, stream));
+    hmeta.upload(mesh.hmeta.data(), mesh.hmeta.size(), stream);
+    memOff.upload(mesh.memOff.data(), mesh.memOff.size(), stream);
+    memRec.upload(mesh.memRec.data(), mesh.memRec.size(), stream);
+    hinOff.upload(mesh.hinOff.data(), mesh.hinOff.size(), stream);
+    hinRec.alloc(std::max<size_t>(mesh.hinRec.size(), 1));
+    hinRec.upload(mesh.hinRec.data(), mesh.hinRec.size(), stream);
+    v2tOff.upload((const int*)mesh.v2tOff.data(), mesh.v2tOff.size(), stream);
+    v2t.alloc(std::max<size_t>(mesh.v2t.size(), 1));
+    v2t.upload((const int*)mesh.v2t.data(), mesh.v2t.size(), stream);
+    domStart.upload(mesh.domStart.data(), mesh.domStart.size(), stream);
+    domVerts.upload(mesh.domVerts.data(), mesh.domVerts.size(), stream);
+    domFlag.alloc(std::max(mesh.D, 1));
+    L.alloc((size_t)std::max(mesh.D, 1) * 576);
+    for (DBuf<double>* b : {&vx, &vv, &vx0, &vyHat, &vg, &vdiag, &vdx, &vr, &vz, &vp, &vAp, &vxt, &vcgrad, &vcHp})
+      b->alloc(n3);
+    CK(cudaMemsetAsync(vcgrad.p, 0, n3 * 8, stream));
+    CK(cudaMemsetAsync(vcHp.p, 0, n3 * 8, stream));
+    const size_t tcap = std::max(n3, (size_t)cm.m + (size_t)cm.hg);
+    for (DBuf<double>* b : {&T0, &T1, &T2, &T3}) b->alloc(tcap);
+    Tc.alloc(1);
+    elem.alloc(std::max<size_t>((size_t)cm.m * 18, 1));
+    helem.alloc(std::max<size_t>((size_t)cm.hg * 12, 1));
+    const int partStride = (int)((std::max(std::max(n3, (size_t)cm.m), (size_t)cm.hg) + kThreads - 1) / kThreads) + 1;
+    part.alloc((size_t)NPART * partStride);
+    scal.alloc(S_NSCALARS);
+    CK(cudaMemsetAsync(scal.p, 0, S_NSCALARS * 8, stream));
+    pinned.alloc(cm.n);
+    CK(cudaMemsetAsync(pinned.p, 0, cm.n, stream));
+    vx.upload(x, n3, stream);
+    if (v) vv.upload(v, n3, stream);
+    else CK(cudaMemsetAsync(vv.p, 0, n3 * 8, stream));
+    d = Dev{};
+    d.n = cm.n; d.m = cm.m; d.hg = cm.hg;
+    d.idx = idx.p; d.inv = inv.p; d.area = area.p; d.mass = mass.p; d.hinge = hinge.p; d.hmeta = hmeta.p;
+    d.memOff = memOff.p; d.memRec = memRec.p; d.hinOff = hinOff.p; d.hinRec = hinRec.p;
+    d.pinned = pinned.p;
+    d.x = vx.p; d.v = vv.p; d.x0 = vx0.p; d.yHat = vyHat.p; d.g = vg.p; d.diag = vdiag.p; d.dx = vdx.p;
+    d.r = vr.p; d.z = vz.p; d.p = vp.p; d.Ap = vAp.p; d.xt = vxt.p; d.cgrad = vcgrad.p; d.cHp = vcHp.p;
+    d.elem = elem.p; d.helem = helem.p; d.part = part.p; d.partStride = partStride; d.scal = scal.p;
+    d.D = mesh.D; d.domStart = domStart.p; d.domVerts = domVerts.p; d.v2tOff = v2tOff.p; d.v2t = v2t.p;
+    d.L = L.p; d.domFlag = domFlag.p;
+    d.T0 = T0.p; d.T1 = T1.p; d.T2 = T2.p; d.T3 = T3.p; d.Tc = Tc.p;
+    set_material(m);
+    for (int k = 0; k < 3; k++) d.gravity[k] = gravity[k];
+    pcgBlocks = pcg_grid_blocks(d);
+    upload_pins();
+    contact.reset();
+    CK(cudaStreamSynchronize(stream));
+    ready = true;
+  }
+
+  void set_pins(int k, const int* ids, const double* pos) {
+    for (int i = 0; i < k; i++)
+      if (ids[i] < 0 || ids[i] >= mesh.n) throw std::invalid_argument("pin id out of range");
+    pinIds.assign(ids, ids + k);
+    pinPos.assign(pos, pos + 3 * (size_t)k);
+    if (ready) upload_pins();
+  }
+
+  void upload_pins() {
+    std::vector<uint8_t> mask(mesh.n, 0);
+    for (int id : pinIds) mask[id] = 1;
+    CK(cudaMemcpyAsync(pinned.p, mask.data(), mesh.n, cudaMemcpyHostToDevice, stream));
+    const int k = (int)pinIds.size();
+    if (k) {
+      pinIdsD.upload(pinIds.data(), k, stream);
+      pinPosD.upload(pinPos.data(), 3 * (size_t)k, stream);
+    }
+    d.npins = k;
+    d.pinIds = pinIdsD.p;
+    d.pinPos = pinPosD.p;
+    CK(cudaStreamSynchronize(stream));  // host vectors above are temporaries
+  }
+
+  void read_scalars() {
+    CK(cudaMemcpyAsync(hscal, scal.p, S_NSCALARS * 8, cudaMemcpyDeviceToHost, stream));
+    CK(cudaStreamSynchronize(stream));
+  }
+
+  // One implicit-Euler step (newton.ts:27-232).
+  void step(double h) {
+    if (!ready) throw std::logic_error("CpuSolver not initialized");
+    d.h = h;
+    d.invH2 = 1 / (h * h);
+    for (int k = 0; k < 3; k++) d.gravity[k] = gravity[k];
+    d.precond = opts.precond == CS_PRECOND_SCHWARZ ? 1 : 0;
+    d.hasContact = contact ? 1 : 0;
+    int64_t& lc = launch_counter();
+    launch_predict(d, stream);
+    lc += 1 + (d.npins > 0);
+    if (contact) contact->begin_step_and_bisect(*this);
+    if (contact) contact->update_active_set(*this, d.x);
+    if (contact) contact->merit_energy(*this, d.x);
+    launch_energy(d, d.x, stream);
+    lc += 2;
+    const double beta = std::max(std::max(mat.stretch_warp, mat.stretch_weft), mat.shear) * mat.thickness * 0.1 + 1e-6;
+    launch_diag_init(d, beta, stream);
+    lc += 1;
+    read_scalars();
+    double energy = hscal[S_ENERGY_TRIAL];
+    double gradNorm = INFINITY, maxStrain = 0;
+    int pcgTotal = 0, used = 0, trials = 0;
+    bool converged = false;
+    for (int ni = 0; ni < opts.newton_iters; ni++) {
+      used = ni + 1;
+      if (contact) contact->gradient_terms(*this);  // active set, barrier+friction grad, diag estimate
+      launch_grad(d, stream);
+      lc += 3 + (d.kb > 0 && d.hg > 0);
+      read_scalars();
+      gradNorm = hscal[S_GRADNORM];
+      maxStrain = hscal[S_MAXSTRAIN];
+      if (!std::isfinite(gradNorm)) throw NonFinite();
+      if (gradNorm < opts.grad_tol) { converged = true; break; }
+      if (d.precond == 1) { launch_schwarz_factor(d, stream); lc += 1; }
+      if (prof) CK(cudaEventRecord(pev0, stream));
+      CK((cudaError_t)launch_pcg(d, opts.pcg_max_iters, 1e-3, pcgBlocks, stream));
+      if (prof) { CK(cudaEventRecord(pev1, stream)); profPending = true; }
+      lc += 1;
+      double alpha = 1;
+      bool accepted = false;
+      bool haveSlope = false;
+      double gtdx = 0;
+      for (int li = 0; li < opts.ls_iters; li++) {
+        trials++;
+        launch_trial(d, alpha, stream);
+        lc += 1 + (d.npins > 0);
+        if (contact && !contact->check_trial(*this, d.xt)) {
+          contact->rejections++;
+          alpha *= 0.5;
+          continue;
+        }
+        if (contact) contact->merit_energy(*this, d.xt);
+        launch_energy(d, d.xt, stream);
+        lc += 2;
+        read_scalars();
+        if (!haveSlope) {
+          gtdx = hscal[S_GTDX];
+          pcgTotal += (int)hscal[S_PCG_ITERS];
+          prof_collect((int)hscal[S_PCG_ITERS]);
+          haveSlope = true;
+        }
+        const double eNew = hscal[S_ENERGY_TRIAL];
+        if (!std::isfinite(eNew)) {
+          if (contact) contact->rejections++;
+          alpha *= 0.5;
+          continue;
+        }
+        if (eNew <= energy + 1e-4 * alpha * gtdx) {
+          std::swap(d.x, d.xt);
+          energy = eNew;
+          accepted = true;
+          if (contact) contact->commit(*this, d.x);
+          break;
+        }
+        if (contact) contact->rejections++;
+        alpha *= 0.5;
+      }
+      if (!haveSlope) {
+        read_scalars();
+        pcgTotal += (int)hscal[S_PCG_ITERS];
+        prof_collect((int)hscal[S_PCG_ITERS]);
+      }
+      if (!accepted) break;
+      if (alpha < 1e-6) break;
+    }
+    const double damp = 1 - std::min(std::max(mat.damping, 0.0), 0.1);
+    launch_velocity(d, damp, stream);
+    lc += 1;
+    if (contact) contact->kill_approach_velocity(*this);
+    launch_pins(d, d.x, stream);
+    lc += (d.npins > 0);
+    // keep the state in the primary buffer
+    if (d.x != vx.p) {
+      CK(cudaMemcpyAsync(vx.p, d.x, 3 * (size_t)mesh.n * 8, cudaMemcpyDeviceToDevice, stream));
+      d.xt = d.x;
+      d.x = vx.p;
+    }
+    stats = cs_step_stats{};
+    stats.newton_iters = opts.newton_iters;
+    stats.pcg_iters = pcgTotal;
+    stats.grad_norm = gradNorm;
+    stats.energy = energy;
+    stats.max_strain = maxStrain;
+    stats.converged = converged;
+    stats.has_contact = contact ? 1 : 0;
+    stats.newton_iters_used = used;
+    stats.armijo_trials = trials;
+    if (contact) contact->fill_stats(*this, stats);
+    haveStats = true;
+  }
+
+  void get(double* out, bool vel) {
+    CK(cudaMemcpyAsync(out, vel ? d.v : d.x, 3 * (size_t)mesh.n * 8, cudaMemcpyDeviceToHost, stream));
+    CK(cudaStreamSynchronize(stream));
+  }
+  void set_state(const double* x, const double* v) {
+    if (x) CK(cudaMemcpyAsync(d.x, x, 3 * (size_t)mesh.n * 8, cudaMemcpyHostToDevice, stream));
+    if (v) CK(cudaMemcpyAsync(d.v, v, 3 * (size_t)mesh.n * 8, cudaMemcpyHostToDevice, stream));
+    CK(cudaStreamSynchronize(stream));
+  }
+};
+
+}  // namespace cs
+

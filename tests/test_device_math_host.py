@@ -1,0 +1,99 @@
+"""The device contact primitives (closim_b200/csrc/contact_math.cuh and
+jsmath.cuh), compiled for the host, agree bit for bit with the oracle on
+random and edge-case inputs. Catches porting slips without a GPU."""
+import ctypes as C
+import math
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "hostcheck", "libhostcheck.so")
+
+
+@pytest.fixture(scope="module")
+def hc():
+    if not os.path.exists(LIB):
+        subprocess.run(["make", "-s", "-C", os.path.join(HERE, "hostcheck")], check=True)
+    L = C.CDLL(LIB)
+    d = C.c_double
+    p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+    for name, res, args in [("hc_js_acos", d, [d]), ("hc_js_log", d, [d]), ("hc_js_cbrt", d, [d]),
+                            ("hc_hypot3", d, [d, d, d]), ("hc_closest_vt", None, [p, p]),
+                            ("hc_closest_ee", None, [p, p]), ("hc_vt_ccd", d, [p, p, d]), ("hc_ee_ccd", d, [p, p, d]),
+                            ("hc_solve_cubic01", C.c_int, [d, d, d, d, p]), ("hc_barrier_value", d, [d, d]),
+                            ("hc_barrier_grad", d, [d, d, d]), ("hc_barrier_curv", d, [d, d, d])]:
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    return L
+
+
+def same(a, b):
+    return (a == b) or (math.isnan(a) and math.isnan(b))
+
+
+def test_js_math_matches_oracle(hc):
+    ol = O.lib()
+    for f in ["orc_js_acos", "orc_js_log", "orc_js_cbrt"]:
+        getattr(ol, f).restype = C.c_double
+        getattr(ol, f).argtypes = [C.c_double]
+    rng = np.random.default_rng(5)
+    xs = list(rng.uniform(-1, 1, 3000)) + list(np.exp(rng.uniform(-700, 700, 3000))) + \
+        [0.0, -0.0, 1.0, -1.0, 5e-324, 1e-310, math.inf, -math.inf, math.nan, 1 - 1e-16, -1 + 1e-16]
+    for x in xs:
+        assert same(hc.hc_js_acos(x), ol.orc_js_acos(x)), x
+        assert same(hc.hc_js_log(x), ol.orc_js_log(x)), x
+        assert same(hc.hc_js_cbrt(x), ol.orc_js_cbrt(x)), x
+        assert same(hc.hc_js_cbrt(-x), ol.orc_js_cbrt(-x)), x
+
+
+def _random_stencils(rng, k, scale):
+    base = rng.uniform(-scale, scale, (k, 4, 3))
+    move = base + rng.normal(0, scale * 0.3, (k, 4, 3)) * rng.integers(0, 2, (k, 1, 1))
+    return base, move
+
+
+def test_closest_points_match_oracle(hc):
+    rng = np.random.default_rng(1)
+    for _ in range(3000):
+        q = rng.uniform(-1, 1, 12) * rng.choice([1e-3, 1.0])
+        o1 = np.zeros(6)
+        hc.hc_closest_vt(q, o1)
+        assert np.array_equal(o1, O.closest_vt(q[0:3], q[3:6], q[6:9], q[9:12]))
+        hc.hc_closest_ee(q, o1)
+        assert np.array_equal(o1, O.closest_ee(q[0:3], q[3:6], q[6:9], q[9:12]))
+
+
+def test_ccd_matches_oracle(hc):
+    rng = np.random.default_rng(2)
+    hits = 0
+    for _ in range(3000):
+        P0, P1 = _random_stencils(rng, 1, 0.01)
+        P0 = np.ascontiguousarray(P0.ravel())
+        P1 = np.ascontiguousarray(P1.ravel())
+        for th in (1e-4, 2e-3):
+            a = hc.hc_vt_ccd(P0, P1, th)
+            b = O.vt_ccd(P0, P1, th)
+            assert same(a, b), (a, b)
+            c = hc.hc_ee_ccd(P0, P1, th)
+            d = O.ee_ccd(P0, P1, th)
+            assert same(c, d), (c, d)
+            hits += (0 < a < 1) + (0 < c < 1)
+    assert hits > 0
+
+
+def test_cubic_and_barrier_match_oracle(hc):
+    rng = np.random.default_rng(3)
+    o = np.zeros(3)
+    for _ in range(5000):
+        a = rng.normal(0, 1, 4) * rng.choice([1e-14, 1e-6, 1.0], 4)
+        k = hc.hc_solve_cubic01(*a, o)
+        assert list(o[:k]) == O.solve_cubic01(*a)
+    for d in np.concatenate([rng.uniform(0, 2e-3, 2000), [1e-12, 1e-13, 2e-3, 5e-3, 0.0]]):
+        assert same(hc.hc_barrier_value(d, 2e-3), O.barrier_value(d, 2e-3))
+        assert same(hc.hc_barrier_grad(d, 2e-3, 50.0), O.lib().orc_barrier_grad_scalar(d, 2e-3, 50.0, 1.0))
