@@ -46,7 +46,7 @@ class cs_step_stats(C.Structure):
 
 EXPORTS = ["cs_create", "cs_destroy", "cs_last_error", "cs_initialize", "cs_set_contact",
            "cs_set_stepper_options", "cs_set_material", "cs_set_pins", "cs_step", "cs_get_positions",
-           "cs_get_velocities", "cs_set_state", "cs_last_stats", "cs_step_n", "cs_sync",
+           "cs_get_velocities", "cs_set_state", "cs_last_stats", "cs_membrane_hvp", "cs_step_n", "cs_sync",
            "cs_kernel_launches", "cs_stream", "cs_profile", "cs_profile_read", "cs_build_grid",
            "cs_preprocess"]
 
@@ -79,6 +79,7 @@ def load():
         "cs_get_velocities": (C.c_int, [vp, vp]),
         "cs_set_state": (C.c_int, [vp, vp, vp]),
         "cs_last_stats": (C.c_int, [vp, C.POINTER(cs_step_stats)]),
+        "cs_membrane_hvp": (C.c_int, [vp, vp, vp, vp]),
         "cs_sync": (C.c_int, [vp]),
         "cs_kernel_launches": (C.c_int64, [vp]),
         "cs_stream": (vp, [vp]),

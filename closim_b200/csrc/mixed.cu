@@ -1,0 +1,527 @@
+// Mixed-precision path of the Newton step (FP32 linear solve, FP64 where it
+// matters). Compiled with FMA contraction on.
+//
+// Per Newton iteration the membrane state of every triangle is evaluated once
+// in FP64 (deformation gradient F, 2nd Piola stress S) and stored as FP32, so
+// the PCG's matrix-free HVP is the exact directional derivative of the
+// gradient (src/physics/membrane-hvp.ts:18-75) at ~60 FP32 flops and 64 bytes
+// per triangle. PCG vectors are FP32; every dot product and norm accumulates
+// in FP64 through a fixed-order two-level tree (deterministic). The one-level
+// Schwarz preconditioner (src/solver/schwarz.ts) is assembled and factored in
+// FP64 and applied as an FP32 dense inverse per domain, one warp per domain.
+// Gradient, energies, contact and CCD stay on the FP64 kernels.
+#include "contact.cuh"
+#include "mixed.cuh"
+
+namespace cs {
+
+static inline int mblk(long n) { return (int)((n + kThreads - 1) / kThreads); }
+
+__device__ __forceinline__ void ld3(const double* x, int v, double o[3]) {
+  o[0] = x[v * 3]; o[1] = x[v * 3 + 1]; o[2] = x[v * 3 + 2];
+}
+
+// ---- per-triangle membrane state (F, S) and the 9x9 block -------------------------
+// tris: 16 floats per triangle: F00 F10 F20 F01 F11 F21, S00 S11 S01, a b c d, s, pad x2
+__global__ void __launch_bounds__(kThreads) k_mx_tristate(Dev d, MixBufs mb) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= d.m) return;
+  double x0[3], x1[3], x2[3];
+  ld3(d.x, d.idx[t * 3], x0); ld3(d.x, d.idx[t * 3 + 1], x1); ld3(d.x, d.idx[t * 3 + 2], x2);
+  const float4 iv = d.inv[t];
+  const double a = iv.x, b = iv.y, c = iv.z, dd = iv.w;
+  const double e1[3] = {x1[0] - x0[0], x1[1] - x0[1], x1[2] - x0[2]};
+  const double e2[3] = {x2[0] - x0[0], x2[1] - x0[1], x2[2] - x0[2]};
+  double F0[3], F1[3];
+  for (int i = 0; i < 3; i++) { F0[i] = a * e1[i] + c * e2[i]; F1[i] = b * e1[i] + dd * e2[i]; }
+  const double E00 = 0.5 * (F0[0] * F0[0] + F0[1] * F0[1] + F0[2] * F0[2] - 1);
+  const double E11 = 0.5 * (F1[0] * F1[0] + F1[1] * F1[1] + F1[2] * F1[2] - 1);
+  const double E01 = 0.5 * (F0[0] * F1[0] + F0[1] * F1[1] + F0[2] * F1[2]);
+  const Mat<double>& m = d.mat;
+  float* o = mb.tris + (size_t)t * 16;
+  for (int i = 0; i < 3; i++) { o[i] = (float)F0[i]; o[3 + i] = (float)F1[i]; }
+  o[6] = (float)(m.C00 * E00 + m.C01 * E11);
+  o[7] = (float)(m.C11 * E11 + m.C01 * E00);
+  o[8] = (float)(2 * m.G * E01);
+  o[9] = iv.x; o[10] = iv.y; o[11] = iv.z; o[12] = iv.w;
+  o[13] = (float)(m.thickness * (double)d.area[t]);
+  o[14] = 0.f; o[15] = 0.f;
+}
+
+// Full 9x9 membrane block per triangle (FP64 closed form), stored FP32.
+__global__ void __launch_bounds__(kThreads) k_mx_h9(Dev d, MixBufs mb) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= d.m) return;
+  double x0[3], x1[3], x2[3];
+  ld3(d.x, d.idx[t * 3], x0); ld3(d.x, d.idx[t * 3 + 1], x1); ld3(d.x, d.idx[t * 3 + 2], x2);
+  const float4 iv = d.inv[t];
+  double h[81];
+  tri_hessian9_rows<double>(x0, x1, x2, iv.x, iv.y, iv.z, iv.w, d.area[t], d.mat, 0, 9, h);
+  float* o = mb.h9 + (size_t)t * 81;
+  for (int k = 0; k < 81; k++) o[k] = (float)h[k];
+}
+
+// Schwarz factor: assemble (FP64 sums of the stored blocks + Jacobi diagonal),
+// symmetrize, Cholesky; store A^-1 = L^-T L^-1 as FP32 (Jacobi inverse on failure).
+constexpr int kMxWarps = 4;
+__global__ void __launch_bounds__(kMxWarps * 32) k_mx_schwarz_factor(Dev d, MixBufs mb) {
+  __shared__ double A[kMxWarps][24 * 24];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int dom = blockIdx.x * kMxWarps + wib;
+  if (dom >= d.D) return;
+  double* a = A[wib];
+  const int start = d.domStart[dom], dv = d.domStart[dom + 1] - start, dw = dv * 3;
+  for (int i = lane; i < 24 * 24; i += 32) a[i] = 0;
+  __syncwarp();
+  if (lane < dv) {
+    const int v = d.domVerts[start + lane];
+    for (int k = d.v2tOff[v]; k < d.v2tOff[v + 1]; k++) {
+      const int t = d.v2t[k];
+      const int cvs[3] = {(int)d.idx[t * 3], (int)d.idx[t * 3 + 1], (int)d.idx[t * 3 + 2]};
+      const int ci = cvs[0] == v ? 0 : cvs[1] == v ? 1 : 2;
+      const float* h = mb.h9 + (size_t)t * 81;
+      for (int cj = 0; cj < 3; cj++) {
+        int lw = -1;
+        for (int q = 0; q < dv; q++)
+          if (d.domVerts[start + q] == cvs[cj]) { lw = q; break; }
+        if (lw < 0) continue;
+        for (int aa = 0; aa < 3; aa++)
+          for (int bb = 0; bb < 3; bb++) a[(lane * 3 + aa) * dw + lw * 3 + bb] += h[(ci * 3 + aa) * 9 + cj * 3 + bb];
+      }
+    }
+  }
+  __syncwarp();
+  if (lane < dw) a[lane * dw + lane] += d.diag[d.domVerts[start + lane / 3] * 3 + lane % 3];
+  __syncwarp();
+  for (int i = lane; i < dw; i += 32)
+    for (int j = i + 1; j < dw; j++) {
+      const double s = 0.5 * (a[i * dw + j] + a[j * dw + i]);
+      a[i * dw + j] = s;
+      a[j * dw + i] = s;
+    }
+  __syncwarp();
+  double scale = 0;
+  for (int i = 0; i < dw; i++) scale = fmax(scale, fabs(a[i * dw + i]));
+  const double tiny = 1e-20 * (1 + scale);
+  bool ok = true;
+  for (int k = 0; k < dw; k++) {
+    if (lane == 0) {
+      double sum = a[k * dw + k];
+      for (int s = 0; s < k; s++) sum -= a[k * dw + s] * a[k * dw + s];
+      ok = sum > tiny;
+      if (ok) a[k * dw + k] = sqrt(sum);
+    }
+    ok = __shfl_sync(0xffffffffu, ok, 0);
+    __syncwarp();
+    if (!ok) break;
+    if (lane > k && lane < dw) {
+      double s2 = a[lane * dw + k];
+      for (int s = 0; s < k; s++) s2 -= a[lane * dw + s] * a[k * dw + s];
+      a[lane * dw + k] = s2 / a[k * dw + k];
+    }
+    __syncwarp();
+  }
+  float* Li = mb.Linv + (size_t)dom * 576;
+  if (!ok) {
+    for (int i = lane; i < 24; i += 32)
+      for (int j = 0; j < 24; j++) {
+        double v = 0;
+        if (i == j && i < dw) {
+          const double dd = d.diag[d.domVerts[start + i / 3] * 3 + i % 3];
+          v = dd > 1e-12 ? 1 / dd : 0.0;
+        }
+        Li[i * 24 + j] = (float)v;
+      }
+    return;
+  }
+  // column j of L^-1 by forward substitution (lane j), kept in registers
+  double col[24];
+  for (int i = 0; i < 24; i++) col[i] = 0;
+  if (lane < dw) {
+    for (int i = 0; i < dw; i++) {
+      double s = i == lane ? 1.0 : 0.0;
+      for (int k = 0; k < i; k++) s -= a[i * dw + k] * col[k];
+      col[i] = i < lane ? 0.0 : s / a[i * dw + i];
+    }
+  }
+  __syncwarp();
+  // overwrite the upper triangle region with L^-1 columns: reuse a[] as Linv (row-major)
+  // (L is no longer needed after every lane finished its column)
+  for (int i = 0; i < dw; i++) {
+    const double v = lane < dw ? col[i] : 0.0;
+    __syncwarp();
+    if (lane < dw) a[i * dw + lane] = v;  // a = L^-1
+    __syncwarp();
+  }
+  // A^-1[i][j] = sum_k Linv[k][i] Linv[k][j]; lane i writes row i
+  if (lane < 24) {
+    for (int j = 0; j < 24; j++) {
+      double s = 0;
+      if (lane < dw && j < dw)
+        for (int k = 0; k < dw; k++) s += a[k * dw + lane] * a[k * dw + j];
+      Li[lane * 24 + j] = (float)s;
+    }
+  }
+}
+
+// ---- PCG (pcg.ts:11-95) in FP32 with FP64 reductions, + newton.ts:152-179 --------------
+struct MxArgs {
+  Dev d;
+  MixBufs mb;
+  int maxIters;
+  double tol;
+};
+
+__device__ __forceinline__ double mx_total(const Dev& d, int row, double* bc) {
+  if (threadIdx.x < 32) {
+    const double s = warp_sum_partials(d.part + row * d.partStride, gridDim.x);
+    if (threadIdx.x == 0) bc[0] = s;
+  }
+  __syncthreads();
+  const double r = bc[0];
+  __syncthreads();
+  return r;
+}
+__device__ __forceinline__ void mx_put(const Dev& d, int row, double v, double* sm) {
+  const double b = block_sum(v, sm);
+  if (threadIdx.x == 0) d.part[row * d.partStride + blockIdx.x] = b;
+}
+
+// z = A_d^-1 r on every domain, one warp per domain, lane = local dof.
+__device__ __forceinline__ double mx_schwarz(const Dev& d, const MixBufs& mb, int gwarp, int nwarps) {
+  const int lane = threadIdx.x & 31;
+  double rz = 0;
+  for (int dom = gwarp; dom < d.D; dom += nwarps) {
+    const int start = d.domStart[dom], dv = d.domStart[dom + 1] - start, dw = dv * 3;
+    float rv = 0.f;
+    int gi = -1;
+    if (lane < dw) {
+      gi = d.domVerts[start + lane / 3] * 3 + lane % 3;
+      rv = mb.r[gi];
+    }
+    const float* Li = mb.Linv + (size_t)dom * 576 + lane * 24;
+    float z = 0.f;
+    for (int j = 0; j < 24; j++) {
+      const float rj = __shfl_sync(0xffffffffu, rv, j);
+      if (lane < dw) z = fmaf(Li[j], rj, z);
+    }
+    if (lane < dw) {
+      if (d.pinned[gi / 3]) z = 0.f;
+      mb.z[gi] = z;
+      rz += (double)rv * (double)z;
+    }
+  }
+  return rz;
+}
+
+__global__ void __launch_bounds__(kThreads) k_mx_pcg(MxArgs A) {
+  cg::grid_group grid = cg::this_grid();
+  __shared__ double sm[32];
+  __shared__ double bc[2];
+  const Dev& d = A.d;
+  const MixBufs& mb = A.mb;
+  const int n3 = d.n * 3;
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+  const int gwarp = tid >> 5, nwarps = nth >> 5;
+  const bool jacobi = d.precond == 0;
+  const float invH2 = (float)d.invH2;
+  double bb = 0, rr = 0, rz0 = 0;
+  for (int i = tid; i < n3; i += nth) {
+    const double bi = -d.g[i];
+    bb += bi * bi;
+    const float ri = d.pinned[i / 3] ? 0.f : (float)bi;
+    mb.r[i] = ri;
+    mb.x[i] = 0.f;
+    rr += (double)ri * ri;
+    if (jacobi) {
+      float zi = d.diag[i] > 1e-12 ? (float)((double)ri / d.diag[i]) : ri;
+      if (d.pinned[i / 3]) zi = 0.f;
+      mb.z[i] = zi;
+      mb.p[i] = zi;
+      rz0 += (double)ri * zi;
+    }
+  }
+  mx_put(d, 0, bb, sm);
+  mx_put(d, 1, rr, sm);
+  if (jacobi) mx_put(d, 2, rz0, sm);
+  grid.sync();
+  if (!jacobi) {
+    const double rzp = mx_schwarz(d, mb, gwarp, nwarps);
+    mx_put(d, 2, rzp, sm);
+    grid.sync();
+    for (int i = tid; i < n3; i += nth) mb.p[i] = mb.z[i];
+  }
+  double rz = mx_total(d, 2, bc);
+  const double bNorm = sqrt(mx_total(d, 0, bc));
+  const double absTol = fmax(A.tol * fmax(bNorm, 1e-12), 1e-12);
+  double residual = sqrt(mx_total(d, 1, bc));
+  int iters = 0;
+  bool done = residual < absTol;
+  if (!done) grid.sync();
+  int k = 0;
+  for (; !done && k < A.maxIters; k++) {
+    // element HVP from the stored (F, S): dF = Ds(p) Dm^-1, dE, dS, dP = dF S + F dS
+    for (int t = tid; t < d.m; t += nth) {
+      const float* T = mb.tris + (size_t)t * 16;
+      const float4 t0 = *(const float4*)T, t1 = *(const float4*)(T + 4), t2 = *(const float4*)(T + 8),
+                   t3 = *(const float4*)(T + 12);
+      const float F0[3] = {t0.x, t0.y, t0.z}, F1[3] = {t0.w, t1.x, t1.y};
+      const float S00 = t1.z, S11 = t1.w, S01 = t2.x;
+      const float a = t2.y, b = t2.z, c = t2.w, dd = t3.x, s = t3.y;
+      const uint32_t i0 = d.idx[t * 3], i1 = d.idx[t * 3 + 1], i2 = d.idx[t * 3 + 2];
+      float w1[3], w2[3];
+      for (int q = 0; q < 3; q++) {
+        const float p0 = mb.p[i0 * 3 + q];
+        w1[q] = mb.p[i1 * 3 + q] - p0;
+        w2[q] = mb.p[i2 * 3 + q] - p0;
+      }
+      float dF0[3], dF1[3];
+      for (int q = 0; q < 3; q++) { dF0[q] = a * w1[q] + c * w2[q]; dF1[q] = b * w1[q] + dd * w2[q]; }
+      const float dE00 = F0[0] * dF0[0] + F0[1] * dF0[1] + F0[2] * dF0[2];
+      const float dE11 = F1[0] * dF1[0] + F1[1] * dF1[1] + F1[2] * dF1[2];
+      const float dE01 = 0.5f * (dF0[0] * F1[0] + F0[0] * dF1[0] + dF0[1] * F1[1] + F0[1] * dF1[1] +
+                                 dF0[2] * F1[2] + F0[2] * dF1[2]);
+      const float dS00 = mb.C00 * dE00 + mb.C01 * dE11;
+      const float dS11 = mb.C11 * dE11 + mb.C01 * dE00;
+      const float dS01 = 2.f * mb.G * dE01;
+      float* o = mb.elem + (size_t)t * 9;
+      for (int q = 0; q < 3; q++) {
+        const float P0 = dF0[q] * S00 + F0[q] * dS00 + dF1[q] * S01 + F1[q] * dS01;
+        const float P1 = dF0[q] * S01 + F0[q] * dS01 + dF1[q] * S11 + F1[q] * dS11;
+        const float g1 = s * (P0 * a + P1 * b);
+        const float g2 = s * (P0 * c + P1 * dd);
+        o[q] = -(g1 + g2);
+        o[3 + q] = g1;
+        o[6 + q] = g2;
+      }
+    }
+    if (d.hasContact) {
+      // frozen-barrier coefficients in FP64 (contact-assembly.ts:371-387)
+      const Contact& c = d.c;
+      for (int i = tid; i < c.nActive; i += nth) {
+        const Frozen f = c.active[i];
+        const double dist = js_max(frozen_dist(c, d.x, f), 1e-12);
+        double jv;
+        if (f.kind == 2) jv = mb.p[f.p * 3 + 1];
+        else {
+          double v[4][3] = {};
+          const int ids[4] = {f.kind == 0 ? f.p : f.a, f.kind == 0 ? f.a : f.b, f.kind == 0 ? f.b : f.c,
+                              f.kind == 0 ? f.c : f.d};
+          for (int q = 0; q < 4; q++)
+            if (ids[q] >= 0)
+              for (int e = 0; e < 3; e++) v[q][e] = mb.p[ids[q] * 3 + e];
+          const double nv[4] = {f.nx * v[0][0] + f.ny * v[0][1] + f.nz * v[0][2],
+                                f.nx * v[1][0] + f.ny * v[1][1] + f.nz * v[1][2],
+                                f.nx * v[2][0] + f.ny * v[2][1] + f.nz * v[2][2],
+                                f.nx * v[3][0] + f.ny * v[3][1] + f.nz * v[3][2]};
+          if (f.kind == 0) jv = nv[0] - f.w0 * nv[1] - f.w1 * nv[2] - f.w2 * nv[3];
+          else jv = f.w0 * nv[0] + f.w1 * nv[1] + f.w2 * nv[2] + f.w3 * nv[3];
+        }
+        c.dd[i] = dist < c.dHat ? barrier_curvature(dist, c.dHat, c.kappa) * jv : 0.0;
+      }
+    }
+    grid.sync();
+    double pAp = 0;
+    for (int v = tid; v < d.n; v += nth) {
+      float sp[3] = {0.f, 0.f, 0.f};
+      for (uint32_t q = d.memOff[v]; q < d.memOff[v + 1]; q++) {
+        const uint32_t rec = d.memRec[q];
+        const float* e = mb.elem + (size_t)(rec >> 2) * 9 + (rec & 3) * 3;
+        sp[0] += e[0]; sp[1] += e[1]; sp[2] += e[2];
+      }
+      double ch[3] = {0, 0, 0};
+      if (d.hasContact) contact_hvp_gather(d, v, ch);
+      const float M = d.mass[v];
+      const bool pin = d.pinned[v];
+      for (int q = 0; q < 3; q++) {
+        const int i = v * 3 + q;
+        float ap = M * mb.p[i] * invH2 + sp[q] + (float)ch[q];
+        if (pin) ap = 0.f;
+        mb.Ap[i] = ap;
+        pAp += (double)mb.p[i] * ap;
+      }
+    }
+    mx_put(d, 3, pAp, sm);
+    grid.sync();
+    const double pApT = mx_total(d, 3, bc);
+    if (!(pApT > 1e-30)) { iters = k; done = true; break; }
+    const float alpha = (float)(rz / pApT);
+    double rrn = 0, rzn = 0;
+    for (int i = tid; i < n3; i += nth) {
+      const bool pin = d.pinned[i / 3];
+      float xi = mb.x[i] + alpha * mb.p[i];
+      float ri = mb.r[i] - alpha * mb.Ap[i];
+      if (pin) { xi = 0.f; ri = 0.f; }
+      mb.x[i] = xi;
+      mb.r[i] = ri;
+      rrn += (double)ri * ri;
+      if (jacobi) {
+        float zi = d.diag[i] > 1e-12 ? (float)((double)ri / d.diag[i]) : ri;
+        if (pin) zi = 0.f;
+        mb.z[i] = zi;
+        rzn += (double)ri * zi;
+      }
+    }
+    mx_put(d, 4, rrn, sm);
+    if (jacobi) mx_put(d, 5, rzn, sm);
+    grid.sync();
+    residual = sqrt(mx_total(d, 4, bc));
+    if (residual < absTol) { iters = k + 1; done = true; break; }
+    if (!jacobi) {
+      const double rzp = mx_schwarz(d, mb, gwarp, nwarps);
+      mx_put(d, 5, rzp, sm);
+      grid.sync();
+    }
+    const double rzNew = mx_total(d, 5, bc);
+    const float beta = (float)(rzNew / rz);
+    for (int i = tid; i < n3; i += nth) mb.p[i] = mb.z[i] + beta * mb.p[i];
+    rz = rzNew;
+    grid.sync();
+  }
+  if (!done) iters = A.maxIters;
+  grid.sync();
+  // descent safeguard + trust region in FP64 (dx kept in d.dx)
+  double gt = 0;
+  for (int i = tid; i < n3; i += nth) {
+    const double di = mb.x[i];
+    d.dx[i] = di;
+    gt += d.g[i] * di;
+  }
+  mx_put(d, 6, gt, sm);
+  grid.sync();
+  double gtdx = mx_total(d, 6, bc);
+  bool fallback = false;
+  if (!isfinite(gtdx) || gtdx >= 0) {
+    fallback = true;
+    gt = 0;
+    for (int i = tid; i < n3; i += nth) {
+      const double di = -d.g[i] / d.diag[i];
+      d.dx[i] = di;
+      gt += d.g[i] * di;
+    }
+    mx_put(d, 7, gt, sm);
+    grid.sync();
+    gtdx = mx_total(d, 7, bc);
+  }
+  double mxd = 0;
+  for (int i = tid; i < n3; i += nth) {
+    const double a = fabs(d.dx[i]);
+    if (a > mxd) mxd = a;
+  }
+  // max over the grid (exact in any order)
+  {
+    double v = mxd;
+    for (int o = 16; o > 0; o >>= 1) {
+      const double w = __shfl_down_sync(0xffffffffu, v, o);
+      if (w > v) v = w;
+    }
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double r = 0;
+      for (int i = 0; i < (int)(blockDim.x >> 5); i++) if (sm[i] > r) r = sm[i];
+      d.part[0 * d.partStride + blockIdx.x] = r;
+    }
+  }
+  grid.sync();
+  if (threadIdx.x == 0) {
+    double r = 0;
+    for (int i = 0; i < (int)gridDim.x; i++) {
+      const double v = d.part[i];
+      if (v > r) r = v;
+    }
+    bc[0] = r;
+  }
+  __syncthreads();
+  const double maxDx = bc[0];
+  if (maxDx > 0.002) {
+    const double s = 0.002 / maxDx;
+    for (int i = tid; i < n3; i += nth) d.dx[i] *= s;
+    gtdx *= s;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    d.scal[S_PCG_ITERS] = iters;
+    d.scal[S_PCG_RES] = residual;
+    d.scal[S_GTDX] = gtdx;
+    d.scal[S_FALLBACK] = fallback ? 1 : 0;
+    d.scal[S_MAXDX] = maxDx;
+  }
+}
+
+// ---- FP64 reductions as trees (the gradient norm and the Armijo energy) ----------------
+__global__ void __launch_bounds__(kThreads) k_mx_sum_terms(const double* t, int n, double* part) {
+  __shared__ double sm[32];
+  double s = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) s += t[i];
+  const double b = block_sum(s, sm);
+  if (threadIdx.x == 0) part[blockIdx.x] = b;
+}
+__global__ void k_mx_grad_final(Dev d, int nbT, int nbG) {
+  if (threadIdx.x >= 32) return;
+  const double ms = warp_max_partials(d.part + 0 * d.partStride, nbT);
+  const double gs = warp_sum_partials(d.part + 1 * d.partStride, nbG);
+  if (threadIdx.x == 0) {
+    d.scal[S_GRADNORM] = sqrt(gs);
+    d.scal[S_MAXSTRAIN] = ms;
+  }
+}
+__global__ void k_mx_energy_final(Dev d, int nb) {
+  if (threadIdx.x >= 32) return;
+  const double ei = warp_sum_partials(d.part + 2 * d.partStride, nb);
+  const double et = warp_sum_partials(d.part + 3 * d.partStride, nb);
+  const double em = warp_sum_partials(d.part + 4 * d.partStride, nb);
+  if (threadIdx.x == 0) {
+    d.scal[S_E_INERTIA] = ei;
+    d.scal[S_E_TRI] = et;
+    d.scal[S_E_MERIT] = em;
+    double e = ei + et;
+    if (d.hasContact) e += em;
+    d.scal[S_ENERGY_TRIAL] = e;
+  }
+}
+
+// ---- launchers ---------------------------------------------------------------------------
+void mx_prepare(const Dev& d, const MixBufs& mb, bool schwarz, cudaStream_t s, int64_t* lc) {
+  k_mx_tristate<<<mblk(d.m), kThreads, 0, s>>>(d, mb);
+  *lc += 1;
+  if (schwarz) {
+    k_mx_h9<<<mblk(d.m), kThreads, 0, s>>>(d, mb);
+    k_mx_schwarz_factor<<<(d.D + kMxWarps - 1) / kMxWarps, kMxWarps * 32, 0, s>>>(d, mb);
+    *lc += 2;
+  }
+}
+int mx_pcg_grid_blocks(const Dev& d) {
+  int dev = 0, sms = 0, per = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_mx_pcg, kThreads, 0);
+  const int want = mblk(std::max(d.n * 3, d.m));
+  int cap = per * sms;
+  if (cap < 1) cap = 1;
+  return std::max(1, std::min(want, std::min(cap, d.partStride)));
+}
+int mx_launch_pcg(const Dev& d, const MixBufs& mb, int maxIters, double tol, int blocks, cudaStream_t s) {
+  MxArgs a{d, mb, maxIters, tol};
+  void* args[] = {&a};
+  return (int)cudaLaunchCooperativeKernel((void*)k_mx_pcg, dim3(blocks), dim3(kThreads), args, 0, s);
+}
+// Gradient norm from the T0 terms the gather wrote (tree instead of chain).
+void mx_grad_final(const Dev& d, cudaStream_t s, int64_t* lc) {
+  const int nbG = std::min(mblk(d.n * 3), d.partStride);
+  k_mx_sum_terms<<<nbG, kThreads, 0, s>>>(d.T0, d.n * 3, d.part + 1 * d.partStride);
+  k_mx_grad_final<<<1, 32, 0, s>>>(d, mblk(d.m), nbG);
+  *lc += 2;
+}
+// Armijo energy from the T0 / T1 / Tc terms (tree sums).
+void mx_energy_final(const Dev& d, cudaStream_t s, int64_t* lc) {
+  const int nb = std::min(mblk(std::max(std::max(d.n * 3, d.m + d.hg), d.hasContact ? d.c.nActive : 0)),
+                          d.partStride);
+  k_mx_sum_terms<<<nb, kThreads, 0, s>>>(d.T0, d.n * 3, d.part + 2 * d.partStride);
+  k_mx_sum_terms<<<nb, kThreads, 0, s>>>(d.T1, d.m + (d.kb > 0 ? d.hg : 0), d.part + 3 * d.partStride);
+  k_mx_sum_terms<<<nb, kThreads, 0, s>>>(d.Tc, d.hasContact ? d.c.nActive : 0, d.part + 4 * d.partStride);
+  k_mx_energy_final<<<1, 32, 0, s>>>(d, nb);
+  *lc += 4;
+}
+
+}  // namespace cs

@@ -1,0 +1,22 @@
+// Mixed-precision path: FP32 PCG buffers and launchers (mixed.cu).
+#pragma once
+#include "plain.cuh"
+
+namespace cs {
+
+struct MixBufs {
+  float *r, *z, *p, *Ap, *x;   // 3n each
+  float* elem;                 // 9m element HVP terms
+  float* tris;                 // 16m per-triangle F, S, Dm^-1, thickness * area
+  float* h9;                   // 81m 9x9 blocks (Schwarz assembly)
+  float* Linv;                 // D x 576 dense inverses
+  float C00, C11, C01, G;
+};
+
+void mx_prepare(const Dev& d, const MixBufs& mb, bool schwarz, cudaStream_t s, int64_t* lc);
+int mx_pcg_grid_blocks(const Dev& d);
+int mx_launch_pcg(const Dev& d, const MixBufs& mb, int maxIters, double tol, int blocks, cudaStream_t s);
+void mx_grad_final(const Dev& d, cudaStream_t s, int64_t* lc);
+void mx_energy_final(const Dev& d, cudaStream_t s, int64_t* lc);
+
+}  // namespace cs

@@ -15,6 +15,8 @@
 
 namespace cs {
 
+static inline int nblk(int n) { return (n + kThreads - 1) / kThreads; }
+
 __device__ __forceinline__ void load3(const double* x, int v, double o[3]) {
   o[0] = x[v * 3]; o[1] = x[v * 3 + 1]; o[2] = x[v * 3 + 2];
 }
@@ -31,6 +33,44 @@ __device__ __forceinline__ double seq_chain(const double* t, int n, double s = 0
     s = s + a3;
   }
   for (; i < n; i++) s = s + t[i];
+  return s;
+}
+
+// The same left-to-right chain, run by a whole block: warps 1.. stream the
+// terms through a double-buffered shared-memory stage while thread 0 adds the
+// previous stage in order. Every thread of the block must call it; the sum is
+// valid in thread 0.
+constexpr int kChunk = 2048;
+__device__ __forceinline__ double block_chain(const double* t, int n, double* buf) {
+  double s = 0.0;
+  const int first = n < kChunk ? n : kChunk;
+  for (int j = threadIdx.x; j < first; j += blockDim.x) buf[j] = t[j];
+  __syncthreads();
+  const int nchunks = (n + kChunk - 1) / kChunk;
+  for (int c = 0; c < nchunks; c++) {
+    const int base = c * kChunk;
+    const int len = n - base < kChunk ? n - base : kChunk;
+    const double* cur = buf + (c & 1) * kChunk;
+    if (threadIdx.x >= 32) {
+      const int nbase = base + kChunk;
+      if (nbase < n) {
+        double* nxt = buf + ((c + 1) & 1) * kChunk;
+        const int nlen = n - nbase < kChunk ? n - nbase : kChunk;
+        for (int j = threadIdx.x - 32; j < nlen; j += blockDim.x - 32) nxt[j] = t[nbase + j];
+      }
+    } else if (threadIdx.x == 0) {
+      int j = 0;
+      for (; j + 16 <= len; j += 16) {
+        double a[16];
+#pragma unroll
+        for (int q = 0; q < 16; q++) a[q] = cur[j + q];
+#pragma unroll
+        for (int q = 0; q < 16; q++) s = s + a[q];
+      }
+      for (; j < len; j++) s = s + cur[j];
+    }
+    __syncthreads();
+  }
   return s;
 }
 
@@ -122,11 +162,13 @@ __global__ void __launch_bounds__(kThreads) k_gather_grad(Dev d) {
 
 // Final reduction of the gradient pass: sqrt(sum g^2) in index order
 // (newton.ts:128), max strain (order-free).
-__global__ void k_grad_final(Dev d, int nbT) {
+__global__ void __launch_bounds__(kThreads) k_grad_final(Dev d, int nbT) {
+  __shared__ double cbuf[2 * kChunk];
+  const double gs = block_chain(d.T0, d.n * 3, cbuf);
   if (threadIdx.x >= 32) return;
   const double ms = warp_max_partials(d.part + 0 * d.partStride, nbT);
   if (threadIdx.x == 0) {
-    d.scal[S_GRADNORM] = sqrt(seq_chain(d.T0, d.n * 3));
+    d.scal[S_GRADNORM] = sqrt(gs);
     d.scal[S_MAXSTRAIN] = ms;
   }
 }
@@ -159,24 +201,19 @@ __global__ void __launch_bounds__(kThreads) k_energy(Dev d, const double* x) {
 }
 
 // totalEnergy (newton.ts:76-88): ((sum inertia) + internal) + merit, each sum a
-// left-to-right chain; the three chains run on three warps.
-__global__ void k_energy_final(Dev d, int nMerit) {
-  __shared__ double part[3];
-  const int w = threadIdx.x >> 5;
-  if ((threadIdx.x & 31) == 0) {
-    if (w == 0) part[0] = seq_chain(d.T0, d.n * 3);
-    if (w == 1) part[1] = seq_chain(d.T1, d.m + (d.kb > 0 ? d.hg : 0));
-    if (w == 2) part[2] = d.hasContact ? seq_chain(d.Tc, nMerit) : 0.0;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    d.scal[S_E_INERTIA] = part[0];
-    d.scal[S_E_TRI] = part[1];
-    d.scal[S_E_MERIT] = part[2];
-    double e = part[0] + part[1];
-    if (d.hasContact) e += part[2];
-    d.scal[S_ENERGY_TRIAL] = e;
-  }
+// left-to-right chain; block 0 inertia, block 1 internal, block 2 merit.
+__global__ void __launch_bounds__(kThreads) k_energy_chains(Dev d, int nMerit) {
+  __shared__ double cbuf[2 * kChunk];
+  double v = 0.0;
+  if (blockIdx.x == 0) v = block_chain(d.T0, d.n * 3, cbuf);
+  if (blockIdx.x == 1) v = block_chain(d.T1, d.m + (d.kb > 0 ? d.hg : 0), cbuf);
+  if (blockIdx.x == 2) v = d.hasContact ? block_chain(d.Tc, nMerit, cbuf) : 0.0;
+  if (threadIdx.x == 0) d.scal[S_E_INERTIA + blockIdx.x] = v;
+}
+__global__ void k_energy_final(Dev d) {
+  double e = d.scal[S_E_INERTIA] + d.scal[S_E_TRI];
+  if (d.hasContact) e += d.scal[S_E_MERIT];
+  d.scal[S_ENERGY_TRIAL] = e;
 }
 
 __global__ void k_diag_init(Dev d, double beta) {
@@ -372,14 +409,29 @@ __device__ __forceinline__ double block_max_nonan(double v, double* sm) {
   return r;
 }
 
-// One thread per chain computes the chained sums after a grid barrier;
-// results land in scal[S_CH0 + w]. Up to 4 chains, one per warp of block 0.
+// Chained sums after a grid barrier: chain w (w < nch) runs on block w as a
+// block_chain; results land in scal[S_CH0 + w]. With fewer blocks than chains,
+// block 0 runs them one after another.
 __device__ __forceinline__ void run_chains(const Dev& d, int nch, const double* a0, const double* a1,
-                                           const double* a2, int n) {
-  if (blockIdx.x == 0 && (threadIdx.x & 31) == 0) {
-    const int w = threadIdx.x >> 5;
-    const double* a = w == 0 ? a0 : w == 1 ? a1 : a2;
-    if (w < nch) d.scal[S_CH0 + w] = seq_chain(a, n);
+                                           const double* a2, int n, double* cbuf) {
+  const double* arr[3] = {a0, a1, a2};
+  if ((int)gridDim.x >= nch) {
+    if ((int)blockIdx.x < nch) {
+      const double v = block_chain(arr[blockIdx.x], n, cbuf);
+      if (threadIdx.x == 0) d.scal[S_CH0 + blockIdx.x] = v;
+    }
+  } else if (blockIdx.x == 0) {
+    for (int w = 0; w < nch; w++) {
+      const double v = block_chain(arr[w], n, cbuf);
+      if (threadIdx.x == 0) d.scal[S_CH0 + w] = v;
+    }
+  }
+}
+// One chain into scal[slot], on block 0.
+__device__ __forceinline__ void run_chain1(const Dev& d, const double* a, int n, int slot, double* cbuf) {
+  if (blockIdx.x == 0) {
+    const double v = block_chain(a, n, cbuf);
+    if (threadIdx.x == 0) d.scal[slot] = v;
   }
 }
 
@@ -387,6 +439,7 @@ __global__ void __launch_bounds__(kThreads) k_pcg(PcgArgs A) {
   cg::grid_group grid = cg::this_grid();
   __shared__ double sm[32];
   __shared__ double bc[2];
+  __shared__ double cbuf[2 * kChunk];
   const Dev& d = A.d;
   const int n3 = d.n * 3;
   const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
@@ -414,7 +467,7 @@ __global__ void __launch_bounds__(kThreads) k_pcg(PcgArgs A) {
     for (int i = tid; i < n3; i += nth) d.p[i] = d.z[i];
   }
   // chains: rz (T2), |b|^2 (T0), |r|^2 (T1)
-  run_chains(d, 3, d.T2, d.T0, d.T1, n3);
+  run_chains(d, 3, d.T2, d.T0, d.T1, n3, cbuf);
   grid.sync();
   double rz = d.scal[S_CH0];
   const double bNorm = sqrt(d.scal[S_CH1]);
@@ -425,7 +478,7 @@ __global__ void __launch_bounds__(kThreads) k_pcg(PcgArgs A) {
   if (!done) {
     for (int i = tid; i < n3; i += nth) d.T3[i] = d.p[i] * d.p[i];
     grid.sync();
-    if (blockIdx.x == 0 && threadIdx.x == 0) d.scal[S_CH3] = seq_chain(d.T3, n3);
+    run_chain1(d, d.T3, n3, S_CH3, cbuf);
     grid.sync();
   }
   int k = 0;
@@ -479,7 +532,7 @@ __global__ void __launch_bounds__(kThreads) k_pcg(PcgArgs A) {
       }
     }
     grid.sync();
-    if (blockIdx.x == 0 && threadIdx.x == 0) d.scal[S_CH1] = seq_chain(d.T0, n3);
+    run_chain1(d, d.T0, n3, S_CH1, cbuf);
     grid.sync();
     const double pAp = d.scal[S_CH1];
     if (!(pAp > 1e-30)) { iters = k; done = true; break; }
@@ -500,14 +553,14 @@ __global__ void __launch_bounds__(kThreads) k_pcg(PcgArgs A) {
       }
     }
     grid.sync();
-    run_chains(d, jacobi ? 2 : 1, d.T1, d.T2, d.T2, n3);  // |r|^2 -> CH0, r.z -> CH1
+    run_chains(d, jacobi ? 2 : 1, d.T1, d.T2, d.T2, n3, cbuf);  // |r|^2 -> CH0, r.z -> CH1
     grid.sync();
     residual = sqrt(d.scal[S_CH0]);
     if (residual < absTol) { iters = k + 1; done = true; break; }
     if (!jacobi) {
       for (int dom = tid; dom < d.D; dom += nth) schwarz_apply_domain(d, dom);
       grid.sync();
-      if (blockIdx.x == 0 && threadIdx.x == 0) d.scal[S_CH1] = seq_chain(d.T2, n3);
+      run_chain1(d, d.T2, n3, S_CH1, cbuf);
       grid.sync();
     }
     const double rzNew = d.scal[S_CH1];
@@ -519,7 +572,7 @@ __global__ void __launch_bounds__(kThreads) k_pcg(PcgArgs A) {
     }
     rz = rzNew;
     grid.sync();
-    if (blockIdx.x == 0 && threadIdx.x == 0) d.scal[S_CH3] = seq_chain(d.T3, n3);
+    run_chain1(d, d.T3, n3, S_CH3, cbuf);
     grid.sync();
   }
   if (!done) iters = A.maxIters;
@@ -527,7 +580,7 @@ __global__ void __launch_bounds__(kThreads) k_pcg(PcgArgs A) {
   grid.sync();
   for (int i = tid; i < n3; i += nth) d.T0[i] = d.g[i] * d.dx[i];
   grid.sync();
-  if (blockIdx.x == 0 && threadIdx.x == 0) d.scal[S_CH2] = seq_chain(d.T0, n3);
+  run_chain1(d, d.T0, n3, S_CH2, cbuf);
   grid.sync();
   double gtdx = d.scal[S_CH2];
   bool fallback = false;
@@ -539,7 +592,7 @@ __global__ void __launch_bounds__(kThreads) k_pcg(PcgArgs A) {
       d.T1[i] = d.g[i] * di;
     }
     grid.sync();
-    if (blockIdx.x == 0 && threadIdx.x == 0) d.scal[S_CH3] = seq_chain(d.T1, n3);
+    run_chain1(d, d.T1, n3, S_CH3, cbuf);
     grid.sync();
     gtdx = d.scal[S_CH3];
   }
@@ -567,6 +620,70 @@ __global__ void __launch_bounds__(kThreads) k_pcg(PcgArgs A) {
   }
 }
 
+// ---- standalone FD membrane HVP (fem.ts:108-130) -----------------------------------
+// out = (gradM(x + h p) - gradM(x - h p)) / (2h), h = 1e-8 (1 + |p|): the same
+// element and gather arithmetic as the PCG kernel's HVP phase, as plain kernels.
+__global__ void k_hvp_terms(const double* p, int n3, double* T) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n3) T[i] = p[i] * p[i];
+}
+__global__ void __launch_bounds__(kThreads) k_hvp_h(const double* T, int n3, double* h) {
+  __shared__ double cbuf[2 * kChunk];
+  const double pp = block_chain(T, n3, cbuf);
+  if (threadIdx.x == 0) *h = 1e-8 * (1 + sqrt(pp));
+}
+__device__ __forceinline__ void hvp_elem_tri(int t, const uint32_t* idx, const float4* inv, const float* area,
+                                             const Mat<double>& mat, const double* x, const double* p, double h,
+                                             double* elem) {
+  const uint32_t vi[3] = {idx[t * 3], idx[t * 3 + 1], idx[t * 3 + 2]};
+  double xp[9], xm[9];
+#pragma unroll
+  for (int c = 0; c < 3; c++)
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+      const double xx = x[vi[c] * 3 + q], pq = p[vi[c] * 3 + q];
+      xp[c * 3 + q] = xx + h * pq;
+      xm[c * 3 + q] = xx - h * pq;
+    }
+  const float4 iv = inv[t];
+  double e, gp[9], gm[9], E[3];
+  tri_grad<double>(xp, xp + 3, xp + 6, iv.x, iv.y, iv.z, iv.w, area[t], mat, e, gp, E);
+  tri_grad<double>(xm, xm + 3, xm + 6, iv.x, iv.y, iv.z, iv.w, area[t], mat, e, gm, E);
+  double* o = elem + (size_t)t * 18;
+#pragma unroll
+  for (int q = 0; q < 9; q++) { o[q] = gp[q]; o[9 + q] = gm[q]; }
+}
+__global__ void __launch_bounds__(kThreads) k_hvp_elem(const uint32_t* idx, const float4* inv, const float* area,
+                                                       Mat<double> mat, int m, const double* x, const double* p,
+                                                       const double* h, double* elem) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < m) hvp_elem_tri(t, idx, inv, area, mat, x, p, *h, elem);
+}
+__global__ void __launch_bounds__(kThreads) k_hvp_gather(const uint32_t* memOff, const uint32_t* memRec, int n,
+                                                         const double* elem, const double* h, double* out) {
+  const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= n) return;
+  double sp[3] = {0, 0, 0}, sn[3] = {0, 0, 0};
+  for (uint32_t q = memOff[v]; q < memOff[v + 1]; q++) {
+    const uint32_t rec = memRec[q];
+    const double* e = elem + (size_t)(rec >> 2) * 18 + (rec & 3) * 3;
+    sp[0] += e[0]; sp[1] += e[1]; sp[2] += e[2];
+    sn[0] += e[9]; sn[1] += e[10]; sn[2] += e[11];
+  }
+  const double hh = *h;
+#pragma unroll
+  for (int c = 0; c < 3; c++) out[v * 3 + c] = (sp[c] - sn[c]) / (2 * hh);
+}
+
+void launch_membrane_hvp(const uint32_t* idx, const float4* inv, const float* area, const Mat<double>& mat, int n,
+                         int m, const uint32_t* memOff, const uint32_t* memRec, const double* x, const double* p,
+                         double* out, double* T, double* h, double* elem, cudaStream_t s) {
+  k_hvp_terms<<<nblk(n * 3), kThreads, 0, s>>>(p, n * 3, T);
+  k_hvp_h<<<1, kThreads, 0, s>>>(T, n * 3, h);
+  k_hvp_elem<<<nblk(m), kThreads, 0, s>>>(idx, inv, area, mat, m, x, p, h, elem);
+  k_hvp_gather<<<nblk(n), kThreads, 0, s>>>(memOff, memRec, n, elem, h, out);
+}
+
 // ---- Armijo trial + velocity ----------------------------------------------------
 __global__ void k_trial(Dev d, double alpha) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -581,7 +698,6 @@ __global__ void k_velocity(Dev d, double damp) {
 }
 
 // ---- launchers ------------------------------------------------------------------
-static inline int nblk(int n) { return (n + kThreads - 1) / kThreads; }
 
 void launch_predict(const Dev& d, cudaStream_t s) {
   k_predict<<<nblk(d.n), kThreads, 0, s>>>(d);
@@ -590,16 +706,23 @@ void launch_predict(const Dev& d, cudaStream_t s) {
 void launch_pins(const Dev& d, double* x, cudaStream_t s) {
   if (d.npins > 0) k_pins<<<nblk(d.npins), kThreads, 0, s>>>(d, x);
 }
-void launch_grad(const Dev& d, cudaStream_t s) {
+void launch_grad_terms(const Dev& d, cudaStream_t s) {
   k_tri_grad<<<nblk(d.m), kThreads, 0, s>>>(d);
   if (d.kb > 0 && d.hg > 0) k_hinge_grad<<<nblk(d.hg), kThreads, 0, s>>>(d);
   k_gather_grad<<<nblk(d.n), kThreads, 0, s>>>(d);
-  k_grad_final<<<1, 32, 0, s>>>(d, nblk(d.m));
 }
-void launch_energy(const Dev& d, const double* x, cudaStream_t s) {
+void launch_grad(const Dev& d, cudaStream_t s) {
+  launch_grad_terms(d, s);
+  k_grad_final<<<1, kThreads, 0, s>>>(d, nblk(d.m));
+}
+void launch_energy_terms(const Dev& d, const double* x, cudaStream_t s) {
   const int nb = nblk(std::max(std::max(d.n, d.m), d.hg));
   k_energy<<<nb, kThreads, 0, s>>>(d, x);
-  k_energy_final<<<1, 96, 0, s>>>(d, d.hasContact ? d.c.nActive : 0);
+}
+void launch_energy(const Dev& d, const double* x, cudaStream_t s) {
+  launch_energy_terms(d, x, s);
+  k_energy_chains<<<3, kThreads, 0, s>>>(d, d.hasContact ? d.c.nActive : 0);
+  k_energy_final<<<1, 1, 0, s>>>(d);
 }
 void launch_diag_init(const Dev& d, double beta, cudaStream_t s) {
   k_diag_init<<<nblk(d.n * 3), kThreads, 0, s>>>(d, beta);

@@ -11,7 +11,7 @@ namespace cs {
 // Slots of the device scalar array (double).
 enum ScalarSlot {
   S_GRADNORM = 0, S_MAXSTRAIN, S_ENERGY_TRIAL, S_GTDX, S_PCG_ITERS, S_PCG_RES, S_E_INERTIA,
-  S_E_TRI, S_E_HINGE, S_E_MERIT, S_FALLBACK, S_MAXDX, S_VALID, S_MINDIST, S_MINTOI, S_CCDFAIL,
+  S_E_TRI, S_E_MERIT, S_E_HINGE, S_FALLBACK, S_MAXDX, S_VALID, S_MINDIST, S_MINTOI, S_CCDFAIL,
   S_BARRIER_E, S_FWORK, S_CH0 = 24, S_CH1, S_CH2, S_CH3, S_NSCALARS = 32
 };
 
@@ -90,6 +90,8 @@ constexpr int NPART = 8;
 void launch_predict(const Dev& d, cudaStream_t s);
 void launch_pins(const Dev& d, double* x, cudaStream_t s);
 void launch_grad(const Dev& d, cudaStream_t s);           // g, gradNorm, maxStrain
+void launch_grad_terms(const Dev& d, cudaStream_t s);     // g and its squared terms, strain partials
+void launch_energy_terms(const Dev& d, const double* x, cudaStream_t s);
 void launch_energy(const Dev& d, const double* x, cudaStream_t s);  // S_ENERGY_TRIAL
 void launch_diag_init(const Dev& d, double beta, cudaStream_t s);
 void launch_schwarz_factor(const Dev& d, cudaStream_t s);
@@ -97,5 +99,9 @@ int launch_pcg(const Dev& d, int maxIters, double tol, int gridBlocks, cudaStrea
 void launch_trial(const Dev& d, double alpha, cudaStream_t s);   // xt = x + alpha dx, pins
 void launch_velocity(const Dev& d, double damp, cudaStream_t s);
 int pcg_grid_blocks(const Dev& d);
+// FD membrane HVP over device arrays (T: 3n terms, h: 1 double, elem: 18m scratch).
+void launch_membrane_hvp(const uint32_t* idx, const float4* inv, const float* area, const Mat<double>& mat, int n,
+                         int m, const uint32_t* memOff, const uint32_t* memRec, const double* x, const double* p,
+                         double* out, double* T, double* h, double* elem, cudaStream_t s);
 
 }  // namespace cs

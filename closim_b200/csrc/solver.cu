@@ -118,6 +118,12 @@ int cs_set_state(cs_solver* h, const double* x, const double* v) {
     h->s.set_state(x, v);
   });
 }
+int cs_membrane_hvp(cs_solver* h, const double* x, const double* p, double* out) {
+  return guarded(h, [&] {
+    if (!x || !p || !out) throw std::invalid_argument("null argument");
+    h->s.membrane_hvp(x, p, out);
+  });
+}
 int cs_last_stats(cs_solver* h, cs_step_stats* out) {
   return guarded(h, [&] {
     if (!h->s.haveStats) throw std::logic_error("CpuSolver not initialized: no step taken");

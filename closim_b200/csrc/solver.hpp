@@ -13,6 +13,7 @@
 
 #include "../../include/closim_cuda.h"
 #include "contact_host.hpp"
+#include "mixed.cuh"
 #include "plain.cuh"
 #include "setup.hpp"
 
@@ -87,6 +88,10 @@ class Solver {
   DBuf<uint8_t> domFlag;
   double* hscal = nullptr;  // pinned host mirror of scal
   int pcgBlocks = 1;
+  // mixed-precision path
+  DBuf<float> fr, fz, fp, fAp, fx, felem, ftris, fh9, fLinv;
+  MixBufs mb{};
+  int mxBlocks = 1;
   Dev d{};
   // profiling of the linear-solve kernel
   bool prof = false;
@@ -140,6 +145,14 @@ class Solver {
     mat = m;
     d.mat = Mat<double>{m.stretch_warp, m.stretch_weft, m.stretch_coupling, m.shear, m.thickness};
     d.kb = 0.5 * (m.bend_warp + m.bend_weft);
+    mb.C00 = (float)m.stretch_warp; mb.C11 = (float)m.stretch_weft; mb.C01 = (float)m.stretch_coupling;
+    mb.G = (float)m.shear;
+  }
+  bool mixed() const { return precision == CS_PRECISION_MIXED; }
+  void energy_of(const double* x) {
+    int64_t& lc = launch_counter();
+    if (mixed()) { launch_energy_terms(d, x, stream); lc += 1; mx_energy_final(d, stream, &lc); }
+    else { launch_energy(d, x, stream); lc += 3; }
   }
 
   void initialize(const cs_mesh& cm, const cs_material& m, const double* g, const double* x, const double* v) {
@@ -218,6 +231,16 @@ class Solver {
     set_material(m);
     for (int k = 0; k < 3; k++) d.gravity[k] = gravity[k];
     pcgBlocks = pcg_grid_blocks(d);
+    if (precision == CS_PRECISION_MIXED) {
+      for (DBuf<float>* b : {&fr, &fz, &fp, &fAp, &fx}) b->alloc(n3);
+      felem.alloc((size_t)cm.m * 9);
+      ftris.alloc((size_t)cm.m * 16);
+      fh9.alloc((size_t)cm.m * 81);
+      fLinv.alloc((size_t)std::max(mesh.D, 1) * 576);
+      mb.r = fr.p; mb.z = fz.p; mb.p = fp.p; mb.Ap = fAp.p; mb.x = fx.p;
+      mb.elem = felem.p; mb.tris = ftris.p; mb.h9 = fh9.p; mb.Linv = fLinv.p;
+      mxBlocks = mx_pcg_grid_blocks(d);
+    }
     upload_pins();
     contact.reset();
     CK(cudaStreamSynchronize(stream));
@@ -266,8 +289,7 @@ class Solver {
     if (contact) contact->begin_step_and_bisect(*this);
     if (contact) contact->update_active_set(*this, d.x);
     if (contact) contact->merit_energy(*this, d.x);
-    launch_energy(d, d.x, stream);
-    lc += 2;
+    energy_of(d.x);
     const double beta = std::max(std::max(mat.stretch_warp, mat.stretch_weft), mat.shear) * mat.thickness * 0.1 + 1e-6;
     launch_diag_init(d, beta, stream);
     lc += 1;
@@ -279,16 +301,24 @@ class Solver {
     for (int ni = 0; ni < opts.newton_iters; ni++) {
       used = ni + 1;
       if (contact) contact->gradient_terms(*this);  // active set, barrier+friction grad, diag estimate
-      launch_grad(d, stream);
-      lc += 3 + (d.kb > 0 && d.hg > 0);
+      if (mixed()) {
+        launch_grad_terms(d, stream);
+        lc += 2 + (d.kb > 0 && d.hg > 0);
+        mx_grad_final(d, stream, &lc);
+      } else {
+        launch_grad(d, stream);
+        lc += 3 + (d.kb > 0 && d.hg > 0);
+      }
       read_scalars();
       gradNorm = hscal[S_GRADNORM];
       maxStrain = hscal[S_MAXSTRAIN];
       if (!std::isfinite(gradNorm)) throw NonFinite();
       if (gradNorm < opts.grad_tol) { converged = true; break; }
-      if (d.precond == 1) { launch_schwarz_factor(d, stream); lc += 1; }
+      if (mixed()) mx_prepare(d, mb, d.precond == 1, stream, &lc);
+      else if (d.precond == 1) { launch_schwarz_factor(d, stream); lc += 1; }
       if (prof) CK(cudaEventRecord(pev0, stream));
-      CK((cudaError_t)launch_pcg(d, opts.pcg_max_iters, 1e-3, pcgBlocks, stream));
+      if (mixed()) CK((cudaError_t)mx_launch_pcg(d, mb, opts.pcg_max_iters, 1e-3, mxBlocks, stream));
+      else CK((cudaError_t)launch_pcg(d, opts.pcg_max_iters, 1e-3, pcgBlocks, stream));
       if (prof) { CK(cudaEventRecord(pev1, stream)); profPending = true; }
       lc += 1;
       double alpha = 1;
@@ -305,8 +335,7 @@ class Solver {
           continue;
         }
         if (contact) contact->merit_energy(*this, d.xt);
-        launch_energy(d, d.xt, stream);
-        lc += 2;
+        energy_of(d.xt);
         read_scalars();
         if (!haveSlope) {
           gtdx = hscal[S_GTDX];
@@ -362,6 +391,19 @@ class Solver {
     stats.armijo_trials = trials;
     if (contact) contact->fill_stats(*this, stats);
     haveStats = true;
+  }
+
+  // membraneHvp (fem.ts:108-130) at x along p; host arrays of 3n doubles.
+  void membrane_hvp(const double* x, const double* p, double* out) {
+    if (!ready) throw std::logic_error("CpuSolver not initialized");
+    const size_t b = 3 * (size_t)mesh.n * 8;
+    CK(cudaMemcpyAsync(vr.p, x, b, cudaMemcpyHostToDevice, stream));
+    CK(cudaMemcpyAsync(vz.p, p, b, cudaMemcpyHostToDevice, stream));
+    launch_membrane_hvp(idx.p, inv.p, area.p, d.mat, mesh.n, mesh.m, memOff.p, memRec.p, vr.p, vz.p, vAp.p, T3.p,
+                        scal.p + S_CH3, elem.p, stream);
+    launch_counter() += 4;
+    CK(cudaMemcpyAsync(out, vAp.p, b, cudaMemcpyDeviceToHost, stream));
+    CK(cudaStreamSynchronize(stream));
   }
 
   void get(double* out, bool vel) {

@@ -341,6 +341,16 @@ class CudaSolver:
         return StepStats(st.newton_iters, st.pcg_iters, st.grad_norm, st.energy, st.max_strain, bool(st.converged),
                          con, st.newton_iters_used, st.armijo_trials)
 
+    def membraneHvp(self, x, p) -> np.ndarray:
+        """membraneHvp (src/physics/fem.ts:108-130) on the GPU: central-difference
+        membrane Hessian-vector product at x along p."""
+        self._need()
+        x = np.ascontiguousarray(x, np.float64)
+        p = np.ascontiguousarray(p, np.float64)
+        out = np.zeros_like(x)
+        self._check(self._lib.cs_membrane_hvp(self._h, L.ptr(x), L.ptr(p), L.ptr(out)))
+        return out
+
     def kernelLaunches(self) -> int:
         return int(self._lib.cs_kernel_launches(self._h))
 

@@ -122,6 +122,11 @@ int cs_set_state(cs_solver* s, const double* x, const double* v);
 /* CpuSolver.lastStats (cpu-solver.ts:6). */
 int cs_last_stats(cs_solver* s, cs_step_stats* out);
 
+/* membraneHvp(x, p) (src/physics/fem.ts:108-130): the central-difference
+ * membrane Hessian-vector product the FP64 path's PCG applies, h = 1e-8 (1 + |p|),
+ * on the initialized mesh and current material. Host arrays of 3n doubles. */
+int cs_membrane_hvp(cs_solver* s, const double* x, const double* p, double* out);
+
 /* ---- device-resident helpers (no reference counterpart needed by a drop-in) ---- */
 /* Runs `nsteps` steps back to back without copying state to the host. */
 int cs_step_n(cs_solver* s, double dt, int32_t nsteps);

@@ -112,3 +112,22 @@ def test_nonfinite_gradient_raises():
     s.initialize(sc)
     with pytest.raises(FloatingPointError, match="non-finite gradient"):
         s.step(0.01)
+
+
+def test_membrane_hvp_bit_exact():
+    """membraneHvp (fem.ts:108-130) on the GPU equals the oracle bit for bit."""
+    from oracle import oracle as O
+    cfg = configs.floor_drape(nx=20, ny=13, w=0.3, hgt=0.2)
+    sc = configs.make_scene(cfg)
+    s = cb.CudaSolver("fp64")
+    s.initialize(sc)
+    mesh = O.Mesh(cfg["pos"], cfg["uv"], cfg["idx"], cfg["density"])
+    m = cfg["material"]
+    mat = dict(arealDensity=m["arealDensityKgM2"], thickness=m["thickness"], C00=m["stretchWarp"],
+               C11=m["stretchWeft"], C01=m["stretchCoupling"], G=m["shear"], bendWarp=m["bendWarp"],
+               bendWeft=m["bendWeft"], damping=m["damping"])
+    rng = np.random.default_rng(4)
+    for _ in range(3):
+        x = cfg["x"] + rng.uniform(-2e-3, 2e-3, len(cfg["x"]))
+        p = rng.normal(0, 1, len(cfg["x"]))
+        assert np.array_equal(s.membraneHvp(x, p), O.membrane_hvp(mesh, mat, x, p))
