@@ -144,14 +144,63 @@ def run_reference(args, rank):
     return 0
 
 
+def run_precision(cfg, precision, local, args, ext_stream_cb, flush, sampler=None, prof_out=None):
+    """Warm-up W steps, then K device-resident steps, each bracketed by CUDA
+    events on the solver's stream after an L2 flush. Returns (ms_total, solver,
+    scene, final positions, kernel launches)."""
+    import torch
+    import closim_b200 as cb
+    from closim_b200 import configs
+    sc = configs.make_scene(cfg)
+    solver = cb.CudaSolver(precision, device=local, **cfg["options"])
+    solver.initialize(sc)
+    ext = torch.cuda.ExternalStream(solver.stream(), device=local)
+    k = [0]
+
+    def set_pins():
+        sc.pinned.clear()
+        sc.pinned.update(configs.pins_at(cfg, k[0] % cfg["steps"]))
+        k[0] += 1
+
+    for _ in range(args.warmup):
+        set_pins()
+        solver.advance(cfg["h"], 1)
+    torch.cuda.synchronize()
+    ext_stream_cb()
+    if sampler:
+        sampler.start()
+    launches0 = solver.kernelLaunches()
+    solver.profile(True)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    total = 0.0
+    for _ in range(args.steps):
+        set_pins()
+        with torch.cuda.stream(ext):
+            flush.fill_(1.0)
+        ev0.record(ext)
+        solver.advance(cfg["h"], 1)
+        ev1.record(ext)
+        ev1.synchronize()
+        total += ev0.elapsed_time(ev1)
+    torch.cuda.synchronize()
+    if prof_out is not None:
+        prof_out.update(solver.profileRead())
+    solver.profile(False)
+    launches = solver.kernelLaunches() - launches0
+    solver.pull()
+    return total, solver, sc, sc.positions.copy(), launches, ext, set_pins
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=60)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
     ap.add_argument("--workload", default="floor_drape", choices=["floor_drape", "strip_pull"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--small", action="store_true", help="32x32 floor drape (for profiler captures)")
+    ap.add_argument("--precision", default="both", choices=["both", "fp64", "mixed"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -169,61 +218,39 @@ def main():
     if world > 1:
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
-    import closim_b200 as cb
     from closim_b200 import configs
-    cfg = workload(args.workload, args.steps)
+    if args.small:
+        cfg = configs.floor_drape(nx=31, ny=31, w=0.4, hgt=0.4)
+    else:
+        cfg = workload(args.workload, args.steps)
     n = len(cfg["x"]) // 3
-    sc = configs.make_scene(cfg)
-    solver = cb.CudaSolver(args.precision, device=local, **cfg["options"])
-    solver.initialize(sc)
-    ext = torch.cuda.ExternalStream(solver.stream(), device=local)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{local}")  # 256 MiB > 126 MB L2
 
-    step_idx = [0]
+    def barrier():
+        if world > 1:
+            dist.barrier()
 
-    def set_pins():
-        sc.pinned.clear()
-        sc.pinned.update(configs.pins_at(cfg, step_idx[0] % cfg["steps"]))
-        step_idx[0] += 1
-
-    for _ in range(args.warmup):
-        set_pins()
-        solver.advance(cfg["h"], 1)
-    torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
-
-    # ---- device-resident timed region ----
+    headline = "mixed" if args.precision in ("both", "mixed") else "fp64"
+    res = {}
+    if args.precision in ("both", "fp64"):
+        t, _, _, pos, la, _, _ = run_precision(cfg, "fp64", local, args, barrier, flush)
+        res["fp64"] = dict(ms=t, pos=pos, launches=la)
     sampler = ClockSampler(local)
-    sampler.start()
-    launches0 = solver.kernelLaunches()
-    solver.profile(True)
-    total_ms = 0.0
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
-    for _ in range(args.steps):
-        set_pins()
-        with torch.cuda.stream(ext):
-            flush.fill_(1.0)
-        ev0.record(ext)
-        solver.advance(cfg["h"], 1)
-        ev1.record(ext)
-        ev1.synchronize()
-        total_ms += ev0.elapsed_time(ev1)
-    torch.cuda.synchronize()
-    prof = solver.profileRead()
-    solver.profile(False)
-    launches = solver.kernelLaunches() - launches0
+    prof = {}
+    t, solver, sc, pos, la, ext, set_pins = run_precision(cfg, headline, local, args, barrier, flush, sampler, prof)
     clocks = sampler.stop()
+    res[headline] = dict(ms=t, pos=pos, launches=la)
 
     # ---- end to end through the public API: host state in, host state out ----
-    # scene arrays in pinned host memory (the copies each step read and write them)
     px = torch.empty(n * 3, dtype=torch.float64).pin_memory()
     pv = torch.empty(n * 3, dtype=torch.float64).pin_memory()
+    px.numpy()[:] = sc.positions
+    pv.numpy()[:] = sc.velocities
     sc.positions = px.numpy()
     sc.velocities = pv.numpy()
     solver.syncFromScene = True
-    solver.pull()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
     e2e_ms = 0.0
     e_steps = max(3, args.steps // 2)
     for _ in range(e_steps):
@@ -236,35 +263,44 @@ def main():
     h2d = 2 * n * 3 * 8 + len(sc.pinned) * (4 + 24)
     d2h = 2 * n * 3 * 8
 
-    t = torch.tensor([total_ms, e2e_ms], dtype=torch.float64, device=f"cuda:{local}")
+    times = [res[headline]["ms"], e2e_ms, res.get("fp64", {}).get("ms", 0.0)]
+    t = torch.tensor(times, dtype=torch.float64, device=f"cuda:{local}")
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         dist.barrier()
-    total_ms, e2e_ms = t.tolist()
-    ms_per_step = total_ms / args.steps
+    total_ms, e2e_ms, fp64_ms = t.tolist()
     value = world * args.steps / (total_ms / 1000.0)
     e2e_value = world * e_steps / (e2e_ms / 1000.0)
 
     if rank == 0:
         peak, peak_kind = measured_peak()
-        achieved = prof["bytes"] / prof["launches"] / (prof["ms_per_launch"] / 1000.0) / 1e9 if prof["launches"] else 0.0
+        achieved = (prof["bytes"] / prof["launches"] / (prof["ms_per_launch"] / 1000.0) / 1e9
+                    if prof.get("launches") else 0.0)
         line = {
             "metric": "sim steps/s", "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if headline == "mixed" else "f64",
             "data": "synthetic (seeded)", "impl": "cuda",
-            "config": {"workload": cfg["name"], "n": n, "m": len(cfg["idx"]) // 3, "h": cfg["h"],
-                       "precision": args.precision, "precond": cfg["options"]["precond"],
+            "config": {"workload": cfg["name"] + ("_32x32" if args.small else ""), "n": n, "m": len(cfg["idx"]) // 3,
+                       "h": cfg["h"], "precision": headline, "precond": cfg["options"]["precond"],
                        "parallelism": f"replicas x{world}", "l2": "flushed between timed steps (256 MiB write)"},
-            "roofline": {"bound": "hbm", "kernel": "k_pcg", "achieved": achieved, "peak": peak,
-                         "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": None, "launches": prof["launches"], "ms_per_launch": prof["ms_per_launch"],
-                         "pcg_iters": prof["iters"], "alg_bytes_per_launch": prof["bytes"] / max(1, prof["launches"]),
-                         "share_of_step": prof["ms"] / total_ms if total_ms else None},
+            "roofline": {"bound": "hbm", "kernel": "k_mx_pcg" if headline == "mixed" else "k_pcg",
+                         "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None, "launches": prof.get("launches"),
+                         "ms_per_launch": prof.get("ms_per_launch"), "pcg_iters": prof.get("iters"),
+                         "alg_bytes_per_launch": prof["bytes"] / max(1, prof["launches"]) if prof else None,
+                         "share_of_step": prof["ms"] / total_ms if total_ms and prof else None},
             "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-            "gpu_launches": launches,
+            "gpu_launches": res[headline]["launches"],
             "clocks": clocks,
         }
+        if "fp64" in res and headline == "mixed":
+            a, b = res["fp64"]["pos"], res["mixed"]["pos"]
+            line["fp64_path"] = {"value": world * args.steps / (fp64_ms / 1000.0), "unit": "steps/s",
+                                 "ms_per_step": fp64_ms / args.steps,
+                                 "gpu_launches": res["fp64"]["launches"]}
+            line["mixed_vs_fp64_rel_pos_err"] = float(np.max(np.abs(b - a)) / np.max(np.abs(a)))
+            line["mixed_vs_fp64_steps"] = args.warmup + args.steps
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(cfg, budget_s=20.0, max_steps=cfg["steps"])
         print(json.dumps(line), flush=True)

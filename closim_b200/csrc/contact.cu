@@ -141,9 +141,30 @@ __device__ double block_min2(const double* a, int na, const double* b, int nb) {
   return r;
 }
 
-__global__ void __launch_bounds__(1024) k_active_min(CView v, int C, int nf) {
-  const double m = block_min2(v.cmin, C, v.vtmp, nf);
-  if (threadIdx.x == 0 && m < v.diag->minDistance) v.diag->minDistance = m;
+// Per-block minima (NaN ignored) of a[0..na) and b[0..nb) into part[blockIdx].
+constexpr int kMinBlocks = 128;
+__global__ void __launch_bounds__(256) k_min_part(const double* a, int na, const double* b, int nb, double* part) {
+  __shared__ double sm[256];
+  double m = INFINITY;
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < na; i += stride) if (a[i] < m) m = a[i];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += stride) if (b[i] < m) m = b[i];
+  sm[threadIdx.x] = m;
+  __syncthreads();
+  for (int off = 128; off > 0; off >>= 1) {
+    if ((int)threadIdx.x < off && sm[threadIdx.x + off] < sm[threadIdx.x]) sm[threadIdx.x] = sm[threadIdx.x + off];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) part[blockIdx.x] = sm[0];
+}
+__device__ __forceinline__ double min_of_parts(const double* part) {
+  double m = INFINITY;
+  for (int i = 0; i < kMinBlocks; i++) if (part[i] < m) m = part[i];
+  return m;
+}
+__global__ void k_active_min(CView v, const double* part) {
+  const double m = min_of_parts(part);
+  if (m < v.diag->minDistance) v.diag->minDistance = m;
 }
 
 // CSR records: one per (contact, slot) whose vertex is a cloth vertex.
@@ -426,10 +447,9 @@ __global__ void k_trial_floor(CView v, const double* xt, double dMin) {
   }
 }
 
-__global__ void __launch_bounds__(1024) k_trial_final(CView v, int C, double dMin) {
-  const double minDist = block_min2(v.cmin, C, v.vtmp, v.n);
-  const double minTOI = block_min2(v.ctoi, C, v.vtmp2, v.n);
-  if (threadIdx.x != 0) return;
+__global__ void k_trial_final(CView v, const double* partDist, const double* partToi, double dMin) {
+  const double minDist = min_of_parts(partDist);
+  const double minTOI = min_of_parts(partToi);
   int valid = 0;
   DevDiag* dg = v.diag;
   if (v.cint[CI_FIRSTNF] != INT_MAX) {
@@ -567,7 +587,7 @@ ContactHost::~ContactHost() {
                    (void**)&cg, (void**)&tc, (void**)&tf, (void**)&rk0, (void**)&rk1, (void**)&rp0, (void**)&rp1,
                    (void**)&rhist, (void**)&cOff, (void**)&lagFloor, (void**)&lagFloorOk, (void**)&lk0,
                    (void**)&lk1, (void**)&lp0, (void**)&lp1, (void**)&lhist, (void**)&lval, (void**)&lsorted,
-                   (void**)&probe, (void**)&diag, (void**)&cint})
+                   (void**)&probe, (void**)&diag, (void**)&cint, (void**)&minpart})
     if (*q) cudaFree(*q);
   if (hint) cudaFreeHost(hint);
   if (hdiag) cudaFreeHost(hdiag);
@@ -623,6 +643,7 @@ void ContactHost::init(Solver& s, const cs_contact_params* prm, int floor_on, do
   dalloc(lagFloorOk, (size_t)n);
   dalloc(probe, 5 * (size_t)n);
   dalloc(diag, 1);
+  dalloc(minpart, 2 * kMinBlocks);
   dalloc(cint, CI_N);
   CK(cudaMallocHost(&hint, CI_N * sizeof(int)));
   CK(cudaMallocHost(&hdiag, sizeof(DevDiag)));
@@ -760,8 +781,9 @@ void ContactHost::update_active_set(Solver& s, double* x) {
     lc++;
   }
   k_floor_flags<<<cnb(n), kCT, 0, st>>>(v, x);
-  k_active_min<<<1, 1024, 0, st>>>(v, C, n);
-  lc += 2;
+  k_min_part<<<kMinBlocks, 256, 0, st>>>(cmin, C, v.vtmp, n, minpart);
+  k_active_min<<<1, 1, 0, st>>>(v, minpart);
+  lc += 3;
   if (C > 0) scan_counts(cflag, C, (uint32_t*)(cint + CI_NCAND), st, &lc);
   else CK(cudaMemsetAsync(cint + CI_NCAND, 0, sizeof(int), st));
   scan_counts(fflag, n, (uint32_t*)(cint + CI_NFLOOR), st, &lc);
@@ -842,8 +864,10 @@ bool ContactHost::check_trial(Solver& s, const double* xt) {
     lc++;
   }
   k_trial_floor<<<cnb(n), kCT, 0, st>>>(v, xt, p.dmin);
-  k_trial_final<<<1, 1024, 0, st>>>(v, C, p.dmin);
-  lc += 3;
+  k_min_part<<<kMinBlocks, 256, 0, st>>>(cmin, C, v.vtmp, n, minpart);
+  k_min_part<<<kMinBlocks, 256, 0, st>>>(ctoi, C, v.vtmp2, n, minpart + kMinBlocks);
+  k_trial_final<<<1, 1, 0, st>>>(v, minpart, minpart + kMinBlocks, p.dmin);
+  lc += 5;
   read_ints(s);
   return hint[CI_VALID] != 0;
 }

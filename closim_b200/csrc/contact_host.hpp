@@ -76,6 +76,7 @@ class ContactHost {
   // probes
   double* probe = nullptr;
   DevDiag* diag = nullptr;
+  double* minpart = nullptr;   // per-block minima (2 x 128)
   int* cint = nullptr;
   int* hint = nullptr;         // pinned mirror of cint
   DevDiag* hdiag = nullptr;    // pinned mirror of diag

@@ -43,26 +43,43 @@ __global__ void __launch_bounds__(kSortThreads) k_radix_hist(const Key<KW>* keys
   hist[threadIdx.x * ntiles + blockIdx.x] = h[threadIdx.x];
 }
 
-// Exclusive scan of `n` u32 in place by one block (chunked, running carry).
+// Exclusive scan of `n` u32 in place by one block: chunks of 4096 (4 per
+// thread), warp-shuffle scans of the thread totals, one running carry.
 static __global__ void __launch_bounds__(1024) k_scan_exclusive(uint32_t* a, int n, uint32_t* total) {
-  __shared__ uint32_t s[1024];
-  __shared__ uint32_t carry;
-  if (threadIdx.x == 0) carry = 0;
-  __syncthreads();
-  for (int base = 0; base < n; base += 1024) {
-    const int i = base + threadIdx.x;
-    const uint32_t v = i < n ? a[i] : 0;
-    s[threadIdx.x] = v;
-    __syncthreads();
-    for (int off = 1; off < 1024; off <<= 1) {
-      const uint32_t t = threadIdx.x >= off ? s[threadIdx.x - off] : 0;
-      __syncthreads();
-      s[threadIdx.x] += t;
-      __syncthreads();
+  __shared__ uint32_t wsum[32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t carry = 0;
+  for (int base = 0; base < n; base += 4096) {
+    const int i0 = base + threadIdx.x * 4;
+    uint32_t v[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) v[k] = i0 + k < n ? a[i0 + k] : 0u;
+    const uint32_t t = v[0] + v[1] + v[2] + v[3];
+    uint32_t incl = t;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += y;
     }
-    if (i < n) a[i] = carry + s[threadIdx.x] - v;
+    if (lane == 31) wsum[warp] = incl;
     __syncthreads();
-    if (threadIdx.x == 1023) carry += s[1023];
+    if (warp == 0) {
+      uint32_t w = lane < (int)(blockDim.x >> 5) ? wsum[lane] : 0u;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
+        if (lane >= o) w += y;
+      }
+      wsum[lane] = w;
+    }
+    __syncthreads();
+    uint32_t excl = carry + (warp > 0 ? wsum[warp - 1] : 0u) + incl - t;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      if (i0 + k < n) a[i0 + k] = excl;
+      excl += v[k];
+    }
+    carry += wsum[31];
     __syncthreads();
   }
   if (threadIdx.x == 0 && total) *total = carry;

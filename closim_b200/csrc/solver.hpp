@@ -107,6 +107,17 @@ class Solver {
   // Schwarz adds one read of its 24x24 factors (4608 B per domain).
   double pcg_bytes(int iters) const {
     const double n = mesh.n, m = mesh.m;
+    if (precision == CS_PRECISION_MIXED) {
+      // FP32 path per iteration: per triangle the stored F/S/Dm^-1 record (64 B),
+      // 3 indices, the 9-float element result written and gathered (2 x 36 B) and
+      // its incidence records (12 B); per vertex p and mass read, Ap written, the
+      // x/r/z/p updates (read p, Ap, x, r, z; write x, r, z, p: 9 x 12 B) and the
+      // CSR offset; Schwarz reads one 24x24 FP32 inverse per domain.
+      const double tri = 64 + 12 + 72 + 12;
+      const double vert = 12 + 4 + 12 + 9 * 12 + 4;
+      const double dom = d.precond == 1 ? 2304.0 + 2 * 96 : 0.0;
+      return 5 * 12 * n + iters * (tri * m + vert * n + dom * mesh.D) + 4 * 24 * n;
+    }
     double hvp = 2 * 24 * n + 32 * m + 2 * 144 * m + 4 * n + 24 * n;
     double vec = 9 * 24 * n + (d.precond == 1 ? 4608.0 * mesh.D : 0.0);
     double init = 6 * 24 * n;
