@@ -143,6 +143,31 @@ void* cs_stream(cs_solver* s);
 int cs_profile(cs_solver* s, int enable);
 int cs_profile_read(cs_solver* s, double* out5);
 
+/* ---- allocation-free membrane HVP (no counterpart in the reference) ----
+ * For callers that may not call cudaMalloc while stepping: a frame recorded into
+ * a CUDA graph (no allocation during stream capture), a real-time loop that
+ * cannot absorb cudaMalloc's device-wide synchronization, or a plugin whose
+ * device memory belongs to another runtime. Computes exactly what
+ * cs_membrane_hvp computes, without a solver handle: every argument is a
+ * device pointer the caller owns (inv_dm 16-byte aligned), `stream` is a
+ * cudaStream_t (NULL = the legacy default stream), and the kernels' scratch
+ * (18 doubles per triangle plus 3 per vertex, about 11 MB) is a fixed array
+ * inside this library that every GPU loading the library holds until exit.
+ * inc_offsets (n+1) and inc_records (3m, value = triangle * 4 + corner, in
+ * ascending triangle order per vertex) are the membrane incidence of
+ * src/mesh/incidence.ts:41-55. Limits: n <= CS_STATIC_HVP_MAX_VERTICES and
+ * m <= CS_STATIC_HVP_MAX_TRIANGLES, else CS_E_CAPACITY. The first call on a
+ * device resolves the array's address (cudaGetSymbolAddress): make that call
+ * before any stream capture. All calls share the array: calls that overlap on
+ * the GPU race, so serialize them. Returns CS_OK, CS_E_ARG, CS_E_CAPACITY or
+ * CS_E_CUDA. */
+#define CS_STATIC_HVP_MAX_VERTICES 65536
+#define CS_STATIC_HVP_MAX_TRIANGLES 65536
+int cs_membrane_hvp_static(int32_t n, int32_t m, const uint32_t* indices, const float* inv_dm,
+                           const float* area, const uint32_t* inc_offsets, const uint32_t* inc_records,
+                           const cs_material* mat, const double* x, const double* p, double* out,
+                           void* stream);
+
 /* ---- mesh preprocessing (src/mesh/mesh.ts:17-126), host side ---- */
 /* buildGrid(nx, ny, w, h): pos 3n f32, uv 2n f32, idx 6*nx*ny u32. */
 int cs_build_grid(int32_t nx, int32_t ny, double w, double h, float* pos, float* uv, uint32_t* idx);
