@@ -12,6 +12,7 @@ LIB_PATH = os.path.join(_HERE, "libclosim_cuda.so")
 CS_OK, CS_E_UNINIT, CS_E_NONFINITE, CS_E_CAPACITY, CS_E_CUDA, CS_E_ARG = range(6)
 CS_PRECISION_FP64, CS_PRECISION_MIXED = 0, 1
 CS_PRECOND_JACOBI, CS_PRECOND_SCHWARZ = 0, 1
+CS_BROADPHASE_MIRROR, CS_BROADPHASE_EXACT = 0, 1
 
 
 class cs_material(C.Structure):
@@ -44,11 +45,18 @@ class cs_step_stats(C.Structure):
                [("newton_iters_used", C.c_int32), ("armijo_trials", C.c_int32)]
 
 
+class cs_broadphase_diag(C.Structure):
+    _fields_ = [("scanned_count", C.c_int64), ("written_count", C.c_int64), ("capacity", C.c_int64),
+                ("candidate_overflow", C.c_int32), ("tree_depth", C.c_int32), ("root", C.c_int32),
+                ("reserved", C.c_int32)]
+
+
 EXPORTS = ["cs_create", "cs_destroy", "cs_last_error", "cs_initialize", "cs_set_contact",
            "cs_set_stepper_options", "cs_set_material", "cs_set_pins", "cs_step", "cs_get_positions",
            "cs_get_velocities", "cs_set_state", "cs_last_stats", "cs_membrane_hvp", "cs_step_n", "cs_sync",
            "cs_kernel_launches", "cs_stream", "cs_profile", "cs_profile_read", "cs_build_grid",
-           "cs_preprocess"]
+           "cs_preprocess", "cs_broadphase_create", "cs_broadphase_destroy", "cs_broadphase_last_error",
+           "cs_broadphase_build", "cs_broadphase_diagnostics", "cs_broadphase_pairs", "cs_broadphase_state"]
 
 _lib = None
 
@@ -88,6 +96,13 @@ def load():
         "cs_build_grid": (C.c_int, [C.c_int32, C.c_int32, C.c_double, C.c_double, vp, vp, vp]),
         "cs_preprocess": (C.c_int, [C.c_int32, C.c_int32, vp, vp, vp, C.c_double, vp, vp, vp,
                                     C.POINTER(C.c_int32), vp, vp]),
+        "cs_broadphase_create": (vp, [C.c_int32, C.c_int32, vp, C.c_double, C.c_int64, C.c_int32]),
+        "cs_broadphase_destroy": (None, [vp]),
+        "cs_broadphase_last_error": (C.c_char_p, [vp]),
+        "cs_broadphase_build": (C.c_int, [vp, vp, vp]),
+        "cs_broadphase_diagnostics": (C.c_int, [vp, C.POINTER(cs_broadphase_diag)]),
+        "cs_broadphase_pairs": (C.c_int, [vp, vp]),
+        "cs_broadphase_state": (C.c_int, [vp] + [vp] * 9),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

@@ -123,7 +123,8 @@ __device__ __forceinline__ int delta_pos(const Key<1>* keys, int p, int q, int n
 }
 
 // gpu-broadphase.ts:253-299: range + split per internal node (power-of-two strides).
-__global__ void k_karras(BvhBufs b, const Key<1>* sk) {
+// Also writes the children's codes into the node's traversal record.
+__global__ void k_karras(BvhBufs b, const Key<1>* sk, const uint32_t* sp) {
   const int m = b.m;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= m - 1) return;
@@ -151,26 +152,50 @@ __global__ void k_karras(BvhBufs b, const Key<1>* sk) {
     if (mid < hi && delta_pos(sk, lo, mid, m) > dNode) split = mid;
     stride /= 2;
   }
-  const int L = split == lo ? m - 1 + lo : split;
-  const int R = split + 1 == hi ? m - 1 + split + 1 : split + 1;
+  const bool leafL = split == lo, leafR = split + 1 == hi;
+  const int L = leafL ? m - 1 + lo : split;
+  const int R = leafR ? m - 1 + split + 1 : split + 1;
   b.left[i] = L;
   b.right[i] = R;
   b.parent[L] = i;
   b.parent[R] = i;
+  const int codeL = leafL ? ~(int)sp[lo] : L;
+  const int codeR = leafR ? ~(int)sp[split + 1] : R;
+  b.rec[4 * i + 0].w = __int_as_float(codeL);
+  b.rec[4 * i + 2].w = __int_as_float(codeR);
   if (lo == 0 && hi == m - 1) *b.root = i;
 }
 
-__global__ void k_node_init(BvhBufs b) {
+__global__ void k_topo_init(BvhBufs b) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int nn = 2 * b.m - 1;
-  if (i >= nn) return;
+  if (i >= 2 * b.m - 1) return;
+  b.parent[i] = -1;
+}
+
+__global__ void k_refit_init(BvhBufs b) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= 2 * b.m - 1) return;
   if (i < b.m - 1) {
-    // Unreached internal nodes stay infinite, which keeps traversal conservative.
+    // A node the climb never reaches stays infinite, which keeps traversal conservative.
     for (int k = 0; k < 3; k++) { b.nbox[i * 6 + k] = -INFINITY; b.nbox[i * 6 + 3 + k] = INFINITY; }
+    for (int q = 0; q < 4; q += 2) {
+      float4 lo = b.rec[4 * i + q], hi = b.rec[4 * i + q + 1];
+      lo.x = lo.y = lo.z = -INFINITY;
+      hi.x = hi.y = hi.z = INFINITY;
+      b.rec[4 * i + q] = lo;
+      b.rec[4 * i + q + 1] = hi;
+    }
   }
   b.visit[i] = 0;
-  b.parent[i] = -1;
   b.depth[i] = 1;
+}
+
+// Writes node `child`'s finished box into its parent's record.
+__device__ __forceinline__ void put_child_box(BvhBufs& b, int parent, int child, const float* bx) {
+  const int side = b.left[parent] == child ? 0 : 2;
+  float* r = (float*)(b.rec + 4 * parent + side);
+  r[0] = bx[0]; r[1] = bx[1]; r[2] = bx[2];
+  r[4] = bx[3]; r[5] = bx[4]; r[6] = bx[5];
 }
 
 // Leaf boxes, then climb: the second child to arrive at a node merges both
@@ -182,10 +207,15 @@ __global__ void k_refit(BvhBufs b, const uint32_t* sp, bool mirror) {
   const int slot = m - 1 + s;
   const uint32_t tri = sp[s];
   const float* src = mirror ? b.boxr : b.boxc;
-  for (int k = 0; k < 6; k++) b.nbox[slot * 6 + k] = src[tri * 6 + k];
+  float bx[6];
+  for (int k = 0; k < 6; k++) {
+    bx[k] = src[tri * 6 + k];
+    b.nbox[slot * 6 + k] = bx[k];
+  }
   b.depth[slot] = 1;
-  __threadfence();
   int node = b.parent[slot];
+  if (node >= 0) put_child_box(b, node, slot, bx);
+  __threadfence();
   for (int guard = 0; node >= 0 && guard < 2 * m; guard++) {
     const uint32_t prev = atomicAdd(&b.visit[node], 1u);
     if (prev == 0) return;
@@ -193,19 +223,26 @@ __global__ void k_refit(BvhBufs b, const uint32_t* sp, bool mirror) {
     const int L = b.left[node], R = b.right[node];
     for (int k = 0; k < 3; k++) {
       const float a = ((volatile float*)b.nbox)[L * 6 + k], c = ((volatile float*)b.nbox)[R * 6 + k];
-      b.nbox[node * 6 + k] = fminf(a, c);
+      bx[k] = fminf(a, c);
       const float a2 = ((volatile float*)b.nbox)[L * 6 + 3 + k], c2 = ((volatile float*)b.nbox)[R * 6 + 3 + k];
-      b.nbox[node * 6 + 3 + k] = fmaxf(a2, c2);
+      bx[3 + k] = fmaxf(a2, c2);
     }
+    for (int k = 0; k < 6; k++) b.nbox[node * 6 + k] = bx[k];
     const int dL = ((volatile int*)b.depth)[L], dR = ((volatile int*)b.depth)[R];
     b.depth[node] = max(dL, dR) + 1;
+    const int up = b.parent[node];
+    if (up >= 0) put_child_box(b, up, node, bx);
     __threadfence();
-    node = b.parent[node];
+    node = up;
   }
 }
 
 __device__ __forceinline__ bool ov6(const float* a, const float* c) {
   return a[0] <= c[3] && a[3] >= c[0] && a[1] <= c[4] && a[4] >= c[1] && a[2] <= c[5] && a[5] >= c[2];
+}
+// query box a (min xyz, max xyz) against a record box (lo = min + code, hi = max)
+__device__ __forceinline__ bool ov_rec(const float* a, const float4& lo, const float4& hi) {
+  return a[0] <= hi.x && a[3] >= lo.x && a[1] <= hi.y && a[4] >= lo.y && a[2] <= hi.z && a[5] >= lo.z;
 }
 __device__ __forceinline__ bool ov6d(const double* a, const double* c) {
   return a[0] <= c[3] && a[3] >= c[0] && a[1] <= c[4] && a[4] >= c[1] && a[2] <= c[5] && a[5] >= c[2];
@@ -217,22 +254,35 @@ __device__ __forceinline__ bool share_vertex(const uint32_t* idx, int a, int c) 
 }
 
 constexpr int kStack = 64;
+constexpr int kLocalPairs = 8;
+
+// Appends a thread's buffered pairs to the output through one atomic.
+__device__ __forceinline__ void flush_pairs(int2* out, uint32_t cap, uint32_t* counter, const int2* buf, int k) {
+  if (k == 0) return;
+  const uint32_t base = atomicAdd(counter, (uint32_t)k);
+  for (int q = 0; q < k; q++)
+    if (base + q < cap) out[base + q] = buf[q];
+}
 
 // Self traversal per sorted leaf s (gpu-broadphase.ts:321-357): children of
 // each popped node are tested against the query leaf's box; leaves with a
-// larger triangle id that share no vertex are pairs. emit = false counts only.
-template <bool EMIT>
-__global__ void k_self(BvhBufs b, const uint32_t* sp, bool mirror) {
+// larger triangle id that share no vertex are pairs.
+// MODE 0 counts per leaf, 1 writes at the scanned offsets (the reference's
+// per-leaf stack order), 2 appends the exact set through b.cnt[0].
+template <int MODE>
+__global__ void __launch_bounds__(128) k_self(BvhBufs b, const uint32_t* sp, bool mirror) {
   const int m = b.m;
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= m) return;
   const int q = (int)sp[s];
-  const float* qb = b.nbox + (size_t)(m - 1 + s) * 6;
+  const float* qb = (mirror ? b.boxr : b.boxc) + (size_t)q * 6;
   float qbox[6];
   for (int k = 0; k < 6; k++) qbox[k] = qb[k];
   const double* q64 = b.box64 + (size_t)q * 6;
   uint32_t count = 0;
-  uint32_t out = EMIT ? b.cnt[s] : 0;
+  uint32_t out = MODE == 1 ? b.cnt[s] : 0;
+  int2 buf[kLocalPairs];
+  int nbuf = 0;
   int stack[kStack];
   int sp_ = 0;
   stack[sp_++] = *b.root;
@@ -240,23 +290,31 @@ __global__ void k_self(BvhBufs b, const uint32_t* sp, bool mirror) {
   while (sp_ > 0) {
     if (++guard > 4l * m + 8) { atomicOr(b.flags, 2); return; }
     const int node = stack[--sp_];
-    const int ch[2] = {b.left[node], b.right[node]};
+    const float4* r = b.rec + 4 * node;
+    const float4 r0 = __ldg(r), r1 = __ldg(r + 1), r2 = __ldg(r + 2), r3 = __ldg(r + 3);
+#pragma unroll
     for (int c = 0; c < 2; c++) {
-      const int child = ch[c];
-      if (child < 0 || !ov6(qbox, b.nbox + (size_t)child * 6)) continue;
-      if (child >= m - 1) {
-        const int tL = (int)sp[child - (m - 1)];
+      const float4 lo = c == 0 ? r0 : r2, hi = c == 0 ? r1 : r3;
+      if (!ov_rec(qbox, lo, hi)) continue;
+      const int code = __float_as_int(lo.w);
+      if (code < 0) {
+        const int tL = ~code;
         if (tL > q && !share_vertex(b.idx, q, tL) && (mirror || ov6d(q64, b.box64 + (size_t)tL * 6))) {
-          if (EMIT) b.pairs[out++] = make_int2(q, tL);
+          if (MODE == 1) b.pairs[out++] = make_int2(q, tL);
+          if (MODE == 2) {
+            buf[nbuf++] = make_int2(q, tL);
+            if (nbuf == kLocalPairs) { flush_pairs(b.pairs, b.pairCap, b.cnt, buf, nbuf); nbuf = 0; }
+          }
           count++;
         }
       } else {
         if (sp_ >= kStack) { atomicOr(b.flags, 1); return; }
-        stack[sp_++] = child;
+        stack[sp_++] = code;
       }
     }
   }
-  if (!EMIT) b.cnt[s] = count;
+  if (MODE == 0) b.cnt[s] = count;
+  if (MODE == 2) flush_pairs(b.pairs, b.pairCap, b.cnt, buf, nbuf);
 }
 
 // Static triangles against the cloth hierarchy (contact-assembly.ts:96-140):
@@ -274,8 +332,8 @@ __device__ __forceinline__ void static_box(const BvhBufs& b, int st, double pad,
   for (int k = 0; k < 3; k++) { o[k] = mn[k] - pad; o[3 + k] = mx[k] + pad; }
 }
 
-template <bool EMIT>
-__global__ void k_static(BvhBufs b, const uint32_t* sp, double pad, int2* outp) {
+__global__ void __launch_bounds__(128) k_static(BvhBufs b, const uint32_t* sp, double pad, int2* outp, uint32_t cap,
+                                                uint32_t* counter) {
   const int st = blockIdx.x * blockDim.x + threadIdx.x;
   if (st >= b.ms) return;
   const int m = b.m;
@@ -283,46 +341,55 @@ __global__ void k_static(BvhBufs b, const uint32_t* sp, double pad, int2* outp) 
   static_box(b, st, pad, s64);
   float sb[6];
   for (int k = 0; k < 3; k++) { sb[k] = __double2float_rd(s64[k]); sb[3 + k] = __double2float_ru(s64[3 + k]); }
-  uint32_t count = 0;
-  uint32_t out = EMIT ? b.cnt[st] : 0;
+  int2 buf[kLocalPairs];
+  int nbuf = 0;
   int stack[kStack];
   int sp_ = 0;
   if (m == 1) {
-    if (ov6d(b.box64, s64)) {
-      if (EMIT) outp[out++] = make_int2(0, st);
-      count++;
-    }
+    if (ov6d(b.box64, s64)) buf[nbuf++] = make_int2(0, st);
   } else {
-    stack[sp_++] = *b.root;
+    const int root = *b.root;
     // the root itself is tested too (queryBvhAll tests every popped node)
-    if (!ov6(sb, b.nbox + (size_t)(*b.root) * 6)) sp_ = 0;
+    if (ov6(sb, b.nbox + (size_t)root * 6)) stack[sp_++] = root;
   }
   long guard = 0;
   while (sp_ > 0) {
     if (++guard > 4l * m + 8) { atomicOr(b.flags, 2); return; }
     const int node = stack[--sp_];
-    const int ch[2] = {b.left[node], b.right[node]};
+    const float4* r = b.rec + 4 * node;
+    const float4 r0 = __ldg(r), r1 = __ldg(r + 1), r2 = __ldg(r + 2), r3 = __ldg(r + 3);
+#pragma unroll
     for (int c = 0; c < 2; c++) {
-      const int child = ch[c];
-      if (child < 0 || !ov6(sb, b.nbox + (size_t)child * 6)) continue;
-      if (child >= m - 1) {
-        const int tL = (int)sp[child - (m - 1)];
+      const float4 lo = c == 0 ? r0 : r2, hi = c == 0 ? r1 : r3;
+      if (!ov_rec(sb, lo, hi)) continue;
+      const int code = __float_as_int(lo.w);
+      if (code < 0) {
+        const int tL = ~code;
         if (ov6d(b.box64 + (size_t)tL * 6, s64)) {
-          if (EMIT) outp[out++] = make_int2(tL, st);
-          count++;
+          buf[nbuf++] = make_int2(tL, st);
+          if (nbuf == kLocalPairs) { flush_pairs(outp, cap, counter, buf, nbuf); nbuf = 0; }
         }
       } else {
         if (sp_ >= kStack) { atomicOr(b.flags, 1); return; }
-        stack[sp_++] = child;
+        stack[sp_++] = code;
       }
     }
   }
-  if (!EMIT) b.cnt[st] = count;
+  flush_pairs(outp, cap, counter, buf, nbuf);
 }
 
 void scan_counts(uint32_t* cnt, int n, uint32_t* total, cudaStream_t s, int64_t* launches) {
   k_scan_exclusive<<<1, 1024, 0, s>>>(cnt, n, total);
   if (launches) *launches += 1;
+}
+
+static void boxes_and_refit(BvhBufs& b, const double* x0, const double* x1, double pad, bool mirror, cudaStream_t s,
+                            int64_t* launches) {
+  const int m = b.m;
+  k_boxes<<<nb(m), kBT, 0, s>>>(b, x0, x1, pad);
+  k_refit_init<<<nb(2 * m - 1), kBT, 0, s>>>(b);
+  k_refit<<<nb(m), kBT, 0, s>>>(b, b.p0, mirror);
+  *launches += 3;
 }
 
 void bvh_build(BvhBufs& b, const double* x0, const double* x1, double pad, bool mirror, cudaStream_t s,
@@ -333,118 +400,101 @@ void bvh_build(BvhBufs& b, const double* x0, const double* x1, double pad, bool 
   k_morton<<<nb(m), kBT, 0, s>>>(b);
   *launches += 3;
   const bool flip = radix_sort<1>(b.k0, b.p0, b.k1, b.p1, m, 30, b.hist, s, launches);
-  const Key<1>* sk = flip ? b.k1 : b.k0;
-  const uint32_t* sp = flip ? b.p1 : b.p0;
   if (flip) {  // keep the sorted result in (k0, p0)
-    cudaMemcpyAsync(b.k0, sk, (size_t)m * sizeof(Key<1>), cudaMemcpyDeviceToDevice, s);
-    cudaMemcpyAsync(b.p0, sp, (size_t)m * 4, cudaMemcpyDeviceToDevice, s);
+    cudaMemcpyAsync(b.k0, b.k1, (size_t)m * sizeof(Key<1>), cudaMemcpyDeviceToDevice, s);
+    cudaMemcpyAsync(b.p0, b.p1, (size_t)m * 4, cudaMemcpyDeviceToDevice, s);
   }
-  k_node_init<<<nb(2 * m - 1), kBT, 0, s>>>(b);
+  k_topo_init<<<nb(2 * m - 1), kBT, 0, s>>>(b);
   *launches += 1;
   cudaMemsetAsync(b.root, 0, sizeof(int), s);
   if (m > 1) {
-    k_karras<<<nb(m - 1), kBT, 0, s>>>(b, b.k0);
+    k_karras<<<nb(m - 1), kBT, 0, s>>>(b, b.k0, b.p0);
     *launches += 1;
   }
+  k_refit_init<<<nb(2 * m - 1), kBT, 0, s>>>(b);
   k_refit<<<nb(m), kBT, 0, s>>>(b, b.p0, mirror);
-  *launches += 1;
+  *launches += 2;
 }
+
+void bvh_refit(BvhBufs& b, const double* x0, const double* x1, double pad, bool mirror, cudaStream_t s,
+               int64_t* launches) {
+  boxes_and_refit(b, x0, x1, pad, mirror, s, launches);
+}
+
+static inline int nq(int n) { return (n + 127) / 128; }
 
 void bvh_count_self(BvhBufs& b, bool mirror, cudaStream_t s, int64_t* launches) {
   if (b.m < 2) {
     cudaMemsetAsync(b.cnt, 0, (size_t)(b.m + 1) * 4, s);
     return;
   }
-  k_self<false><<<nb(b.m), kBT, 0, s>>>(b, b.p0, mirror);
+  k_self<0><<<nq(b.m), 128, 0, s>>>(b, b.p0, mirror);
   *launches += 1;
 }
 void bvh_emit_self(BvhBufs& b, bool mirror, cudaStream_t s, int64_t* launches) {
   if (b.m < 2) return;
-  k_self<true><<<nb(b.m), kBT, 0, s>>>(b, b.p0, mirror);
+  k_self<1><<<nq(b.m), 128, 0, s>>>(b, b.p0, mirror);
   *launches += 1;
 }
-void bvh_count_static(BvhBufs& b, double pad, cudaStream_t s, int64_t* launches) {
-  if (b.ms <= 0) return;
-  k_static<false><<<nb(b.ms), kBT, 0, s>>>(b, b.p0, pad, nullptr);
+void bvh_append_self(BvhBufs& b, cudaStream_t s, int64_t* launches) {
+  if (b.m < 2) return;
+  k_self<2><<<nq(b.m), 128, 0, s>>>(b, b.p0, false);
   *launches += 1;
 }
-void bvh_emit_static(BvhBufs& b, double pad, int2* out, cudaStream_t s, int64_t* launches) {
+void bvh_append_static(BvhBufs& b, double pad, int2* out, uint32_t cap, uint32_t* cnt, cudaStream_t s,
+                       int64_t* launches) {
   if (b.ms <= 0) return;
-  k_static<true><<<nb(b.ms), kBT, 0, s>>>(b, b.p0, pad, out);
+  k_static<<<nq(b.ms), 128, 0, s>>>(b, b.p0, pad, out, cap, cnt);
   *launches += 1;
 }
 
 // ---- candidates (contact-assembly.ts:87-121, self-collision.ts:23-41) -----------
-__device__ __forceinline__ void put_cand(int* rec, Key<4>* keys, uint32_t* pay, int slot, int kind, int p, int a,
-                                         int bb, int c, int d, int ns) {
+__device__ __forceinline__ void put_cand(int* rec, int slot, int kind, int p, int a, int bb, int c, int d) {
   int* r = rec + (size_t)slot * 6;
   r[0] = kind; r[1] = p; r[2] = a; r[3] = bb; r[4] = c; r[5] = d;
-  // ids shifted by ns + 2 so static ids -(i+2), -2 and -1 order below cloth ids; 24 bits each
-  const uint64_t off = (uint64_t)(ns + 2);
-  const uint64_t P = (uint64_t)((int64_t)p + off), A = (uint64_t)((int64_t)a + off), B = (uint64_t)((int64_t)bb + off);
-  const uint64_t Cc = (uint64_t)((int64_t)c + off), D = (uint64_t)((int64_t)d + off);
-  const uint64_t hi = ((uint64_t)kind << 56) | (P << 32) | (A << 8) | (B >> 16);
-  const uint64_t lo = ((B & 0xffffull) << 48) | (Cc << 24) | D;
-  keys[slot].w[0] = (uint32_t)(hi >> 32);
-  keys[slot].w[1] = (uint32_t)hi;
-  keys[slot].w[2] = (uint32_t)(lo >> 32);
-  keys[slot].w[3] = (uint32_t)lo;
-  pay[slot] = (uint32_t)slot;
 }
 
-__global__ void k_expand_self(CandBufs c, const uint32_t* idx, const int2* pairs, int np, int ns) {
+__global__ void k_expand_self(CandBufs c, const uint32_t* idx, const int2* pairs, int np) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= np) return;
   const int tA = pairs[i].x, tB = pairs[i].y;
   const int A[3] = {(int)idx[tA * 3], (int)idx[tA * 3 + 1], (int)idx[tA * 3 + 2]};
   const int B[3] = {(int)idx[tB * 3], (int)idx[tB * 3 + 1], (int)idx[tB * 3 + 2]};
   int slot = i * 15;
-  for (int k = 0; k < 3; k++) put_cand(c.rec, c.k0, c.p0, slot++, 0, A[k], B[0], B[1], B[2], -1, ns);
-  for (int k = 0; k < 3; k++) put_cand(c.rec, c.k0, c.p0, slot++, 0, B[k], A[0], A[1], A[2], -1, ns);
+  for (int k = 0; k < 3; k++) put_cand(c.rec, slot++, 0, A[k], B[0], B[1], B[2], -1);
+  for (int k = 0; k < 3; k++) put_cand(c.rec, slot++, 0, B[k], A[0], A[1], A[2], -1);
   const int TE[3][2] = {{0, 1}, {1, 2}, {2, 0}};
   for (int ea = 0; ea < 3; ea++)
     for (int eb = 0; eb < 3; eb++) {
       const int a = A[TE[ea][0]], bb = A[TE[ea][1]], cc = B[TE[eb][0]], d = B[TE[eb][1]];
-      if (a == cc || a == d || bb == cc || bb == d) put_cand(c.rec, c.k0, c.p0, slot++, 3, 0, 0, 0, 0, 0, ns);
-      else put_cand(c.rec, c.k0, c.p0, slot++, 1, -1, a, bb, cc, d, ns);
+      if (a == cc || a == d || bb == cc || bb == d) put_cand(c.rec, slot++, 3, 0, 0, 0, 0, 0);
+      else put_cand(c.rec, slot++, 1, -1, a, bb, cc, d);
     }
 }
 
 __global__ void k_expand_static(CandBufs c, const uint32_t* idx, const uint32_t* sidx, const int2* pairs, int np,
-                                int base, int ns) {
+                                int base) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= np) return;
   const int ct = pairs[i].x, st = pairs[i].y;
   const int A[3] = {(int)idx[ct * 3], (int)idx[ct * 3 + 1], (int)idx[ct * 3 + 2]};
   const int B[3] = {(int)sidx[st * 3], (int)sidx[st * 3 + 1], (int)sidx[st * 3 + 2]};
   int slot = base + i * 12;
-  for (int k = 0; k < 3; k++) put_cand(c.rec, c.k0, c.p0, slot++, 0, A[k], -(B[0] + 2), -(B[1] + 2), -(B[2] + 2), -2, ns);
+  for (int k = 0; k < 3; k++) put_cand(c.rec, slot++, 0, A[k], -(B[0] + 2), -(B[1] + 2), -(B[2] + 2), -2);
   const int E[3][2] = {{0, 1}, {1, 2}, {2, 0}};
   for (int e = 0; e < 3; e++)
     for (int f = 0; f < 3; f++)
-      put_cand(c.rec, c.k0, c.p0, slot++, 1, -1, A[E[e][0]], A[E[e][1]], -(B[E[f][0]] + 2), -(B[E[f][1]] + 2), ns);
+      put_cand(c.rec, slot++, 1, -1, A[E[e][0]], A[E[e][1]], -(B[E[f][0]] + 2), -(B[E[f][1]] + 2));
 }
 
-__global__ void k_gather_cand(const int* rec, const uint32_t* order, int n, int* out) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const int* r = rec + (size_t)order[i] * 6;
-  int* o = out + (size_t)i * 6;
-  for (int k = 0; k < 6; k++) o[k] = r[k];
-}
-
-void make_candidates(CandBufs& c, const uint32_t* idx, const uint32_t* sidx, int ns, const int2* selfPairs, int nSelf,
-                     const int2* staticPairs, int nStatic, cudaStream_t s, int64_t* launches) {
-  const int n = nSelf * 15 + nStatic * 12;
-  if (n == 0) return;
-  if (nSelf) { k_expand_self<<<nb(nSelf), kBT, 0, s>>>(c, idx, selfPairs, nSelf, ns); *launches += 1; }
+void expand_candidates(CandBufs& c, const uint32_t* idx, const uint32_t* sidx, int ns, const int2* selfPairs,
+                       int nSelf, const int2* staticPairs, int nStatic, cudaStream_t s, int64_t* launches) {
+  (void)ns;
+  if (nSelf) { k_expand_self<<<nb(nSelf), kBT, 0, s>>>(c, idx, selfPairs, nSelf); *launches += 1; }
   if (nStatic) {
-    k_expand_static<<<nb(nStatic), kBT, 0, s>>>(c, idx, sidx, staticPairs, nStatic, nSelf * 15, ns);
+    k_expand_static<<<nb(nStatic), kBT, 0, s>>>(c, idx, sidx, staticPairs, nStatic, nSelf * 15);
     *launches += 1;
   }
-  const bool flip = radix_sort<4>(c.k0, c.p0, c.k1, c.p1, n, 122, c.hist, s, launches);
-  k_gather_cand<<<nb(n), kBT, 0, s>>>(c.rec, flip ? c.p1 : c.p0, n, c.srt);
-  *launches += 1;
 }
 
 }  // namespace cs

@@ -25,7 +25,9 @@ struct CView {  // kernel view of the contact host buffers
   Contact c;
   int nCand, nFloor, n;
   const double* x0;  // xStep
-  const int* srt;
+  const int* rec;              // candidates in expansion order (6 ints each)
+  int ns, idBits;              // static vertex count, bits per id in the order key
+  unsigned long long* badKey;  // [hi, lo] smallest (key, status) of a failing CCD candidate
   uint32_t* cflag;
   uint32_t* fflag;
   double* cmin;
@@ -72,7 +74,7 @@ __device__ __forceinline__ void cand_closest(const CView& v, const double* x, co
 __global__ void k_cand_flags(CView v, const double* x, int C) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= C) return;
-  const int* r = v.srt + (size_t)i * 6;
+  const int* r = v.rec + (size_t)i * 6;
   if (r[0] == 3) { v.cflag[i] = 0; v.cmin[i] = INFINITY; return; }
   Closest cp;
   cand_closest(v, x, r, cp);
@@ -91,14 +93,33 @@ __global__ void k_floor_flags(CView v, const double* x) {
   v.fflag[i] = d >= v.c.dHat ? 0u : 1u;
 }
 
-__global__ void k_cand_compact(CView v, const double* x, int C) {
+__device__ __forceinline__ bool cand_active(const CView& v, int i) {
+  const double d = v.cmin[i];
+  return !(d >= v.c.dHat || d < 1e-12);
+}
+
+// The active candidates' order keys at their compacted positions (cflag holds
+// the exclusive scan of the activity flags); the payload is the candidate.
+__global__ void k_cand_keys(CView v, int C, Key<4>* keys, uint32_t* pay) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= C) return;
-  const int* r = v.srt + (size_t)i * 6;
-  if (r[0] == 3) return;
+  if (i >= C || !cand_active(v, i)) return;
+  const CandKey k = cand_key(v.rec + (size_t)i * 6, v.ns, v.idBits, 0, 0);
+  const uint32_t pos = v.cflag[i];
+  keys[pos].w[0] = (uint32_t)(k.hi >> 32);
+  keys[pos].w[1] = (uint32_t)k.hi;
+  keys[pos].w[2] = (uint32_t)(k.lo >> 32);
+  keys[pos].w[3] = (uint32_t)k.lo;
+  pay[pos] = (uint32_t)i;
+}
+
+// Frozen record j of the active set from the j-th candidate in key order
+// (updateActiveSet, contact-assembly.ts:164-220).
+__global__ void k_cand_active(CView v, const double* x, const uint32_t* order, int nAct) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= nAct) return;
+  const int* r = v.rec + (size_t)order[j] * 6;
   Closest cp;
   cand_closest(v, x, r, cp);
-  if (cp.dist >= v.c.dHat || cp.dist < 1e-12) return;
   Frozen f;
   f.kind = r[0]; f.p = r[1]; f.a = r[2]; f.b = r[3]; f.c = r[4]; f.d = r[5];
   f.nx = cp.rx / cp.dist; f.ny = cp.ry / cp.dist; f.nz = cp.rz / cp.dist;
@@ -109,7 +130,7 @@ __global__ void k_cand_compact(CView v, const double* x, int C) {
     f.p = -1;
     f.w0 = 1 - cp.s; f.w1 = cp.s; f.w2 = -(1 - cp.t); f.w3 = -cp.t;
   }
-  v.active[v.cflag[i]] = f;
+  v.active[j] = f;
 }
 
 __global__ void k_floor_compact(CView v, const double* x) {
@@ -390,17 +411,18 @@ __global__ void k_gather_vals(const double4* src, const uint32_t* order, int n, 
 }
 
 // ---- trial validation (contact-assembly.ts:489-553) ----------------------------------
-__global__ void k_trial_reset(int* cint) {
+__global__ void k_trial_reset(int* cint, unsigned long long* badKey) {
   cint[CI_FIRSTNF] = INT_MAX;
-  cint[CI_FIRSTBAD] = INT_MAX;
   cint[CI_FLOORBAD] = 0;
   cint[CI_VALID] = 0;
+  badKey[0] = ~0ull;
+  badKey[1] = ~0ull;
 }
 
 __global__ void k_trial_cand(CView v, const double* xt, int C, double dMin) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= C) return;
-  const int* r = v.srt + (size_t)i * 6;
+  const int* r = v.rec + (size_t)i * 6;
   v.cflag[i] = 0;
   v.ctoi[i] = INFINITY;
   if (r[0] == 3) { v.cmin[i] = INFINITY; return; }
@@ -427,7 +449,20 @@ __global__ void k_trial_cand(CView v, const double* xt, int C, double dMin) {
   if (isnan(toi)) st = 2;
   else if (toi > 0 && toi < 1 - 1e-9) st = 1;
   v.cflag[i] = st;
-  if (st) atomicMin(&v.cint[CI_FIRSTBAD], i);
+  // The reference stops at the first failing candidate in key order; its
+  // status (NaN or crossing) is the low two bits of the smallest (key, status).
+  if (st) atomicMin(&v.badKey[0], (unsigned long long)cand_key(r, v.ns, v.idBits, 2, st).hi);
+}
+
+// Second half of the smallest failing (key, status): the low word among the
+// failing candidates whose high word is the minimum.
+__global__ void k_trial_bad_lo(CView v, int C) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= C) return;
+  const uint32_t st = v.cflag[i];
+  if (!st) return;
+  const CandKey k = cand_key(v.rec + (size_t)i * 6, v.ns, v.idBits, 2, st);
+  if (k.hi == v.badKey[0]) atomicMin(&v.badKey[1], (unsigned long long)k.lo);
 }
 
 __global__ void k_trial_floor(CView v, const double* xt, double dMin) {
@@ -455,8 +490,8 @@ __global__ void k_trial_final(CView v, const double* partDist, const double* par
   if (v.cint[CI_FIRSTNF] != INT_MAX) {
     dg->ccdFailures += 1;
   } else if (minDist <= dMin) {
-  } else if (v.cint[CI_FIRSTBAD] != INT_MAX) {
-    if (v.cflag[v.cint[CI_FIRSTBAD]] == 2) dg->ccdFailures += 1;
+  } else if (v.badKey[0] != ~0ull) {
+    if ((v.badKey[1] & 3ull) == 2) dg->ccdFailures += 1;
   } else if (v.cint[CI_FLOORBAD]) {
   } else {
     valid = 1;
@@ -554,7 +589,10 @@ static CView view(ContactHost& h, Solver& s) {
   v.nFloor = h.nFloor;
   v.n = h.n;
   v.x0 = s.d.x0;
-  v.srt = h.cand.srt;
+  v.rec = h.cand.rec;
+  v.ns = h.ns;
+  v.idBits = h.idBits;
+  v.badKey = h.badKey;
   v.cflag = h.cflag;
   v.fflag = h.fflag;
   v.cmin = h.cmin;
@@ -580,8 +618,8 @@ ContactHost::~ContactHost() {
   for (void** q : {(void**)&spos, (void**)&sidx, (void**)&bvh.box64, (void**)&bvh.boxc, (void**)&bvh.boxr,
                    (void**)&bvh.cent, (void**)&bvh.scene, (void**)&bvh.k0, (void**)&bvh.k1, (void**)&bvh.p0,
                    (void**)&bvh.p1, (void**)&bvh.hist, (void**)&bvh.left, (void**)&bvh.right, (void**)&bvh.parent,
-                   (void**)&bvh.depth, (void**)&bvh.nbox, (void**)&bvh.visit, (void**)&bvh.root, (void**)&bvh.cnt,
-                   (void**)&bvh.pairs, (void**)&scnt, (void**)&spairs, (void**)&cand.rec, (void**)&cand.srt,
+                   (void**)&bvh.depth, (void**)&bvh.nbox, (void**)&bvh.rec, (void**)&bvh.visit, (void**)&bvh.root,
+                   (void**)&bvh.pairs, (void**)&badKey, (void**)&spairs, (void**)&cand.rec,
                    (void**)&cand.k0, (void**)&cand.k1, (void**)&cand.p0, (void**)&cand.p1, (void**)&cand.hist,
                    (void**)&cflag, (void**)&fflag, (void**)&cmin, (void**)&ctoi, (void**)&active, (void**)&dd,
                    (void**)&cg, (void**)&tc, (void**)&tf, (void**)&rk0, (void**)&rk1, (void**)&rp0, (void**)&rp1,
@@ -603,6 +641,7 @@ void ContactHost::init(Solver& s, const cs_contact_params* prm, int floor_on, do
   ns = nsv;
   ms = msv;
   if ((long)n + ns + 2 >= (1l << 24)) throw std::invalid_argument("too many vertices for the candidate key");
+  idBits = cand_id_bits(n, ns);
   if (ms > 0) {
     for (int i = 0; i < 3 * ms; i++)
       if ((int)si[i] >= ns) throw std::invalid_argument("static index out of range");
@@ -633,10 +672,10 @@ void ContactHost::init(Solver& s, const cs_contact_params* prm, int floor_on, do
   dalloc(bvh.parent, nn);
   dalloc(bvh.depth, nn);
   dalloc(bvh.nbox, 6 * nn);
+  dalloc(bvh.rec, 4 * (size_t)std::max(1, m - 1));
   dalloc(bvh.visit, nn);
   dalloc(bvh.root, 1);
-  dalloc(bvh.cnt, (size_t)m + 1);
-  dalloc(scnt, (size_t)std::max(ms, 1) + 1);
+  dalloc(badKey, 2);
   dalloc(fflag, (size_t)n + 1);
   dalloc(cOff, (size_t)n + 1);
   dalloc(lagFloor, (size_t)n);
@@ -664,7 +703,6 @@ void ContactHost::ensure_cands(size_t nc) {
   const size_t c = nc + nc / 2 + 256;
   cand.cap = (int)c;
   dalloc(cand.rec, 6 * c);
-  dalloc(cand.srt, 6 * c);
   dalloc(cand.k0, c);
   dalloc(cand.k1, c);
   dalloc(cand.p0, c);
@@ -744,28 +782,33 @@ int ContactHost::build_candidates(Solver& s, const double* x, double pad) {
   cudaStream_t st = s.stream;
   int64_t& lc = launch_counter();
   CK(cudaMemsetAsync(cint, 0, CI_N * sizeof(int), st));
-  bvh_build(bvh, s.d.x0, x, pad, false, st, &lc);
-  bvh_count_self(bvh, false, st, &lc);
-  scan_counts(bvh.cnt, m, (uint32_t*)(cint + CI_SELF), st, &lc);
-  BvhBufs sb = bvh;
-  sb.cnt = scnt;
-  if (ms > 0) {
-    bvh_count_static(sb, pad, st, &lc);
-    scan_counts(scnt, ms, (uint32_t*)(cint + CI_STATIC), st, &lc);
+  // The hierarchy is built once per step and refitted for every later segment:
+  // the exact pair set does not depend on the tree's shape.
+  if (!topoValid) {
+    bvh_build(bvh, s.d.x0, x, pad, false, st, &lc);
+    topoValid = true;
+  } else {
+    bvh_refit(bvh, s.d.x0, x, pad, false, st, &lc);
   }
-  read_ints(s);
-  if (hint[CI_OVERFLOW]) throw CapacityError("broadphase traversal aborted (stack deeper than 64 or malformed tree)");
+  for (int attempt = 0; attempt < 2; attempt++) {
+    BvhBufs sb = bvh;
+    sb.cnt = (uint32_t*)(cint + CI_SELF);
+    sb.pairCap = (uint32_t)pairCap;
+    bvh_append_self(sb, st, &lc);
+    if (ms > 0) bvh_append_static(bvh, pad, spairs, (uint32_t)spairCap, (uint32_t*)(cint + CI_STATIC), st, &lc);
+    read_ints(s);
+    if (hint[CI_OVERFLOW]) throw CapacityError("broadphase traversal aborted (stack deeper than 64 or malformed tree)");
+    const uint32_t P = (uint32_t)hint[CI_SELF], S = ms > 0 ? (uint32_t)hint[CI_STATIC] : 0u;
+    if (P <= pairCap && S <= spairCap) break;
+    if (attempt == 1) throw CapacityError("broadphase pair count changed between identical traversals");
+    ensure_pairs(P, S);
+    CK(cudaMemsetAsync(cint + CI_SELF, 0, 2 * sizeof(int), st));
+  }
   const int P = hint[CI_SELF], S = ms > 0 ? hint[CI_STATIC] : 0;
-  ensure_pairs(P, S);
-  if (P > 0) bvh_emit_self(bvh, false, st, &lc);
-  if (S > 0) {
-    sb.pairs = bvh.pairs;
-    bvh_emit_static(sb, pad, spairs, st, &lc);
-  }
   const long C = 15l * P + 12l * S;
   if (C > INT_MAX / 8) throw CapacityError("too many contact candidates");
   ensure_cands(C);
-  make_candidates(cand, s.idx.p, sidx, ns, bvh.pairs, P, spairs, S, st, &lc);
+  expand_candidates(cand, s.idx.p, sidx, ns, bvh.pairs, P, spairs, S, st, &lc);
   return (int)C;
 }
 
@@ -794,8 +837,13 @@ void ContactHost::update_active_set(Solver& s, double* x) {
   const int na = nCand + nFloor;
   ensure_active(s, na);
   v = view(*this, s);
-  if (C > 0) {
-    k_cand_compact<<<cnb(C), kCT, 0, st>>>(v, x, C);
+  if (nCand > 0) {
+    // Only the active candidates are put in the reference's (kind, p, a, b, c, d) order.
+    k_cand_keys<<<cnb(C), kCT, 0, st>>>(v, C, cand.k0, cand.p0);
+    lc++;
+    const bool flip = radix_sort<4>(cand.k0, cand.p0, cand.k1, cand.p1, nCand, cand_key_bits(idBits, 0), cand.hist,
+                                    st, &lc);
+    k_cand_active<<<cnb(nCand), kCT, 0, st>>>(v, x, flip ? cand.p1 : cand.p0, nCand);
     lc++;
   }
   k_floor_compact<<<cnb(n), kCT, 0, st>>>(v, x);
@@ -857,11 +905,13 @@ bool ContactHost::check_trial(Solver& s, const double* xt) {
   int64_t& lc = launch_counter();
   const int C = build_candidates(s, xt, p.dmin);
   candidatePairs = C;
-  k_trial_reset<<<1, 1, 0, st>>>(cint);
+  k_trial_reset<<<1, 1, 0, st>>>(cint, badKey);
+  lc++;
   CView v = view(*this, s);
   if (C > 0) {
     k_trial_cand<<<cnb(C), kCT, 0, st>>>(v, xt, C, p.dmin);
-    lc++;
+    k_trial_bad_lo<<<cnb(C), kCT, 0, st>>>(v, C);
+    lc += 2;
   }
   k_trial_floor<<<cnb(n), kCT, 0, st>>>(v, xt, p.dmin);
   k_min_part<<<kMinBlocks, 256, 0, st>>>(cmin, C, v.vtmp, n, minpart);
@@ -922,6 +972,7 @@ void ContactHost::begin_step_and_bisect(Solver& s) {
   lagCount = 0;
   commitNo = 0;
   rejections = 0;
+  topoValid = false;
   candidatePairs = activePairs = vtPairs = eePairs = floorPairs = 0;
   nCand = nFloor = nVT = 0;
   bind(s);

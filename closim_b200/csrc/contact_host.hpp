@@ -28,7 +28,7 @@ struct DevDiag {
 };
 
 // Device counters read back by the host (int32).
-enum CInt { CI_SELF = 0, CI_STATIC, CI_OVERFLOW, CI_NCAND, CI_NFLOOR, CI_NVT, CI_VALID, CI_FIRSTNF, CI_FIRSTBAD,
+enum CInt { CI_SELF = 0, CI_STATIC, CI_OVERFLOW, CI_NCAND, CI_NFLOOR, CI_NVT, CI_VALID, CI_FIRSTNF,
             CI_FLOORBAD, CI_N = 16 };
 
 class ContactHost {
@@ -47,11 +47,13 @@ class ContactHost {
   uint32_t* sidx = nullptr;
   // broadphase
   BvhBufs bvh;
-  uint32_t* scnt = nullptr;    // ms + 1
   int2* spairs = nullptr;
+  unsigned long long* badKey = nullptr;  // smallest failing (key, status) of a trial
+  int idBits = 24;             // bits per id in the candidate order key
+  bool topoValid = false;      // hierarchy built for the current step
   size_t pairCap = 0, spairCap = 0;
   CandBufs cand;
-  uint32_t* cflag = nullptr;   // per-candidate flag / offset (cand cap + 1)
+  uint32_t* cflag = nullptr;   // per-candidate flag / offset / trial status (cand cap + 1)
   uint32_t* fflag = nullptr;   // per-vertex floor flag / offset (n + 1)
   double* cmin = nullptr;      // per-candidate distance (cand cap)
   double* ctoi = nullptr;      // per-candidate toi
