@@ -1,7 +1,8 @@
 """Benchmark of the CUDA cloth step: sim steps/s on the floor-drape workload.
 
 python bench.py --gpus N --steps K --warmup W [--impl cuda|reference]
-                [--workload floor_drape|strip_pull] [--precision fp64|mixed]
+                [--workload floor_drape|strip_pull|sphere_drape] [--precision fp64|mixed|both]
+                [--skip S]   # S extra untimed steps before timing (e.g. to reach contact)
 
 One process per GPU (torchrun for N > 1); every rank steps its own replica of
 the workload (a single sheet does not shard: "replicas only", weak scaling).
@@ -98,6 +99,8 @@ def workload(name: str, steps_hint: int):
         return configs.floor_drape()
     if name == "strip_pull":
         return configs.strip_pull()
+    if name == "sphere_drape":
+        return configs.sphere_drape()
     raise SystemExit(f"unknown workload {name}")
 
 
@@ -144,6 +147,13 @@ def run_reference(args, rank):
     return 0
 
 
+def pcg_kernel_name(precision, prof):
+    if precision != "mixed":
+        return "k_pcg"
+    info = prof.get("launch_info") or {}
+    return "k_mx_pcg_cluster" if info.get("pcgClusterCtas") else "k_mx_pcg"
+
+
 def run_precision(cfg, precision, local, args, ext_stream_cb, flush, sampler=None, prof_out=None):
     """Warm-up W steps, then K device-resident steps, each bracketed by CUDA
     events on the solver's stream after an L2 flush. Returns (ms_total, solver,
@@ -162,7 +172,7 @@ def run_precision(cfg, precision, local, args, ext_stream_cb, flush, sampler=Non
         sc.pinned.update(configs.pins_at(cfg, k[0] % cfg["steps"]))
         k[0] += 1
 
-    for _ in range(args.warmup):
+    for _ in range(args.warmup + args.skip):
         set_pins()
         solver.advance(cfg["h"], 1)
     torch.cuda.synchronize()
@@ -188,6 +198,17 @@ def run_precision(cfg, precision, local, args, ext_stream_cb, flush, sampler=Non
         prof_out.update(solver.profileRead())
     solver.profile(False)
     launches = solver.kernelLaunches() - launches0
+    if prof_out is not None:
+        prof_out["launch_info"] = solver.launchInfo()
+    if prof_out is not None and args.phase_steps > 0:
+        # wall-time breakdown over a few extra (untimed) steps
+        solver.profile(True, phases=True)
+        for _ in range(args.phase_steps):
+            set_pins()
+            solver.advance(cfg["h"], 1)
+        torch.cuda.synchronize()
+        prof_out["phases_ms_per_step"] = {k: v / args.phase_steps for k, v in solver.profilePhases().items()}
+        solver.profile(False)
     solver.pull()
     return total, solver, sc, sc.positions.copy(), launches, ext, set_pins
 
@@ -198,7 +219,9 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
-    ap.add_argument("--workload", default="floor_drape", choices=["floor_drape", "strip_pull"])
+    ap.add_argument("--workload", default="floor_drape", choices=["floor_drape", "strip_pull", "sphere_drape"])
+    ap.add_argument("--skip", type=int, default=0, help="extra untimed steps before the timed region")
+    ap.add_argument("--phase-steps", type=int, default=3, help="extra steps for the per-phase wall-time breakdown")
     ap.add_argument("--small", action="store_true", help="32x32 floor drape (for profiler captures)")
     ap.add_argument("--precision", default="both", choices=["both", "fp64", "mixed"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -284,7 +307,7 @@ def main():
             "config": {"workload": cfg["name"] + ("_32x32" if args.small else ""), "n": n, "m": len(cfg["idx"]) // 3,
                        "h": cfg["h"], "precision": headline, "precond": cfg["options"]["precond"],
                        "parallelism": f"replicas x{world}", "l2": "flushed between timed steps (256 MiB write)"},
-            "roofline": {"bound": "hbm", "kernel": "k_mx_pcg" if headline == "mixed" else "k_pcg",
+            "roofline": {"bound": "hbm", "kernel": pcg_kernel_name(headline, prof),
                          "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": None, "launches": prof.get("launches"),
                          "ms_per_launch": prof.get("ms_per_launch"), "pcg_iters": prof.get("iters"),
@@ -293,14 +316,18 @@ def main():
             "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": res[headline]["launches"],
             "clocks": clocks,
+            "phases_ms_per_step": prof.get("phases_ms_per_step"),
+            "launch_info": prof.get("launch_info"),
         }
+        if args.skip:
+            line["config"]["untimed_steps_before"] = args.warmup + args.skip
         if "fp64" in res and headline == "mixed":
             a, b = res["fp64"]["pos"], res["mixed"]["pos"]
             line["fp64_path"] = {"value": world * args.steps / (fp64_ms / 1000.0), "unit": "steps/s",
                                  "ms_per_step": fp64_ms / args.steps,
                                  "gpu_launches": res["fp64"]["launches"]}
             line["mixed_vs_fp64_rel_pos_err"] = float(np.max(np.abs(b - a)) / np.max(np.abs(a)))
-            line["mixed_vs_fp64_steps"] = args.warmup + args.steps
+            line["mixed_vs_fp64_steps"] = args.warmup + args.skip + args.steps
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(cfg, budget_s=20.0, max_steps=cfg["steps"])
         print(json.dumps(line), flush=True)

@@ -54,7 +54,8 @@ class cs_broadphase_diag(C.Structure):
 EXPORTS = ["cs_create", "cs_destroy", "cs_last_error", "cs_initialize", "cs_set_contact",
            "cs_set_stepper_options", "cs_set_material", "cs_set_pins", "cs_step", "cs_get_positions",
            "cs_get_velocities", "cs_set_state", "cs_last_stats", "cs_membrane_hvp", "cs_step_n", "cs_sync",
-           "cs_kernel_launches", "cs_stream", "cs_profile", "cs_profile_read", "cs_build_grid",
+           "cs_kernel_launches", "cs_stream", "cs_profile", "cs_profile_read", "cs_profile_phases", "cs_solver_info", "cs_forward", "cs_backward",
+           "cs_set_adjoint_options", "cs_adjoint_stats", "cs_set_newton_mode", "cs_build_grid",
            "cs_preprocess", "cs_broadphase_create", "cs_broadphase_destroy", "cs_broadphase_last_error",
            "cs_broadphase_build", "cs_broadphase_diagnostics", "cs_broadphase_pairs", "cs_broadphase_state"]
 
@@ -93,6 +94,13 @@ def load():
         "cs_stream": (vp, [vp]),
         "cs_profile": (C.c_int, [vp, C.c_int]),
         "cs_profile_read": (C.c_int, [vp, vp]),
+        "cs_profile_phases": (C.c_int, [vp, vp, C.c_int32]),
+        "cs_solver_info": (C.c_int, [vp, vp, C.c_int32]),
+        "cs_forward": (C.c_int, [vp, C.c_double, C.c_int32, C.c_int32]),
+        "cs_backward": (C.c_int, [vp, vp, vp, vp]),
+        "cs_set_adjoint_options": (C.c_int, [vp, C.c_int32, C.c_double]),
+        "cs_adjoint_stats": (C.c_int, [vp, vp]),
+        "cs_set_newton_mode": (C.c_int, [vp, C.c_int32, C.c_double]),
         "cs_build_grid": (C.c_int, [C.c_int32, C.c_int32, C.c_double, C.c_double, vp, vp, vp]),
         "cs_preprocess": (C.c_int, [C.c_int32, C.c_int32, vp, vp, vp, C.c_double, vp, vp, vp,
                                     C.POINTER(C.c_int32), vp, vp]),

@@ -779,6 +779,16 @@ void ContactHost::read_ints(Solver& s) {
 }
 
 int ContactHost::build_candidates(Solver& s, const double* x, double pad) {
+  struct Restore {
+    Solver& s;
+    int prev;
+    ~Restore() {
+      try {
+        s.phase(prev);
+      } catch (...) {
+      }
+    }
+  } restore{s, s.phase(PH_BROADPHASE)};
   cudaStream_t st = s.stream;
   int64_t& lc = launch_counter();
   CK(cudaMemsetAsync(cint, 0, CI_N * sizeof(int), st));

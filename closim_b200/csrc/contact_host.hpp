@@ -87,6 +87,12 @@ class ContactHost {
   void init(Solver& s, const cs_contact_params* prm, int floor_on, double floor_y, const float* sp, int nsv,
             const uint32_t* si, int msv);
   void begin_step_and_bisect(Solver& s);
+  // Start of an independent evaluation at a new segment (the adjoint sweep):
+  // the hierarchy is rebuilt at the next query.
+  void begin_segment(Solver& s) {
+    topoValid = false;
+    (void)s;
+  }
   void update_active_set(Solver& s, double* x);
   void merit_energy(Solver& s, const double* x);
   void gradient_terms(Solver& s);

@@ -16,6 +16,11 @@ struct MixBufs {
 void mx_prepare(const Dev& d, const MixBufs& mb, bool schwarz, cudaStream_t s, int64_t* lc);
 int mx_pcg_grid_blocks(const Dev& d);
 int mx_launch_pcg(const Dev& d, const MixBufs& mb, int maxIters, double tol, int blocks, cudaStream_t s);
+// One-cluster PCG (mixed_cluster.cu): pA/pB are 3n-float direction buffers,
+// coef one double per active contact.
+int mx_cluster_size();
+int mx_launch_pcg_cluster(const Dev& d, const MixBufs& mb, float* pA, float* pB, double* coef, int maxIters,
+                          double tol, int clusterSize, cudaStream_t s);
 void mx_grad_final(const Dev& d, cudaStream_t s, int64_t* lc);
 void mx_energy_final(const Dev& d, cudaStream_t s, int64_t* lc);
 

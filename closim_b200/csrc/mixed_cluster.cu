@@ -1,0 +1,425 @@
+// Mixed-precision PCG (pcg.ts:11-95 + the newton.ts:152-179 epilogue) run by
+// ONE thread-block cluster: up to 16 CTAs on one GPC, synchronized with the
+// hardware cluster barrier and reducing through distributed shared memory.
+// For sheets that fit a cluster this replaces a grid-wide barrier (a round
+// trip through L2 and every SM) with an on-GPC one, and fuses each iteration
+// into two phases:
+//
+//   A  per vertex: p_k = z + beta p_{k-1} formed on the fly for the vertex and
+//      its element neighbours, the membrane HVP of every incident triangle
+//      (corner share only) from the stored FP32 (F, S), the frozen-contact
+//      HVP, Ap = M/h^2 p + H p; partial p.Ap          -- cluster barrier --
+//   B  per Schwarz domain (one warp, lane = local dof) or per dof (Jacobi):
+//      alpha, x += alpha p, r -= alpha Ap, z = M^-1 r; partial r.r and r.z
+//                                                      -- cluster barrier --
+//
+// Every dot product accumulates in FP64; each CTA's partial is read by every
+// CTA in rank order, so all CTAs take the same branch and the result does not
+// depend on timing. Compiled with FMA contraction on.
+#include <cooperative_groups.h>
+
+#include "contact.cuh"
+#include "mixed.cuh"
+
+namespace cg = cooperative_groups;
+
+namespace cs {
+
+constexpr int kClT = 512;
+
+struct ClArgs {
+  Dev d;
+  MixBufs mb;
+  float* pA;      // search direction, double-buffered (3n each)
+  float* pB;
+  double* coef;   // per active contact: barrier curvature at the frozen distance (0 outside dHat)
+  int maxIters;
+  double tol;
+};
+
+// Cluster-wide totals of `k` partials deposited in red[0..k) by every CTA.
+// Lane r of warp 0 reads CTA r's partials, a fixed shuffle tree adds them, and
+// the result is broadcast through shared memory: identical bits in every CTA.
+template <int K>
+__device__ __forceinline__ void cl_totals(cg::cluster_group& cl, double* red, double* out, double* bc) {
+  if (threadIdx.x < 32) {
+    const unsigned nr = cl.num_blocks();
+    double v[K];
+#pragma unroll
+    for (int k = 0; k < K; k++) v[k] = 0;
+    if (threadIdx.x < nr) {
+      const double* peer = cl.map_shared_rank(red, threadIdx.x);
+#pragma unroll
+      for (int k = 0; k < K; k++) v[k] = peer[k];
+    }
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+      double s = v[k];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+      if (threadIdx.x == 0) bc[k] = s;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < K; k++) out[k] = bc[k];
+  __syncthreads();
+}
+
+__device__ __forceinline__ float3 ld_p(const float* z, const float* pc, float beta, bool first, int v) {
+  const float z0 = z[v * 3], z1 = z[v * 3 + 1], z2 = z[v * 3 + 2];
+  if (first) return make_float3(z0, z1, z2);
+  return make_float3(__fmaf_rn(beta, pc[v * 3], z0), __fmaf_rn(beta, pc[v * 3 + 1], z1),
+                     __fmaf_rn(beta, pc[v * 3 + 2], z2));
+}
+
+// Corner share of one triangle's membrane HVP (membrane-hvp.ts:18-75):
+// dF = Ds(p) Dm^-1, dE, dS, dP = dF S + F dS, force = -area * dP Dm^-T.
+__device__ __forceinline__ void tri_hvp_corner(const float* T, const float3 p0, const float3 p1, const float3 p2,
+                                               int corner, float C00, float C11, float C01, float G, float o[3]) {
+  const float4 t0 = __ldg((const float4*)T), t1 = __ldg((const float4*)(T + 4)), t2 = __ldg((const float4*)(T + 8)),
+               t3 = __ldg((const float4*)(T + 12));
+  const float F0[3] = {t0.x, t0.y, t0.z}, F1[3] = {t0.w, t1.x, t1.y};
+  const float S00 = t1.z, S11 = t1.w, S01 = t2.x;
+  const float a = t2.y, b = t2.z, c = t2.w, dd = t3.x, s = t3.y;
+  const float w1[3] = {p1.x - p0.x, p1.y - p0.y, p1.z - p0.z};
+  const float w2[3] = {p2.x - p0.x, p2.y - p0.y, p2.z - p0.z};
+  float dF0[3], dF1[3];
+#pragma unroll
+  for (int q = 0; q < 3; q++) { dF0[q] = a * w1[q] + c * w2[q]; dF1[q] = b * w1[q] + dd * w2[q]; }
+  const float dE00 = F0[0] * dF0[0] + F0[1] * dF0[1] + F0[2] * dF0[2];
+  const float dE11 = F1[0] * dF1[0] + F1[1] * dF1[1] + F1[2] * dF1[2];
+  const float dE01 = 0.5f * (dF0[0] * F1[0] + F0[0] * dF1[0] + dF0[1] * F1[1] + F0[1] * dF1[1] + dF0[2] * F1[2] +
+                             F0[2] * dF1[2]);
+  const float dS00 = C00 * dE00 + C01 * dE11;
+  const float dS11 = C11 * dE11 + C01 * dE00;
+  const float dS01 = 2.f * G * dE01;
+#pragma unroll
+  for (int q = 0; q < 3; q++) {
+    const float P0 = dF0[q] * S00 + F0[q] * dS00 + dF1[q] * S01 + F1[q] * dS01;
+    const float P1 = dF0[q] * S01 + F0[q] * dS01 + dF1[q] * S11 + F1[q] * dS11;
+    const float g1 = s * (P0 * a + P1 * b);
+    const float g2 = s * (P0 * c + P1 * dd);
+    o[q] = corner == 0 ? -(g1 + g2) : corner == 1 ? g1 : g2;
+  }
+}
+
+// Jacobian of the frozen distance along the current direction (distJvp,
+// contact-assembly.ts:394-414), with p formed on the fly. FP64.
+__device__ __forceinline__ double cl_jvp(const Frozen& f, const float* z, const float* pc, float beta, bool first) {
+  if (f.kind == 2) return (double)ld_p(z, pc, beta, first, f.p).y;
+  const int vs[4] = {f.kind == 0 ? f.p : f.a, f.kind == 0 ? f.a : f.b, f.kind == 0 ? f.b : f.c,
+                     f.kind == 0 ? f.c : f.d};
+  double nv[4];
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    nv[q] = 0;
+    if (vs[q] >= 0) {
+      const float3 pv = ld_p(z, pc, beta, first, vs[q]);
+      nv[q] = f.nx * (double)pv.x + f.ny * (double)pv.y + f.nz * (double)pv.z;
+    }
+  }
+  if (f.kind == 0) return nv[0] - f.w0 * nv[1] - f.w1 * nv[2] - f.w2 * nv[3];
+  return f.w0 * nv[0] + f.w1 * nv[1] + f.w2 * nv[2] + f.w3 * nv[3];
+}
+
+// Phase B on one Schwarz domain: lane = local dof. Returns (r.r, r.z) shares.
+__device__ __forceinline__ void cl_domain(const Dev& d, const MixBufs& mb, const float* pn, float alpha, bool init,
+                                          int dom, double& rr, double& rz) {
+  const int lane = threadIdx.x & 31;
+  const int start = d.domStart[dom], dw = (d.domStart[dom + 1] - start) * 3;
+  float rv = 0.f;
+  int gi = -1;
+  bool pin = false;
+  if (lane < dw) {
+    gi = d.domVerts[start + lane / 3] * 3 + lane % 3;
+    pin = d.pinned[gi / 3];
+    float xi, ri;
+    if (init) {
+      xi = 0.f;
+      ri = (float)(-d.g[gi]);
+    } else {
+      xi = mb.x[gi] + alpha * pn[gi];
+      ri = mb.r[gi] - alpha * mb.Ap[gi];
+    }
+    if (pin) { xi = 0.f; ri = 0.f; }
+    mb.x[gi] = xi;
+    mb.r[gi] = ri;
+    rv = ri;
+    rr += (double)ri * ri;
+  }
+  const float* Li = mb.Linv + (size_t)dom * 576 + lane * 24;
+  float z = 0.f;
+#pragma unroll
+  for (int j = 0; j < 24; j++) {
+    const float rj = __shfl_sync(0xffffffffu, rv, j);
+    if (lane < dw) z = fmaf(__ldg(Li + j), rj, z);
+  }
+  if (lane < dw) {
+    if (pin) z = 0.f;
+    mb.z[gi] = z;
+    rz += (double)rv * z;
+  }
+}
+
+__device__ __forceinline__ void cl_dof(const Dev& d, const MixBufs& mb, const float* pn, float alpha, bool init, int i,
+                                       double& rr, double& rz) {
+  const bool pin = d.pinned[i / 3];
+  float xi, ri;
+  if (init) {
+    xi = 0.f;
+    ri = (float)(-d.g[i]);
+  } else {
+    xi = mb.x[i] + alpha * pn[i];
+    ri = mb.r[i] - alpha * mb.Ap[i];
+  }
+  if (pin) { xi = 0.f; ri = 0.f; }
+  mb.x[i] = xi;
+  mb.r[i] = ri;
+  rr += (double)ri * ri;
+  float zi = d.diag[i] > 1e-12 ? (float)((double)ri / d.diag[i]) : ri;
+  if (pin) zi = 0.f;
+  mb.z[i] = zi;
+  rz += (double)ri * zi;
+}
+
+__global__ void __launch_bounds__(kClT, 1) k_mx_pcg_cluster(ClArgs A) {
+  cg::cluster_group cl = cg::this_cluster();
+  __shared__ double sm[32];
+  // Partials alternate between two banks: a bank is rewritten only after the
+  // cluster barrier that follows every CTA's read of it.
+  __shared__ double red[2][4];
+  __shared__ double bc[4];
+  int round = 0;
+  const Dev& d = A.d;
+  const MixBufs& mb = A.mb;
+  const int n3 = d.n * 3;
+  const int rank = (int)cl.block_rank(), nrank = (int)cl.num_blocks();
+  const int tid = rank * blockDim.x + threadIdx.x, nth = nrank * blockDim.x;
+  const int gwarp = tid >> 5, nwarps = nth >> 5;
+  const bool jacobi = d.precond == 0;
+  const float invH2 = (float)d.invH2;
+  const float C00 = mb.C00, C11 = mb.C11, C01 = mb.C01, G = mb.G;
+
+  // ---- init: r = -g (filtered), x = 0, z = M^-1 r; |b|^2, r.r, r.z -------------------
+  double bb = 0, rr = 0, rz = 0;
+  for (int i = tid; i < n3; i += nth) {
+    const double bi = -d.g[i];
+    bb += bi * bi;
+  }
+  if (jacobi) {
+    for (int i = tid; i < n3; i += nth) cl_dof(d, mb, nullptr, 0.f, true, i, rr, rz);
+  } else {
+    for (int dom = gwarp; dom < d.D; dom += nwarps) cl_domain(d, mb, nullptr, 0.f, true, dom, rr, rz);
+  }
+  if (d.hasContact) {
+    const Contact& c = d.c;
+    for (int i = tid; i < c.nActive; i += nth) {
+      const double dist = js_max(frozen_dist(c, d.x, c.active[i]), 1e-12);
+      A.coef[i] = dist < c.dHat ? barrier_curvature(dist, c.dHat, c.kappa) : 0.0;
+    }
+  }
+  {
+    const double s0 = block_sum(bb, sm), s1 = block_sum(rr, sm), s2 = block_sum(rz, sm);
+    if (threadIdx.x == 0) { red[round & 1][0] = s0; red[round & 1][1] = s1; red[round & 1][2] = s2; }
+  }
+  cl.sync();
+  double tot[3];
+  cl_totals<3>(cl, red[round & 1], tot, bc);
+  round++;
+  double rzCur = tot[2];
+  const double bNorm = sqrt(tot[0]);
+  const double absTol = fmax(A.tol * fmax(bNorm, 1e-12), 1e-12);
+  double residual = sqrt(tot[1]);
+  int iters = 0;
+  bool done = residual < absTol;
+  float beta = 0.f;
+  bool first = true;
+  float* pc = A.pA;  // p_{k-1}
+  float* pn = A.pB;  // p_k
+  int k = 0;
+  for (; !done && k < A.maxIters; k++) {
+    // ---- phase A: p_k, Ap_k, p.Ap ------------------------------------------------
+    double pAp = 0;
+    for (int v = tid; v < d.n; v += nth) {
+      const float3 pv = ld_p(mb.z, pc, beta, first, v);
+      float sp[3] = {0.f, 0.f, 0.f};
+      for (uint32_t q = d.memOff[v]; q < d.memOff[v + 1]; q++) {
+        const uint32_t rec = __ldg(d.memRec + q);
+        const uint32_t t = rec >> 2;
+        const int i0 = (int)__ldg(d.idx + t * 3), i1 = (int)__ldg(d.idx + t * 3 + 1), i2 = (int)__ldg(d.idx + t * 3 + 2);
+        const float3 p0 = ld_p(mb.z, pc, beta, first, i0), p1 = ld_p(mb.z, pc, beta, first, i1),
+                     p2 = ld_p(mb.z, pc, beta, first, i2);
+        float o[3];
+        tri_hvp_corner(mb.tris + (size_t)t * 16, p0, p1, p2, (int)(rec & 3), C00, C11, C01, G, o);
+        sp[0] += o[0]; sp[1] += o[1]; sp[2] += o[2];
+      }
+      double ch[3] = {0, 0, 0};
+      if (d.hasContact) {
+        const Contact& c = d.c;
+        for (uint32_t q = c.cOff[v]; q < c.cOff[v + 1]; q++) {
+          const uint32_t rec = c.cRec[q];
+          const double g = A.coef[rec >> 2];
+          if (g == 0) continue;
+          const Frozen f = c.active[rec >> 2];
+          dist_grad_slot(f, rec & 3, g * cl_jvp(f, mb.z, pc, beta, first), ch);
+        }
+      }
+      const float M = d.mass[v];
+      const bool pin = d.pinned[v];
+      const float pvv[3] = {pv.x, pv.y, pv.z};
+#pragma unroll
+      for (int q = 0; q < 3; q++) {
+        const int i = v * 3 + q;
+        float ap = M * pvv[q] * invH2 + sp[q] + (float)ch[q];
+        if (pin) ap = 0.f;
+        pn[i] = pvv[q];
+        mb.Ap[i] = ap;
+        pAp += (double)pvv[q] * ap;
+      }
+    }
+    {
+      const double s = block_sum(pAp, sm);
+      if (threadIdx.x == 0) red[round & 1][0] = s;
+    }
+    cl.sync();
+    cl_totals<1>(cl, red[round & 1], tot, bc);
+    round++;
+    const double pApT = tot[0];
+    if (!(pApT > 1e-30)) { iters = k; done = true; break; }
+    const float alpha = (float)(rzCur / pApT);
+    // ---- phase B: x, r, z; r.r, r.z ---------------------------------------------
+    rr = 0;
+    rz = 0;
+    if (jacobi) {
+      for (int i = tid; i < n3; i += nth) cl_dof(d, mb, pn, alpha, false, i, rr, rz);
+    } else {
+      for (int dom = gwarp; dom < d.D; dom += nwarps) cl_domain(d, mb, pn, alpha, false, dom, rr, rz);
+    }
+    {
+      const double s0 = block_sum(rr, sm), s1 = block_sum(rz, sm);
+      if (threadIdx.x == 0) { red[round & 1][0] = s0; red[round & 1][1] = s1; }
+    }
+    cl.sync();
+    double t2[2];
+    cl_totals<2>(cl, red[round & 1], t2, bc);
+    round++;
+    residual = sqrt(t2[0]);
+    if (residual < absTol) { iters = k + 1; done = true; break; }
+    beta = (float)(t2[1] / rzCur);
+    rzCur = t2[1];
+    first = false;
+    float* tmp = pc;
+    pc = pn;
+    pn = tmp;
+  }
+  if (!done) iters = A.maxIters;
+
+  // ---- descent safeguard + trust region in FP64 (newton.ts:152-179) -------------------
+  double gt = 0;
+  for (int i = tid; i < n3; i += nth) {
+    const double di = mb.x[i];
+    d.dx[i] = di;
+    gt += d.g[i] * di;
+  }
+  {
+    const double s = block_sum(gt, sm);
+    if (threadIdx.x == 0) red[round & 1][0] = s;
+  }
+  cl.sync();
+  double t1[1];
+  cl_totals<1>(cl, red[round & 1], t1, bc);
+  round++;
+  double gtdx = t1[0];
+  bool fallback = false;
+  if (!isfinite(gtdx) || gtdx >= 0) {
+    fallback = true;
+    gt = 0;
+    for (int i = tid; i < n3; i += nth) {
+      const double di = -d.g[i] / d.diag[i];
+      d.dx[i] = di;
+      gt += d.g[i] * di;
+    }
+    const double s = block_sum(gt, sm);
+    if (threadIdx.x == 0) red[round & 1][0] = s;
+    cl.sync();
+    cl_totals<1>(cl, red[round & 1], t1, bc);
+    round++;
+    gtdx = t1[0];
+  }
+  double mxd = 0;
+  for (int i = tid; i < n3; i += nth) mxd = fmax(mxd, fabs(d.dx[i]));
+  {
+    const double s = block_max(mxd, sm);
+    if (threadIdx.x == 0) red[round & 1][0] = s;
+    cl.sync();
+    if (threadIdx.x == 0) {
+      double r = 0;
+      for (int q = 0; q < nrank; q++) r = fmax(r, *cl.map_shared_rank(&red[round & 1][0], q));
+      bc[0] = r;
+    }
+    __syncthreads();
+    round++;
+  }
+  const double maxDx = bc[0];
+  if (maxDx > 0.002) {
+    const double s = 0.002 / maxDx;
+    for (int i = tid; i < n3; i += nth) d.dx[i] *= s;
+    gtdx *= s;
+  }
+  if (rank == 0 && threadIdx.x == 0) {
+    d.scal[S_PCG_ITERS] = iters;
+    d.scal[S_PCG_RES] = residual;
+    d.scal[S_GTDX] = gtdx;
+    d.scal[S_FALLBACK] = fallback ? 1 : 0;
+    d.scal[S_MAXDX] = maxDx;
+  }
+  cl.sync();  // no CTA leaves while a peer may still read its shared memory
+}
+
+// Largest cluster (16, then 8, 4, 2, 1 CTAs) the device can co-schedule for
+// this kernel; 0 when none.
+int mx_cluster_size() {
+  static int cached = -1;
+  if (cached >= 0) return cached;
+  cudaFuncSetAttribute(k_mx_pcg_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+  cached = 0;
+  for (int cs = 16; cs >= 1; cs /= 2) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(cs);
+    cfg.blockDim = dim3(kClT);
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = cs;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int nc = 0;
+    if (cudaOccupancyMaxActiveClusters(&nc, k_mx_pcg_cluster, &cfg) == cudaSuccess && nc >= 1) {
+      cached = cs;
+      break;
+    }
+  }
+  cudaGetLastError();
+  return cached;
+}
+
+int mx_launch_pcg_cluster(const Dev& d, const MixBufs& mb, float* pA, float* pB, double* coef, int maxIters,
+                          double tol, int clusterSize, cudaStream_t s) {
+  ClArgs a{d, mb, pA, pB, coef, maxIters, tol};
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(clusterSize);
+  cfg.blockDim = dim3(kClT);
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = clusterSize;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return (int)cudaLaunchKernelEx(&cfg, k_mx_pcg_cluster, a);
+}
+
+}  // namespace cs

@@ -129,6 +129,92 @@ __global__ void __launch_bounds__(kSortThreads) k_radix_scatter(const Key<KW>* k
   }
 }
 
+// All passes of a stable LSD radix sort in ONE thread block (1024 threads), for
+// sorts small enough that launch latency dominates. Warp w owns the w-th
+// contiguous chunk; per pass: per-warp digit counts, one scan over (digit,
+// warp) in shared memory, then each warp scatters its chunk in order (32 keys
+// at a time, ranked with warp match), which keeps the sort stable.
+constexpr int kBlockSortThreads = 1024;
+constexpr int kBlockSortMax = 32768;
+
+template <int KW>
+__global__ void __launch_bounds__(kBlockSortThreads) k_block_radix(Key<KW>* k0, uint32_t* p0, Key<KW>* k1,
+                                                                   uint32_t* p1, int n, int passes) {
+  __shared__ uint32_t cnt[kBlockSortThreads / 32][256];
+  __shared__ uint32_t tot[256];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  constexpr int kWarps = kBlockSortThreads / 32;
+  const int chunk = ((n + kWarps - 1) / kWarps + 31) & ~31;
+  const int lo = min(n, warp * chunk), hi = min(n, lo + chunk);
+  const uint32_t lt = (1u << lane) - 1u;
+  for (int pass = 0; pass < passes; pass++) {
+    const Key<KW>* ki = (pass & 1) ? k1 : k0;
+    const uint32_t* pi = (pass & 1) ? p1 : p0;
+    Key<KW>* ko = (pass & 1) ? k0 : k1;
+    uint32_t* po = (pass & 1) ? p0 : p1;
+    for (int w = 0; w < kWarps; w++)
+      if (threadIdx.x < 256) cnt[w][threadIdx.x] = 0;
+    __syncthreads();
+    for (int base = lo; base < hi; base += 32) {
+      const int i = base + lane;
+      const int dg = i < hi ? (int)digit_of(ki[i], pass) : -1;
+      const uint32_t peers = __match_any_sync(0xffffffffu, dg);
+      if (dg >= 0 && (peers & lt) == 0) cnt[warp][dg] += __popc(peers);
+      __syncwarp();
+    }
+    __syncthreads();
+    // exclusive offsets: digit-major, warp-minor
+    if (threadIdx.x < 256) {
+      uint32_t run = 0;
+      for (int w = 0; w < kWarps; w++) {
+        const uint32_t c = cnt[w][threadIdx.x];
+        cnt[w][threadIdx.x] = run;
+        run += c;
+      }
+      tot[threadIdx.x] = run;
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+      // scan of the 256 digit totals: 8 per lane, then across lanes
+      uint32_t v[8], sum = 0;
+      for (int q = 0; q < 8; q++) { v[q] = tot[threadIdx.x * 8 + q]; sum += v[q]; }
+      uint32_t incl = sum;
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+      }
+      uint32_t run = incl - sum;
+      for (int q = 0; q < 8; q++) { tot[threadIdx.x * 8 + q] = run; run += v[q]; }
+    }
+    __syncthreads();
+    if (threadIdx.x < 256)
+      for (int w = 0; w < kWarps; w++) cnt[w][threadIdx.x] += tot[threadIdx.x];
+    __syncthreads();
+    for (int base = lo; base < hi; base += 32) {
+      const int i = base + lane;
+      const bool valid = i < hi;
+      Key<KW> k;
+      uint32_t pl = 0;
+      int dg = -1;
+      if (valid) {
+        k = ki[i];
+        pl = pi[i];
+        dg = (int)digit_of(k, pass);
+      }
+      const uint32_t peers = __match_any_sync(0xffffffffu, dg);
+      if (valid) {
+        const uint32_t off = cnt[warp][dg] + __popc(peers & lt);
+        ko[off] = k;
+        po[off] = pl;
+      }
+      __syncwarp();
+      if (valid && (peers & lt) == 0) cnt[warp][dg] += __popc(peers);
+      __syncwarp();
+    }
+    __syncthreads();
+  }
+}
+
 // Sorts n records by key over the low `bits` bits of the key (counted from the
 // least significant end). Ping-pongs between (k0,p0) and (k1,p1); returns true
 // when the result ended in (k1,p1). hist must hold 256 * ceil(n / 2048) + 1 u32.
@@ -138,6 +224,11 @@ bool radix_sort(Key<KW>* k0, uint32_t* p0, Key<KW>* k1, uint32_t* p1, int n, int
   if (n <= 1) return false;
   const int ntiles = (n + kSortTile - 1) / kSortTile;
   const int passes = (bits + 7) / 8;
+  if (n <= kBlockSortMax) {
+    k_block_radix<KW><<<1, kBlockSortThreads, 0, s>>>(k0, p0, k1, p1, n, passes);
+    if (launches) *launches += 1;
+    return (passes & 1) != 0;
+  }
   bool flip = false;
   for (int pass = 0; pass < passes; pass++) {
     const Key<KW>* ki = flip ? k1 : k0;

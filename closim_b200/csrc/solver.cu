@@ -141,6 +141,8 @@ void* cs_stream(cs_solver* h) { return h ? (void*)h->s.stream : nullptr; }
 int cs_profile(cs_solver* h, int enable) {
   return guarded(h, [&] {
     h->s.prof = enable != 0;
+    h->s.profPhases = enable == 2;
+    for (double& v : h->s.phaseMs) v = 0;
     h->s.profMs = h->s.profLaunches = h->s.profBytes = h->s.profIters = 0;
     h->s.profPending = false;
   });
@@ -153,6 +155,58 @@ int cs_profile_read(cs_solver* h, double* out) {
     out[2] = h->s.profBytes;
     out[3] = h->s.profIters;
     out[4] = h->s.profLaunches > 0 ? h->s.profMs / h->s.profLaunches : 0.0;
+  });
+}
+
+int cs_forward(cs_solver* h, double dt, int32_t steps, int32_t checkpoint_every) {
+  return guarded(h, [&] { h->s.forward(dt, steps, checkpoint_every); });
+}
+
+int cs_backward(cs_solver* h, const double* dL_dxN, double* dL_dtheta, double* dL_dv0) {
+  return guarded(h, [&] {
+    if (!dL_dxN) throw std::invalid_argument("null dL/dx_N");
+    h->s.backward(dL_dxN, dL_dtheta, dL_dv0, h->s.adjMaxIters, h->s.adjTol);
+  });
+}
+
+int cs_set_adjoint_options(cs_solver* h, int32_t max_iters, double tol) {
+  return guarded(h, [&] {
+    if (max_iters <= 0 || !(tol > 0)) throw std::invalid_argument("bad adjoint options");
+    h->s.adjMaxIters = max_iters;
+    h->s.adjTol = tol;
+  });
+}
+
+int cs_set_newton_mode(cs_solver* h, int32_t mode, double tol) {
+  return guarded(h, [&] {
+    if ((mode != 0 && mode != 1) || !(tol > 0)) throw std::invalid_argument("bad Newton mode");
+    h->s.newtonMode = mode;
+    h->s.newtonTol = tol;
+  });
+}
+
+int cs_adjoint_stats(cs_solver* h, double* out4) {
+  return guarded(h, [&] {
+    if (!out4) throw std::invalid_argument("null output");
+    out4[0] = (double)h->s.adjStats.pcgIters;
+    out4[1] = h->s.adjStats.solves;
+    out4[2] = h->s.adjStats.recomputedSteps;
+    out4[3] = h->s.adjStats.maxRelResidual;
+  });
+}
+
+int cs_solver_info(cs_solver* h, int32_t* out, int32_t n) {
+  return guarded(h, [&] {
+    if (!out || n <= 0) throw std::invalid_argument("null output");
+    const int32_t v[4] = {h->s.mxCluster, h->s.mxBlocks, h->s.pcgBlocks, h->s.mesh.D};
+    for (int i = 0; i < n; i++) out[i] = i < 4 ? v[i] : 0;
+  });
+}
+
+int cs_profile_phases(cs_solver* h, double* out, int32_t n) {
+  return guarded(h, [&] {
+    if (!out || n <= 0) throw std::invalid_argument("null output");
+    for (int i = 0; i < n; i++) out[i] = i < cs::PH_N ? h->s.phaseMs[i] : 0.0;
   });
 }
 

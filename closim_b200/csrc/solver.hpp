@@ -4,7 +4,9 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <stdexcept>
@@ -12,6 +14,7 @@
 #include <vector>
 
 #include "../../include/closim_cuda.h"
+#include "adjoint.cuh"
 #include "contact_host.hpp"
 #include "mixed.cuh"
 #include "plain.cuh"
@@ -58,6 +61,16 @@ struct NonFinite : std::runtime_error {
   NonFinite() : std::runtime_error("non-finite gradient — blow up; reduce dt/stiffness") {}
 };
 
+// Phases of a step for the wall-time breakdown (cs_profile mode 2).
+struct AdjStats {
+  long pcgIters = 0;
+  int solves = 0, recomputedSteps = 0;
+  double maxRelResidual = 0;
+};
+
+enum Phase { PH_OTHER = 0, PH_BROADPHASE, PH_ACTIVE_SET, PH_GRADIENT, PH_PRECOND, PH_PCG, PH_TRIAL, PH_ENERGY,
+             PH_COMMIT, PH_N };
+
 class Solver {
  public:
   int precision = CS_PRECISION_FP64;
@@ -89,15 +102,33 @@ class Solver {
   double* hscal = nullptr;  // pinned host mirror of scal
   int pcgBlocks = 1;
   // mixed-precision path
-  DBuf<float> fr, fz, fp, fAp, fx, felem, ftris, fh9, fLinv;
+  DBuf<float> fr, fz, fp, fAp, fx, felem, ftris, fh9, fLinv, fp2;
   MixBufs mb{};
   int mxBlocks = 1;
+  int mxCluster = 0;  // CTAs of the one-cluster PCG (0: grid-wide cooperative PCG)
   Dev d{};
   // profiling of the linear-solve kernel
   bool prof = false;
   cudaEvent_t pev0 = nullptr, pev1 = nullptr;
   double profMs = 0, profLaunches = 0, profBytes = 0, profIters = 0;
   bool profPending = false;
+  // Wall time per phase of the step (cs_profile mode 2): the stream is
+  // synchronized at every phase boundary, so each phase is charged its host
+  // launch overhead plus its device time. Diagnostic only (slows the step).
+  bool profPhases = false;
+  int curPhase = PH_OTHER;
+  double phaseMs[PH_N] = {};
+  std::chrono::steady_clock::time_point phaseT0{};
+  int phase(int p) {
+    const int prev = curPhase;
+    if (!profPhases) { curPhase = p; return prev; }
+    CK(cudaStreamSynchronize(stream));
+    const auto now = std::chrono::steady_clock::now();
+    phaseMs[curPhase] += std::chrono::duration<double, std::milli>(now - phaseT0).count();
+    phaseT0 = now;
+    curPhase = p;
+    return prev;
+  }
 
   // Algorithmic bytes of one k_pcg launch that ran `iters` iterations: per
   // iteration the FD HVP reads x, p (2 x 24 B per vertex), Dm^-1, area and 3
@@ -251,6 +282,13 @@ class Solver {
       mb.r = fr.p; mb.z = fz.p; mb.p = fp.p; mb.Ap = fAp.p; mb.x = fx.p;
       mb.elem = felem.p; mb.tris = ftris.p; mb.h9 = fh9.p; mb.Linv = fLinv.p;
       mxBlocks = mx_pcg_grid_blocks(d);
+      // Sheets up to 20k vertices solve inside one thread-block cluster
+      // (on-GPC barriers); larger ones use the grid-wide kernel.
+      // CLOSIM_MX_PCG=grid|cluster overrides the choice.
+      const char* env = std::getenv("CLOSIM_MX_PCG");
+      const bool wantCluster = env ? std::string(env) == "cluster" : mesh.n <= 20000;
+      mxCluster = wantCluster && mesh.maxDomain <= 8 ? mx_cluster_size() : 0;
+      if (mxCluster > 0) fp2.alloc(n3);
     }
     upload_pins();
     contact.reset();
@@ -295,6 +333,7 @@ class Solver {
     d.precond = opts.precond == CS_PRECOND_SCHWARZ ? 1 : 0;
     d.hasContact = contact ? 1 : 0;
     int64_t& lc = launch_counter();
+    if (profPhases) { CK(cudaStreamSynchronize(stream)); phaseT0 = std::chrono::steady_clock::now(); curPhase = PH_OTHER; }
     launch_predict(d, stream);
     lc += 1 + (d.npins > 0);
     if (contact) contact->begin_step_and_bisect(*this);
@@ -311,7 +350,9 @@ class Solver {
     bool converged = false;
     for (int ni = 0; ni < opts.newton_iters; ni++) {
       used = ni + 1;
+      phase(PH_ACTIVE_SET);
       if (contact) contact->gradient_terms(*this);  // active set, barrier+friction grad, diag estimate
+      phase(PH_GRADIENT);
       if (mixed()) {
         launch_grad_terms(d, stream);
         lc += 2 + (d.kb > 0 && d.hg > 0);
@@ -325,10 +366,27 @@ class Solver {
       maxStrain = hscal[S_MAXSTRAIN];
       if (!std::isfinite(gradNorm)) throw NonFinite();
       if (gradNorm < opts.grad_tol) { converged = true; break; }
-      if (mixed()) mx_prepare(d, mb, d.precond == 1, stream, &lc);
-      else if (d.precond == 1) { launch_schwarz_factor(d, stream); lc += 1; }
+      phase(PH_PRECOND);
+      if (newtonMode == 1) {
+        if (d.precond == 1) { launch_schwarz_factor(d, stream); lc += 1; }
+      } else if (mixed()) {
+        mx_prepare(d, mb, d.precond == 1, stream, &lc);
+      } else if (d.precond == 1) {
+        launch_schwarz_factor(d, stream);
+        lc += 1;
+      }
+      phase(PH_PCG);
       if (prof) CK(cudaEventRecord(pev0, stream));
-      if (mixed()) CK((cudaError_t)mx_launch_pcg(d, mb, opts.pcg_max_iters, 1e-3, mxBlocks, stream));
+      if (newtonMode == 1) {
+        ensure_adj_buffers();
+        AdjArgs a{d, adjRhs.p, d.dx, adjR.p, adjZ.p, adjP.p, adjAp.p, adjTri.p, adjHin.p, d.kb, 1,
+                  opts.pcg_max_iters, newtonTol, adjOut.p};
+        CK((cudaError_t)newton_exact_solve(a, adj_grid_blocks(d), stream));
+        lc += 3;
+      } else if (mixed() && mxCluster > 0)
+        CK((cudaError_t)mx_launch_pcg_cluster(d, mb, fp.p, fp2.p, d.hasContact ? d.c.dd : nullptr,
+                                              opts.pcg_max_iters, 1e-3, mxCluster, stream));
+      else if (mixed()) CK((cudaError_t)mx_launch_pcg(d, mb, opts.pcg_max_iters, 1e-3, mxBlocks, stream));
       else CK((cudaError_t)launch_pcg(d, opts.pcg_max_iters, 1e-3, pcgBlocks, stream));
       if (prof) { CK(cudaEventRecord(pev1, stream)); profPending = true; }
       lc += 1;
@@ -338,6 +396,7 @@ class Solver {
       double gtdx = 0;
       for (int li = 0; li < opts.ls_iters; li++) {
         trials++;
+        phase(PH_TRIAL);
         launch_trial(d, alpha, stream);
         lc += 1 + (d.npins > 0);
         if (contact && !contact->check_trial(*this, d.xt)) {
@@ -345,6 +404,7 @@ class Solver {
           alpha *= 0.5;
           continue;
         }
+        phase(PH_ENERGY);
         if (contact) contact->merit_energy(*this, d.xt);
         energy_of(d.xt);
         read_scalars();
@@ -364,6 +424,7 @@ class Solver {
           std::swap(d.x, d.xt);
           energy = eNew;
           accepted = true;
+          phase(PH_COMMIT);
           if (contact) contact->commit(*this, d.x);
           break;
         }
@@ -378,6 +439,7 @@ class Solver {
       if (!accepted) break;
       if (alpha < 1e-6) break;
     }
+    phase(PH_OTHER);
     const double damp = 1 - std::min(std::max(mat.damping, 0.0), 0.1);
     launch_velocity(d, damp, stream);
     lc += 1;
@@ -401,6 +463,7 @@ class Solver {
     stats.newton_iters_used = used;
     stats.armijo_trials = trials;
     if (contact) contact->fill_stats(*this, stats);
+    phase(PH_OTHER);
     haveStats = true;
   }
 
@@ -415,6 +478,133 @@ class Solver {
     launch_counter() += 4;
     CK(cudaMemcpyAsync(out, vAp.p, b, cudaMemcpyDeviceToHost, stream));
     CK(cudaStreamSynchronize(stream));
+  }
+
+  // ---- differentiable rollout (no reference counterpart) -------------------------
+  // forward(): `steps` steps of size h from the current state with the pins
+  // fixed, keeping (x, v) at every K-th step start; backward(): the reverse
+  // sweep through the implicit-function theorem, recomputing each K-step
+  // segment from its checkpoint (one extra forward pass in total).
+  struct Rollout {
+    int steps = 0, K = 0;
+    double h = 0;
+    DBuf<double> ckX, ckV;   // checkpoints, 3n each
+    DBuf<double> seg;        // the K states of the segment being reversed
+    DBuf<double> xN, vN;     // state after the rollout
+    bool valid = false;
+  } ro;
+  DBuf<double> adjRhs, adjMu, adjR, adjZ, adjP, adjAp, adjTri, adjHin, adjTerms, adjLamX, adjLamV, adjAcc, adjOut;
+  AdjStats adjStats{};
+  int adjMaxIters = 2000;
+  double adjTol = 1e-10;
+  // Newton linear solve: 0 = the reference's (FD membrane HVP, PCG to 1e-3);
+  // 1 = full FP64 Hessian (membrane with clamped compression, bending, frozen
+  // contact) solved to newtonTol, for rollouts that must converge tightly.
+  int newtonMode = 0;
+  double newtonTol = 1e-8;
+
+  void ensure_adj_buffers() {
+    const size_t n3 = 3 * (size_t)mesh.n;
+    const int stride = mesh.m + mesh.hg;
+    for (DBuf<double>* b : {&adjRhs, &adjMu, &adjR, &adjZ, &adjP, &adjAp, &adjLamX, &adjLamV})
+      if (b->n < n3) b->alloc(n3);
+    if (adjTri.n < 9 * (size_t)std::max(mesh.m, 1)) adjTri.alloc(9 * (size_t)std::max(mesh.m, 1));
+    if (adjHin.n < 12 * (size_t)std::max(mesh.hg, 1)) adjHin.alloc(12 * (size_t)std::max(mesh.hg, 1));
+    if (adjTerms.n < 4 * (size_t)std::max(stride, 1)) adjTerms.alloc(4 * (size_t)std::max(stride, 1));
+    if (adjAcc.n < 4) adjAcc.alloc(4);
+    if (adjOut.n < 3) adjOut.alloc(3);
+  }
+
+  void forward(double h, int steps, int K) {
+    if (!ready) throw std::logic_error("CpuSolver not initialized");
+    if (steps <= 0 || K <= 0) throw std::invalid_argument("steps and checkpoint interval must be positive");
+    const size_t n3 = 3 * (size_t)mesh.n;
+    const int nck = (steps + K - 1) / K;
+    ro.valid = false;
+    ro.steps = steps; ro.K = K; ro.h = h;
+    ro.ckX.alloc(nck * n3);
+    ro.ckV.alloc(nck * n3);
+    ro.seg.alloc((size_t)K * n3);
+    ro.xN.alloc(n3);
+    ro.vN.alloc(n3);
+    for (int st = 0; st < steps; st++) {
+      if (st % K == 0) {
+        const size_t c = st / K;
+        CK(cudaMemcpyAsync(ro.ckX.p + c * n3, d.x, n3 * 8, cudaMemcpyDeviceToDevice, stream));
+        CK(cudaMemcpyAsync(ro.ckV.p + c * n3, d.v, n3 * 8, cudaMemcpyDeviceToDevice, stream));
+      }
+      step(h);
+    }
+    CK(cudaMemcpyAsync(ro.xN.p, d.x, n3 * 8, cudaMemcpyDeviceToDevice, stream));
+    CK(cudaMemcpyAsync(ro.vN.p, d.v, n3 * 8, cudaMemcpyDeviceToDevice, stream));
+    CK(cudaStreamSynchronize(stream));
+    ro.valid = true;
+  }
+
+  // dLdxN: host 3n; dtheta: host 4 (C00, C11, G, k_bend); dv0: host 3n (may be null).
+  void backward(const double* dLdxN, double* dtheta, double* dv0, int maxIters, double tol) {
+    if (!ro.valid) throw std::logic_error("backward needs a forward rollout");
+    const size_t n3 = 3 * (size_t)mesh.n;
+    ensure_adj_buffers();
+    CK(cudaMemcpyAsync(adjLamX.p, dLdxN, n3 * 8, cudaMemcpyHostToDevice, stream));
+    CK(cudaMemsetAsync(adjLamV.p, 0, n3 * 8, stream));
+    CK(cudaMemsetAsync(adjAcc.p, 0, 4 * 8, stream));
+    const double damp = 1 - std::min(std::max(mat.damping, 0.0), 0.1);
+    const double beta = std::max(std::max(mat.stretch_warp, mat.stretch_weft), mat.shear) * mat.thickness * 0.1 + 1e-6;
+    const int blocks = adj_grid_blocks(d);
+    double* const xPrimary = d.x;
+    double* const x0Primary = d.x0;
+    adjStats = AdjStats{};
+    const int nck = (ro.steps + ro.K - 1) / ro.K;
+    std::vector<double> hout(3);
+    for (int c = nck - 1; c >= 0; c--) {
+      const int s0 = c * ro.K, s1 = std::min(ro.steps, s0 + ro.K);
+      // recompute the segment from its checkpoint
+      CK(cudaMemcpyAsync(d.x, ro.ckX.p + (size_t)c * n3, n3 * 8, cudaMemcpyDeviceToDevice, stream));
+      CK(cudaMemcpyAsync(d.v, ro.ckV.p + (size_t)c * n3, n3 * 8, cudaMemcpyDeviceToDevice, stream));
+      for (int st = s0; st < s1; st++) {
+        step(ro.h);
+        CK(cudaMemcpyAsync(ro.seg.p + (size_t)(st - s0) * n3, d.x, n3 * 8, cudaMemcpyDeviceToDevice, stream));
+        adjStats.recomputedSteps++;
+      }
+      for (int st = s1 - 1; st >= s0; st--) {
+        double* x1 = ro.seg.p + (size_t)(st - s0) * n3;
+        double* x0 = st == s0 ? ro.ckX.p + (size_t)c * n3 : ro.seg.p + (size_t)(st - s0 - 1) * n3;
+        d.x = x1;
+        d.x0 = x0;
+        d.h = ro.h;
+        d.invH2 = 1 / (ro.h * ro.h);
+        if (contact) {
+          contact->begin_segment(*this);
+          contact->update_active_set(*this, x1);
+        }
+        launch_diag_init(d, beta, stream);
+        if (d.precond == 1) launch_schwarz_factor(d, stream);
+        adj_rhs(d, adjLamX.p, adjLamV.p, damp, adjRhs.p, stream);
+        AdjArgs a{d, adjRhs.p, adjMu.p, adjR.p, adjZ.p, adjP.p, adjAp.p, adjTri.p, adjHin.p, d.kb, 0, maxIters, tol,
+                  adjOut.p};
+        CK((cudaError_t)adj_launch_pcg(a, blocks, stream));
+        adj_theta(d, adjMu.p, adjTerms.p, adjAcc.p, stream);
+        adj_propagate(d, adjMu.p, adjLamX.p, adjLamV.p, damp, stream);
+        CK(cudaMemcpyAsync(hout.data(), adjOut.p, 3 * 8, cudaMemcpyDeviceToHost, stream));
+        CK(cudaStreamSynchronize(stream));
+        adjStats.pcgIters += (long)hout[0];
+        adjStats.maxRelResidual = std::max(adjStats.maxRelResidual, hout[2] > 0 ? hout[1] / hout[2] : 0.0);
+        adjStats.solves++;
+        d.x = xPrimary;
+        d.x0 = x0Primary;
+      }
+    }
+    // dL/dv0 is the velocity adjoint after the first step's propagation
+    std::vector<double> acc(4);
+    CK(cudaMemcpyAsync(acc.data(), adjAcc.p, 4 * 8, cudaMemcpyDeviceToHost, stream));
+    if (dv0) CK(cudaMemcpyAsync(dv0, adjLamV.p, n3 * 8, cudaMemcpyDeviceToHost, stream));
+    // restore the state after the rollout
+    CK(cudaMemcpyAsync(d.x, ro.xN.p, n3 * 8, cudaMemcpyDeviceToDevice, stream));
+    CK(cudaMemcpyAsync(d.v, ro.vN.p, n3 * 8, cudaMemcpyDeviceToDevice, stream));
+    CK(cudaStreamSynchronize(stream));
+    if (dtheta) for (int j = 0; j < 4; j++) dtheta[j] = acc[j];
+    if (contact) contact->bind(*this);
   }
 
   void get(double* out, bool vel) {

@@ -358,8 +358,60 @@ class CudaSolver:
         """The solver's cudaStream_t (for events recorded around calls)."""
         return int(self._lib.cs_stream(self._h) or 0)
 
-    def profile(self, enable: bool) -> None:
-        self._check(self._lib.cs_profile(self._h, 1 if enable else 0))
+    PHASES = ["other", "broadphase", "active_set", "gradient", "precond", "pcg", "trial", "energy", "commit"]
+
+    def profile(self, enable, phases: bool = False) -> None:
+        """Per-launch timing of the PCG kernel; phases=True also charges wall
+        time to the step's phases (synchronizing at each boundary)."""
+        self._check(self._lib.cs_profile(self._h, (2 if phases else 1) if enable else 0))
+
+    # ---- differentiable rollout (no reference counterpart) -------------------------
+    def forward(self, dt: float, steps: int, checkpointEvery: int = 20) -> np.ndarray:
+        """`steps` steps from the current state with the pins held fixed, keeping
+        checkpoints every `checkpointEvery` steps; returns the final positions
+        (also written into the scene)."""
+        self._need()
+        self._send_pins()
+        self._check(self._lib.cs_forward(self._h, float(dt), int(steps), int(checkpointEvery)))
+        self._pull()
+        self.lastStats = self._stats()
+        return self.scene.positions
+
+    def backward(self, dLdxN) -> tuple:
+        """Gradient of a loss on the final positions: returns
+        ({C00, C11, G, kBend}: dL/dtheta, dL/dv0 [3n])."""
+        self._need()
+        g = np.ascontiguousarray(dLdxN, np.float64)
+        if g.size != 3 * self.scene.mesh.count:
+            raise ValueError("dL/dx_N must hold 3n values")
+        th = np.zeros(4)
+        dv = np.zeros(g.size)
+        self._check(self._lib.cs_backward(self._h, L.ptr(g), L.ptr(th), L.ptr(dv)))
+        return dict(C00=th[0], C11=th[1], G=th[2], kBend=th[3]), dv
+
+    def setNewtonMode(self, mode: str = "reference", tol: float = 1e-8) -> None:
+        """'reference': the reference's inexact Newton; 'exact': full FP64
+        Hessian solved to `tol` (converges tightly; for differentiable rollouts)."""
+        self._check(self._lib.cs_set_newton_mode(self._h, {"reference": 0, "exact": 1}[mode], tol))
+
+    def setAdjointOptions(self, maxIters: int = 2000, tol: float = 1e-10) -> None:
+        self._check(self._lib.cs_set_adjoint_options(self._h, maxIters, tol))
+
+    def adjointStats(self) -> dict:
+        out = np.zeros(4)
+        self._check(self._lib.cs_adjoint_stats(self._h, L.ptr(out)))
+        return dict(pcgIters=int(out[0]), solves=int(out[1]), recomputedSteps=int(out[2]), maxRelResidual=out[3])
+
+    def launchInfo(self) -> dict:
+        out = np.zeros(4, np.int32)
+        self._check(self._lib.cs_solver_info(self._h, L.ptr(out), len(out)))
+        return dict(pcgClusterCtas=int(out[0]), pcgGridCtas=int(out[1]), fp64PcgCtas=int(out[2]),
+                    schwarzDomains=int(out[3]))
+
+    def profilePhases(self) -> dict:
+        out = np.zeros(len(self.PHASES))
+        self._check(self._lib.cs_profile_phases(self._h, L.ptr(out), len(out)))
+        return dict(zip(self.PHASES, out.tolist()))
 
     def profileRead(self) -> dict:
         out = np.zeros(5)

@@ -142,6 +142,46 @@ void* cs_stream(cs_solver* s);
  * iterations, and the flush-free mean ms per launch. */
 int cs_profile(cs_solver* s, int enable);
 int cs_profile_read(cs_solver* s, double* out5);
+/* Wall-time breakdown of the step (diagnostic, no counterpart in the
+ * reference): after cs_profile(s, 2) the stream is synchronized at every
+ * phase boundary, which slows the step. Fills out[0..n) with milliseconds
+ * accumulated per phase since cs_profile: other, broadphase, active set,
+ * gradient, preconditioner, PCG, trial check, trial energy, commit. */
+int cs_profile_phases(cs_solver* s, double* out, int32_t n);
+/* Launch shapes chosen at cs_initialize (diagnostic): out[0] CTAs of the
+ * one-cluster mixed PCG (0 = the grid-wide kernel is used), out[1] CTAs of the
+ * grid-wide mixed PCG, out[2] CTAs of the FP64 PCG, out[3] Schwarz domains. */
+int cs_solver_info(cs_solver* s, int32_t* out, int32_t n);
+
+/* ---- differentiable rollout (no counterpart in the reference) ----
+ * cs_forward runs `steps` implicit steps of size dt from the current state
+ * (pins held fixed) and keeps (x, v) at every checkpoint_every-th step start.
+ * cs_backward takes dL/dx_N (host, 3n doubles) for a loss on the final
+ * positions and returns dL/d(C00, C11, G, k_bend) in dL_dtheta[4] (k_bend sets
+ * bendWarp = bendWeft) and dL/dv_0 in dL_dv0 (3n, may be NULL), through the
+ * implicit-function theorem on every step (one FP64 solve of H mu = lambda per
+ * step, H the Newton Hessian at the step's end state with membrane, bending
+ * and frozen barrier terms; friction and the restitution filter are held
+ * constant). Each checkpoint segment is recomputed from its checkpoint; the
+ * state after cs_forward is restored on return. The gradient is that of the
+ * converged step map: give cs_set_stepper_options a budget under which every
+ * step converges. */
+int cs_forward(cs_solver* s, double dt, int32_t steps, int32_t checkpoint_every);
+int cs_backward(cs_solver* s, const double* dL_dxN, double* dL_dtheta, double* dL_dv0);
+/* Newton linear solve (no counterpart in the reference). mode 0 (default) is
+ * the reference's: matrix-free FD membrane HVP, PCG to relative 1e-3. mode 1
+ * solves with the full FP64 Hessian (analytic membrane HVP with compressed
+ * principal stresses clamped to zero, exact bending HVP, frozen contact) to the
+ * relative tolerance tol, keeping the reference's descent safeguard, trust
+ * region and Armijo search: the converged step is the same, reached in far
+ * fewer iterations, as the adjoint's implicit-function theorem needs.
+ * cs_set_stepper_options' PCG budget applies to both. */
+int cs_set_newton_mode(cs_solver* s, int32_t mode, double tol);
+/* Adjoint PCG budget (default 2000 iterations, relative residual 1e-10). */
+int cs_set_adjoint_options(cs_solver* s, int32_t max_iters, double tol);
+/* out[4]: adjoint PCG iterations, solves, recomputed steps, largest final
+ * relative residual, for the last cs_backward. */
+int cs_adjoint_stats(cs_solver* s, double* out4);
 
 /* ---- allocation-free membrane HVP (no counterpart in the reference) ----
  * For callers that may not call cudaMalloc while stepping: a frame recorded into

@@ -42,6 +42,7 @@ def lib():
         "orc_mesh_destroy": (None, [VP]),
         "orc_mesh_counts": (None, [VP, I32P]),
         "orc_mesh_arrays": (None, [VP, F32P, F32P, F32P, I32P, F64P]),
+        "orc_hinge_energy": (C.c_double, [F64P, I32P, F64P, C.c_double]),
         "orc_incidence": (None, [VP, C.c_int, U32P, U32P, U32P, C.POINTER(C.c_int)]),
         "orc_js_hypot3": (C.c_double, [C.c_double, C.c_double, C.c_double]),
         "orc_tri_energy_grad": (None, [F64P, F64P, C.c_double, F64P, F64P]),
@@ -182,6 +183,12 @@ class Mesh:
 
 
 # ---- element functions ---------------------------------------------------------
+
+def hinge_energy(q12, meta3, k):
+    """hingeEnergy (src/physics/bending.ts:7-16) of the 4 vertices in q12."""
+    return lib().orc_hinge_energy(np.ascontiguousarray(q12, np.float64), np.arange(4, dtype=np.int32),
+                                  np.ascontiguousarray(meta3, np.float64), k)
+
 
 def tri_energy_grad(x0, x1, x2, inv, area, mat):
     out = np.zeros(13)

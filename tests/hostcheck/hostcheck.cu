@@ -2,6 +2,7 @@
 // (closim_b200/csrc/contact_math.cuh, jsmath.cuh), exported for CPU checks
 // against the oracle. Built with -fmad=false like the FP64 device path.
 #include "../../closim_b200/csrc/contact_math.cuh"
+#include "../../closim_b200/csrc/adjoint_math.cuh"
 
 extern "C" {
 double hc_js_acos(double x) { return cs::js_acos(x); }
@@ -22,4 +23,10 @@ int hc_solve_cubic01(double a3, double a2, double a1, double a0, double* o) { re
 double hc_barrier_value(double d, double dh) { return cs::barrier_value(d, dh); }
 double hc_barrier_grad(double d, double dh, double k) { return cs::barrier_grad_scalar(d, dh, k, 1); }
 double hc_barrier_curv(double d, double dh, double k) { return cs::barrier_curvature(d, dh, k); }
+double hc_bend_grad(const double* q, const double* meta, double k, double* g) {
+  return cs::bend_grad<double>(q, meta[0], meta[1], meta[2], k, g);
+}
+void hc_bend_hvp(const double* q, const double* v, const double* meta, double k, double* o) {
+  cs::bend_hvp(q, v, meta[0], meta[1], meta[2], k, o);
+}
 }

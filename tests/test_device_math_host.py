@@ -97,3 +97,43 @@ def test_cubic_and_barrier_match_oracle(hc):
     for d in np.concatenate([rng.uniform(0, 2e-3, 2000), [1e-12, 1e-13, 2e-3, 5e-3, 0.0]]):
         assert same(hc.hc_barrier_value(d, 2e-3), O.barrier_value(d, 2e-3))
         assert same(hc.hc_barrier_grad(d, 2e-3, 50.0), O.lib().orc_barrier_grad_scalar(d, 2e-3, 50.0, 1.0))
+
+
+def test_bending_gradient_and_hvp(hc):
+    """The adjoint's analytic hinge gradient against central differences of the
+    reference's hinge energy (acos form, bending.ts:7-16), and its dual-number
+    HVP against central differences of that gradient. Near-flat hinges with
+    flat (pi) and curved (2.5 rad) rest angles."""
+    p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+    hc.hc_bend_grad.restype = C.c_double
+    hc.hc_bend_grad.argtypes = [p, p, C.c_double, p]
+    hc.hc_bend_hvp.restype = None
+    hc.hc_bend_hvp.argtypes = [p, p, p, C.c_double, p]
+    rng = np.random.default_rng(11)
+    base = np.array([0, 0, 0, 1, 0, 0, 0.4, 0, 1, 0.6, 0, -1], np.float64)
+    worst_e = worst_g = worst_h = 0.0
+    for trial in range(60):
+        q = base + rng.uniform(-1, 1, 12) * (0.01 if trial < 30 else 0.1)
+        meta = np.array([np.pi if trial % 2 else 2.5, 0.7, 0.9])
+        k = 2e-4
+        g = np.zeros(12)
+        e = hc.hc_bend_grad(q, meta, k, g)
+        e_ref = O.hinge_energy(q, meta, k)
+        worst_e = max(worst_e, abs(e - e_ref) / max(abs(e_ref), 1e-30))
+        fd = np.zeros(12)
+        for a in range(12):
+            qp, qm = q.copy(), q.copy()
+            qp[a] += 1e-6
+            qm[a] -= 1e-6
+            fd[a] = (O.hinge_energy(qp, meta, k) - O.hinge_energy(qm, meta, k)) / 2e-6
+        worst_g = max(worst_g, np.max(np.abs(fd - g)) / max(np.max(np.abs(g)), 1e-30))
+        v = rng.uniform(-1, 1, 12)
+        hv = np.zeros(12)
+        hc.hc_bend_hvp(q, v, meta, k, hv)
+        gp, gm = np.zeros(12), np.zeros(12)
+        hc.hc_bend_grad(q + 1e-6 * v, meta, k, gp)
+        hc.hc_bend_grad(q - 1e-6 * v, meta, k, gm)
+        worst_h = max(worst_h, np.max(np.abs((gp - gm) / 2e-6 - hv)) / max(np.max(np.abs(hv)), 1e-30))
+    assert worst_e < 1e-7, worst_e
+    assert worst_g < 1e-4, worst_g
+    assert worst_h < 1e-6, worst_h
