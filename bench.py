@@ -1,7 +1,8 @@
 """Benchmark of the CUDA cloth step: sim steps/s on the floor-drape workload.
 
 python bench.py --gpus N --steps K --warmup W [--impl cuda|reference]
-                [--workload floor_drape|strip_pull|sphere_drape] [--precision fp64|mixed|both]
+                [--workload floor_drape|strip_pull|sphere_drape|batch_sheets|material_fit]
+                [--precision fp64|mixed|both]
                 [--skip S]   # S extra untimed steps before timing (e.g. to reach contact)
 
 One process per GPU (torchrun for N > 1); every rank steps its own replica of
@@ -213,13 +214,119 @@ def run_precision(cfg, precision, local, args, ext_stream_cb, flush, sampler=Non
     return total, solver, sc, sc.positions.copy(), launches, ext, set_pins
 
 
+def run_batch(args, world, rank, local):
+    """512 uneven sheets stepped by the batched solver: one persistent launch
+    per step, K steps graph-replayed; value = whole-job sheet-steps/s."""
+    import torch
+    import torch.distributed as dist
+    from closim_b200 import configs
+    from closim_b200.batch import BatchSolver
+    sheets = configs.batch_sheets()
+    h = sheets[0]["h"]
+    bs = BatchSolver(sheets, device=local)
+    threads = bs.autotune(h)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{local}")
+    ext = torch.cuda.ExternalStream(bs.stream(), device=local)
+    bs.step(h, args.warmup)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    sampler = ClockSampler(local)
+    sampler.start()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    total = 0.0
+    for _ in range(args.steps):
+        with torch.cuda.stream(ext):
+            flush.fill_(1.0)
+        ev0.record(ext)
+        bs.step(h)
+        ev1.record(ext)
+        ev1.synchronize()
+        total += ev0.elapsed_time(ev1)
+    clocks = sampler.stop()
+    # graph-replayed multi-step call (the production path)
+    ev0.record(ext)
+    bs.step(h, args.steps)
+    ev1.record(ext)
+    ev1.synchronize()
+    graph_ms = ev0.elapsed_time(ev1)
+    st = bs.stats()
+    t = torch.tensor([total, graph_ms], dtype=torch.float64, device=f"cuda:{local}")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total, graph_ms = t.tolist()
+    if rank == 0:
+        S = len(sheets)
+        line = {"metric": "sim steps/s", "value": world * args.steps / (total / 1000.0), "unit": "steps/s",
+                "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": total / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+                "data": "synthetic (seeded)", "impl": "cuda",
+                "config": {"workload": "batch_sheets", "sheets": S, "n": bs.N,
+                           "m": int(sum(len(c["idx"]) // 3 for c in sheets)), "h": h,
+                           "parallelism": f"replicas x{world}", "threads_per_sheet": threads,
+                           "l2": "flushed between timed steps (256 MiB write)"},
+                "sheet_steps_per_s": world * S * args.steps / (total / 1000.0),
+                "graph_replay": {"steps": args.steps, "ms_per_step": graph_ms / args.steps},
+                "converged_sheets_last_step": int(sum(1 for x in st if x["converged"] == 1)),
+                "gpu_launches": 2 * args.steps, "clocks": clocks}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def run_material_fit(args, world, rank, local):
+    """Adjoint cost: a rollout of the material-fit sheet (96 x 96, exact-Newton
+    forward, checkpoints every 20 steps) and its backward; value = forward
+    sim steps/s, plus the backward / forward time ratio."""
+    import torch
+    import closim_b200 as cb
+    from closim_b200 import configs
+    cfg = configs.material_fit(steps=args.rollout_steps, grad_tol=1e-9)
+    sc = configs.make_scene(cfg)
+    s = cb.CudaSolver("fp64", device=local, **cfg["options"])
+    s.initialize(sc)
+    s.setNewtonMode("exact", 1e-8)
+    s.setAdjointOptions(4000, 1e-10)
+    x0 = sc.positions.copy()
+    ext = torch.cuda.ExternalStream(s.stream(), device=local)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    ev[0].record(ext)
+    xN = s.forward(cfg["h"], cfg["steps"], cfg["checkpoint_every"]).copy()
+    ev[1].record(ext)
+    fwd_conv = s.adjointStats()["forwardConverged"]
+    gx = 2 * (xN - x0) / (len(x0) // 3)
+    dth, dv0 = s.backward(gx)
+    ev[2].record(ext)
+    ev[2].synchronize()
+    f_ms = ev[0].elapsed_time(ev[1])
+    b_ms = ev[1].elapsed_time(ev[2])
+    st = s.adjointStats()
+    if rank == 0:
+        line = {"metric": "sim steps/s", "value": cfg["steps"] / (f_ms / 1000.0), "unit": "steps/s", "n_gpus": 1,
+                "steps": cfg["steps"], "warmup": 0, "ms_per_step": f_ms / cfg["steps"], "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)", "impl": "cuda",
+                "config": {"workload": "material_fit", "n": len(x0) // 3, "m": len(cfg["idx"]) // 3,
+                           "checkpoint_every": cfg["checkpoint_every"], "newton": "exact, gradTol 1e-9"},
+                "adjoint": {"backward_ms": b_ms, "forward_ms": f_ms, "backward_over_forward": b_ms / f_ms,
+                            "forward_converged_steps": fwd_conv, "adjoint_pcg_iters": st["pcgIters"],
+                            "max_rel_residual": st["maxRelResidual"],
+                            "dL_dtheta": [dth["C00"], dth["C11"], dth["G"], dth["kBend"]]}}
+        print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
-    ap.add_argument("--workload", default="floor_drape", choices=["floor_drape", "strip_pull", "sphere_drape"])
+    ap.add_argument("--workload", default="floor_drape",
+                    choices=["floor_drape", "strip_pull", "sphere_drape", "batch_sheets", "material_fit"])
+    ap.add_argument("--rollout-steps", type=int, default=40, help="material_fit: steps of the timed rollout")
     ap.add_argument("--skip", type=int, default=0, help="extra untimed steps before the timed region")
     ap.add_argument("--phase-steps", type=int, default=3, help="extra steps for the per-phase wall-time breakdown")
     ap.add_argument("--small", action="store_true", help="32x32 floor drape (for profiler captures)")
@@ -242,6 +349,10 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
     from closim_b200 import configs
+    if args.workload == "batch_sheets":
+        return run_batch(args, world, rank, local)
+    if args.workload == "material_fit":
+        return run_material_fit(args, world, rank, local)
     if args.small:
         cfg = configs.floor_drape(nx=31, ny=31, w=0.4, hgt=0.4)
     else:

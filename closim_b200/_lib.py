@@ -55,7 +55,10 @@ EXPORTS = ["cs_create", "cs_destroy", "cs_last_error", "cs_initialize", "cs_set_
            "cs_set_stepper_options", "cs_set_material", "cs_set_pins", "cs_step", "cs_get_positions",
            "cs_get_velocities", "cs_set_state", "cs_last_stats", "cs_membrane_hvp", "cs_step_n", "cs_sync",
            "cs_kernel_launches", "cs_stream", "cs_profile", "cs_profile_read", "cs_profile_phases", "cs_solver_info", "cs_forward", "cs_backward",
-           "cs_set_adjoint_options", "cs_adjoint_stats", "cs_set_newton_mode", "cs_build_grid",
+           "cs_set_adjoint_options", "cs_adjoint_stats", "cs_set_newton_mode", "cs_batch_create", "cs_batch_destroy",
+           "cs_batch_last_error", "cs_batch_initialize", "cs_batch_set_contact", "cs_batch_set_stepper_options",
+           "cs_batch_step", "cs_batch_get_positions", "cs_batch_get_velocities", "cs_batch_stats",
+           "cs_batch_autotune", "cs_batch_set_threads", "cs_batch_stream", "cs_build_grid",
            "cs_preprocess", "cs_broadphase_create", "cs_broadphase_destroy", "cs_broadphase_last_error",
            "cs_broadphase_build", "cs_broadphase_diagnostics", "cs_broadphase_pairs", "cs_broadphase_state"]
 
@@ -101,6 +104,19 @@ def load():
         "cs_set_adjoint_options": (C.c_int, [vp, C.c_int32, C.c_double]),
         "cs_adjoint_stats": (C.c_int, [vp, vp]),
         "cs_set_newton_mode": (C.c_int, [vp, C.c_int32, C.c_double]),
+        "cs_batch_create": (vp, [C.c_int32]),
+        "cs_batch_destroy": (None, [vp]),
+        "cs_batch_last_error": (C.c_char_p, [vp]),
+        "cs_batch_initialize": (C.c_int, [vp, C.c_int32, vp, vp, vp, vp, vp, vp, vp, vp]),
+        "cs_batch_set_contact": (C.c_int, [vp, C.POINTER(cs_contact_params), C.c_int32, C.c_double]),
+        "cs_batch_set_stepper_options": (C.c_int, [vp, C.POINTER(cs_stepper_options)]),
+        "cs_batch_step": (C.c_int, [vp, C.c_double, C.c_int32]),
+        "cs_batch_get_positions": (C.c_int, [vp, vp]),
+        "cs_batch_get_velocities": (C.c_int, [vp, vp]),
+        "cs_batch_stats": (C.c_int, [vp, vp]),
+        "cs_batch_autotune": (C.c_int, [vp, C.c_double, C.POINTER(C.c_int32)]),
+        "cs_batch_set_threads": (C.c_int, [vp, C.c_int32]),
+        "cs_batch_stream": (vp, [vp]),
         "cs_build_grid": (C.c_int, [C.c_int32, C.c_int32, C.c_double, C.c_double, vp, vp, vp]),
         "cs_preprocess": (C.c_int, [C.c_int32, C.c_int32, vp, vp, vp, C.c_double, vp, vp, vp,
                                     C.POINTER(C.c_int32), vp, vp]),

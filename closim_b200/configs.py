@@ -8,6 +8,7 @@ is the reference's y (vertical), config "z = c" floors are y = c.
   floor_drape   64 x 64 sheet released 0.3 m above a y = 0 floor (barrier + friction)
   sphere_drape  256 x 256 sheet dropped onto a static sphere, folding onto itself
   material_fit  96 x 96 sheet hung from two corners, loss on the final positions (adjoint)
+  batch_sheets  512 independent sheets of uneven size, stepped together (batched solver)
 """
 from __future__ import annotations
 
@@ -141,6 +142,41 @@ def material_fit(seed: int = 4, nx: int = 95, ny: int = 95, w: float = 0.6, hgt:
                 fixed_pins=[0, nx], moving_pins=[], pin_velocity=(0.0, 0.0, 0.0),
                 contact=dict(dHatM=1e-3, kappaJ=50.0, dMinM=1e-4, frictionMu=0.3, frictionEpsM=1e-4, floorY=floor_y),
                 theta_gt=theta_gt, theta0=theta0, seed=seed)
+
+
+def batch_sheets(seed: int = 5, count: int = 512, side_min: int = 16, side_max: int = 128, steps: int = 100,
+                 sheet_size: float = 0.5, floor_y: float = -0.5, spacing: float = 0.0):
+    """Batched uneven instances: `count` independent sheets, vertex-grid side
+    s ~ U{side_min..side_max} (seeded), each buildGrid(s-1, s-1, L, L) with
+    L = sheet_size; C00, C11 ~ U[2e3, 1e4], G ~ U[5e2, 2e3], k_bend ~ logU[1e-5,
+    1e-3]; pinned at two seeded boundary vertices; floor contact at y = -0.5;
+    h = 0.01 s. Sheets do not interact (each is its own scene); `spacing`
+    only offsets them in x for viewing. Returns a list of single-sheet
+    workload dicts sharing h, gravity, contact parameters and options."""
+    rng = np.random.default_rng(seed)
+    sheets = []
+    for i in range(count):
+        sd = int(rng.integers(side_min, side_max + 1))
+        pos, uv, idx = buildGrid(sd - 1, sd - 1, sheet_size, sheet_size)
+        n = len(pos) // 3
+        x = pos.astype(np.float64)
+        x[0::3] += i * spacing
+        c00, c11 = rng.uniform(2e3, 1e4, 2)
+        g = rng.uniform(5e2, 2e3)
+        kb = float(np.exp(rng.uniform(np.log(1e-5), np.log(1e-3))))
+        boundary = [j for j in range(n) if j % sd in (0, sd - 1) or j // sd in (0, sd - 1)]
+        pins = sorted(int(v) for v in rng.choice(boundary, 2, replace=False))
+        sheets.append(dict(name=f"batch_sheet_{i}", pos=pos, uv=uv, idx=idx, density=0.2,
+                           material=_material(stretchWarp=float(c00), stretchWeft=float(c11), shear=float(g),
+                                              bendWarp=kb, bendWeft=kb),
+                           x=x, v=np.zeros(n * 3), gravity=(0.0, -9.81, 0.0), h=0.01, steps=steps,
+                           options=dict(newtonIters=10, pcgMaxIters=60, gradTol=1e-5, lineSearchIters=10,
+                                        precond="jacobi"),
+                           fixed_pins=pins, moving_pins=[], pin_velocity=(0.0, 0.0, 0.0),
+                           contact=dict(dHatM=1e-3, kappaJ=50.0, dMinM=1e-4, frictionMu=0.3, frictionEpsM=1e-4,
+                                        floorY=floor_y),
+                           side=sd, seed=seed))
+    return sheets
 
 
 def with_theta(cfg: dict, theta) -> dict:

@@ -185,13 +185,14 @@ int cs_set_newton_mode(cs_solver* h, int32_t mode, double tol) {
   });
 }
 
-int cs_adjoint_stats(cs_solver* h, double* out4) {
+int cs_adjoint_stats(cs_solver* h, double* out5) {
   return guarded(h, [&] {
-    if (!out4) throw std::invalid_argument("null output");
-    out4[0] = (double)h->s.adjStats.pcgIters;
-    out4[1] = h->s.adjStats.solves;
-    out4[2] = h->s.adjStats.recomputedSteps;
-    out4[3] = h->s.adjStats.maxRelResidual;
+    if (!out5) throw std::invalid_argument("null output");
+    out5[0] = (double)h->s.adjStats.pcgIters;
+    out5[1] = h->s.adjStats.solves;
+    out5[2] = h->s.adjStats.recomputedSteps;
+    out5[3] = h->s.adjStats.maxRelResidual;
+    out5[4] = h->s.adjStats.forwardConverged;
   });
 }
 

@@ -66,6 +66,7 @@ struct AdjStats {
   long pcgIters = 0;
   int solves = 0, recomputedSteps = 0;
   double maxRelResidual = 0;
+  int forwardConverged = 0;  // steps of the last cs_forward that reached gradTol
 };
 
 enum Phase { PH_OTHER = 0, PH_BROADPHASE, PH_ACTIVE_SET, PH_GRADIENT, PH_PRECOND, PH_PCG, PH_TRIAL, PH_ENERGY,
@@ -420,7 +421,11 @@ class Solver {
           alpha *= 0.5;
           continue;
         }
-        if (eNew <= energy + 1e-4 * alpha * gtdx) {
+        // Exact-Newton mode, close to convergence: the energy decrease of a full
+        // step falls below the rounding of the energy sum, so Armijo is decided
+        // by noise; a CCD-valid full step is taken (local quadratic convergence).
+        const bool nearConverged = newtonMode == 1 && gradNorm < 1e-7 && alpha == 1;
+        if (nearConverged || eNew <= energy + 1e-4 * alpha * gtdx) {
           std::swap(d.x, d.xt);
           energy = eNew;
           accepted = true;
@@ -527,6 +532,7 @@ class Solver {
     ro.seg.alloc((size_t)K * n3);
     ro.xN.alloc(n3);
     ro.vN.alloc(n3);
+    int conv = 0;
     for (int st = 0; st < steps; st++) {
       if (st % K == 0) {
         const size_t c = st / K;
@@ -534,7 +540,9 @@ class Solver {
         CK(cudaMemcpyAsync(ro.ckV.p + c * n3, d.v, n3 * 8, cudaMemcpyDeviceToDevice, stream));
       }
       step(h);
+      conv += stats.converged ? 1 : 0;
     }
+    adjStats.forwardConverged = conv;
     CK(cudaMemcpyAsync(ro.xN.p, d.x, n3 * 8, cudaMemcpyDeviceToDevice, stream));
     CK(cudaMemcpyAsync(ro.vN.p, d.v, n3 * 8, cudaMemcpyDeviceToDevice, stream));
     CK(cudaStreamSynchronize(stream));
@@ -554,7 +562,9 @@ class Solver {
     const int blocks = adj_grid_blocks(d);
     double* const xPrimary = d.x;
     double* const x0Primary = d.x0;
+    const int fwdConv = adjStats.forwardConverged;
     adjStats = AdjStats{};
+    adjStats.forwardConverged = fwdConv;
     const int nck = (ro.steps + ro.K - 1) / ro.K;
     std::vector<double> hout(3);
     for (int c = nck - 1; c >= 0; c--) {

@@ -398,9 +398,10 @@ class CudaSolver:
         self._check(self._lib.cs_set_adjoint_options(self._h, maxIters, tol))
 
     def adjointStats(self) -> dict:
-        out = np.zeros(4)
+        out = np.zeros(5)
         self._check(self._lib.cs_adjoint_stats(self._h, L.ptr(out)))
-        return dict(pcgIters=int(out[0]), solves=int(out[1]), recomputedSteps=int(out[2]), maxRelResidual=out[3])
+        return dict(pcgIters=int(out[0]), solves=int(out[1]), recomputedSteps=int(out[2]), maxRelResidual=out[3],
+                    forwardConverged=int(out[4]))
 
     def launchInfo(self) -> dict:
         out = np.zeros(4, np.int32)

@@ -179,9 +179,10 @@ int cs_backward(cs_solver* s, const double* dL_dxN, double* dL_dtheta, double* d
 int cs_set_newton_mode(cs_solver* s, int32_t mode, double tol);
 /* Adjoint PCG budget (default 2000 iterations, relative residual 1e-10). */
 int cs_set_adjoint_options(cs_solver* s, int32_t max_iters, double tol);
-/* out[4]: adjoint PCG iterations, solves, recomputed steps, largest final
- * relative residual, for the last cs_backward. */
-int cs_adjoint_stats(cs_solver* s, double* out4);
+/* out[5]: adjoint PCG iterations, solves, recomputed steps and largest final
+ * relative residual of the last cs_backward; steps of the last cs_forward
+ * that converged (reached gradTol). */
+int cs_adjoint_stats(cs_solver* s, double* out5);
 
 /* ---- allocation-free membrane HVP (no counterpart in the reference) ----
  * For callers that may not call cudaMalloc while stepping: a frame recorded into
