@@ -148,6 +148,31 @@ def run_reference(args, rank):
     return 0
 
 
+def step_algorithmic_bytes(st, mesh, precision, cfg):
+    """Algorithmic bytes of one step from its measured counts (Newton
+    iterations, PCG iterations, Armijo trials, contacts): per Newton iteration a
+    gradient pass, per PCG iteration an HVP and the vector updates, per trial an
+    energy pass, and per broadphase query the boxes, sort passes and nodes; f is
+    the PCG vector width (4 mixed, 8 FP64), constants 4 B, 64 B per frozen
+    contact record, 48 B per CCD candidate primitive."""
+    f = 4 if precision == "mixed" else 8
+    n, m, hg = mesh.count, mesh.triCount, mesh.hinges.shape[0]
+    c = st.contact["activePairs"] if st.contact else 0
+    cand = st.contact["candidatePairs"] if st.contact else 0
+    D = (n + 7) // 8 if cfg["options"]["precond"] == "schwarz" else 0
+    b_grad = (9 * f + 4) * n + 32 * m + (16 + 3 * f) * hg + 64 * c
+    b_e = (6 * f + 4) * n + 32 * m + (16 + 3 * f) * hg + 64 * c
+    b_hvp = (9 * f + 4) * n + 32 * m + 64 * c
+    b_vec = 24 * f * n + D * 300 * 4
+    newton = max(st.newtonItersUsed, 1)
+    trials = st.armijoTrials
+    b = newton * b_grad + st.pcgIters * (b_hvp + b_vec) + trials * b_e
+    if st.contact:
+        queries = newton + trials + 2
+        b += queries * (6 * f * n + 12 * m + 24 * m + 8 * m + 2 * 8 * m * 4 + 2 * m * 40) + trials * 48 * cand
+    return float(b)
+
+
 def pcg_kernel_name(precision, prof):
     if precision != "mixed":
         return "k_pcg"
@@ -185,6 +210,8 @@ def run_precision(cfg, precision, local, args, ext_stream_cb, flush, sampler=Non
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     total = 0.0
+    step_bytes = 0.0
+    mesh = configs.make_scene(cfg).mesh
     for _ in range(args.steps):
         set_pins()
         with torch.cuda.stream(ext):
@@ -194,6 +221,7 @@ def run_precision(cfg, precision, local, args, ext_stream_cb, flush, sampler=Non
         ev1.record(ext)
         ev1.synchronize()
         total += ev0.elapsed_time(ev1)
+        step_bytes += step_algorithmic_bytes(solver.lastStats, mesh, precision, cfg)
     torch.cuda.synchronize()
     if prof_out is not None:
         prof_out.update(solver.profileRead())
@@ -201,6 +229,7 @@ def run_precision(cfg, precision, local, args, ext_stream_cb, flush, sampler=Non
     launches = solver.kernelLaunches() - launches0
     if prof_out is not None:
         prof_out["launch_info"] = solver.launchInfo()
+        prof_out["step_bytes"] = step_bytes
     if prof_out is not None and args.phase_steps > 0:
         # wall-time breakdown over a few extra (untimed) steps
         solver.profile(True, phases=True)
@@ -428,6 +457,10 @@ def main():
             "gpu_launches": res[headline]["launches"],
             "clocks": clocks,
             "phases_ms_per_step": prof.get("phases_ms_per_step"),
+            "step_roofline": {"bound": "hbm", "alg_bytes_per_step": prof.get("step_bytes", 0.0) / args.steps,
+                              "achieved": prof.get("step_bytes", 0.0) / (total_ms / 1000.0) / 1e9,
+                              "peak": measured_peak()[0], "unit": "GB/s",
+                              "frac": prof.get("step_bytes", 0.0) / (total_ms / 1000.0) / 1e9 / measured_peak()[0]},
             "launch_info": prof.get("launch_info"),
         }
         if args.skip:

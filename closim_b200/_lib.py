@@ -58,7 +58,8 @@ EXPORTS = ["cs_create", "cs_destroy", "cs_last_error", "cs_initialize", "cs_set_
            "cs_set_adjoint_options", "cs_adjoint_stats", "cs_set_newton_mode", "cs_batch_create", "cs_batch_destroy",
            "cs_batch_last_error", "cs_batch_initialize", "cs_batch_set_contact", "cs_batch_set_stepper_options",
            "cs_batch_step", "cs_batch_get_positions", "cs_batch_get_velocities", "cs_batch_stats",
-           "cs_batch_autotune", "cs_batch_set_threads", "cs_batch_stream", "cs_build_grid",
+           "cs_batch_autotune", "cs_batch_set_threads", "cs_batch_stream", "cs_session_step", "cs_session_reset",
+           "cs_session_restore_stable", "cs_build_grid",
            "cs_preprocess", "cs_broadphase_create", "cs_broadphase_destroy", "cs_broadphase_last_error",
            "cs_broadphase_build", "cs_broadphase_diagnostics", "cs_broadphase_pairs", "cs_broadphase_state"]
 
@@ -117,6 +118,9 @@ def load():
         "cs_batch_autotune": (C.c_int, [vp, C.c_double, C.POINTER(C.c_int32)]),
         "cs_batch_set_threads": (C.c_int, [vp, C.c_int32]),
         "cs_batch_stream": (vp, [vp]),
+        "cs_session_step": (C.c_int, [vp, C.c_double, vp, C.POINTER(C.c_int32)]),
+        "cs_session_reset": (C.c_int, [vp]),
+        "cs_session_restore_stable": (C.c_int, [vp, C.POINTER(C.c_int32)]),
         "cs_build_grid": (C.c_int, [C.c_int32, C.c_int32, C.c_double, C.c_double, vp, vp, vp]),
         "cs_preprocess": (C.c_int, [C.c_int32, C.c_int32, vp, vp, vp, C.c_double, vp, vp, vp,
                                     C.POINTER(C.c_int32), vp, vp]),

@@ -53,7 +53,7 @@ __device__ bool floor_trial_ok(const BatchDev& b, const Range& R, const double* 
       if (toi < 1 - 1e-9) bad = 1;
     }
   }
-  const double m = -block_max(-mn, sm);
+  const double m = block_min(mn, sm);
   const double anyBad = block_max((double)bad, sm);
   return !(m <= b.dMin) && anyBad == 0;
 }

@@ -423,6 +423,65 @@ void bvh_refit(BvhBufs& b, const double* x0, const double* x1, double pad, bool 
 
 static inline int nq(int n) { return (n + 127) / 128; }
 
+void bvh_boxes(BvhBufs& b, const double* x0, const double* x1, double pad, cudaStream_t s, int64_t* launches) {
+  k_boxes<<<nb(b.m), kBT, 0, s>>>(b, x0, x1, pad);
+  *launches += 1;
+}
+
+// Warp-aggregated append of kept pairs.
+__device__ __forceinline__ void append_pair(bool keep, int2 pr, int2* out, uint32_t cap, uint32_t* cnt) {
+  const uint32_t mask = __ballot_sync(0xffffffffu, keep);
+  if (!mask) return;
+  const int lane = threadIdx.x & 31;
+  const int leader = __ffs(mask) - 1;
+  uint32_t base = 0;
+  if (lane == leader) base = atomicAdd(cnt, (uint32_t)__popc(mask));
+  base = __shfl_sync(0xffffffffu, base, leader);
+  if (keep) {
+    const uint32_t slot = base + __popc(mask & ((1u << lane) - 1u));
+    if (slot < cap) out[slot] = pr;
+  }
+}
+
+__global__ void __launch_bounds__(256) k_filter_self(BvhBufs b, const int2* sup, int nsup, int2* out, uint32_t cap,
+                                                     uint32_t* cnt) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  bool keep = false;
+  int2 pr = make_int2(0, 0);
+  if (i < nsup) {
+    pr = sup[i];
+    keep = ov6d(b.box64 + (size_t)pr.x * 6, b.box64 + (size_t)pr.y * 6);
+  }
+  append_pair(keep, pr, out, cap, cnt);
+}
+
+__global__ void __launch_bounds__(256) k_filter_static(BvhBufs b, const int2* sup, int nsup, double pad, int2* out,
+                                                       uint32_t cap, uint32_t* cnt) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  bool keep = false;
+  int2 pr = make_int2(0, 0);
+  if (i < nsup) {
+    pr = sup[i];
+    double s64[6];
+    static_box(b, pr.y, pad, s64);
+    keep = ov6d(b.box64 + (size_t)pr.x * 6, s64);
+  }
+  append_pair(keep, pr, out, cap, cnt);
+}
+
+void filter_pairs(const BvhBufs& b, const int2* sup, int nsup, int2* out, uint32_t cap, uint32_t* cnt,
+                  const int2* ssup, int nssup, double pad, int2* sout, uint32_t scap, uint32_t* scnt, cudaStream_t s,
+                  int64_t* launches) {
+  if (nsup > 0) {
+    k_filter_self<<<(nsup + 255) / 256, 256, 0, s>>>(b, sup, nsup, out, cap, cnt);
+    *launches += 1;
+  }
+  if (nssup > 0) {
+    k_filter_static<<<(nssup + 255) / 256, 256, 0, s>>>(b, ssup, nssup, pad, sout, scap, scnt);
+    *launches += 1;
+  }
+}
+
 void bvh_count_self(BvhBufs& b, bool mirror, cudaStream_t s, int64_t* launches) {
   if (b.m < 2) {
     cudaMemsetAsync(b.cnt, 0, (size_t)(b.m + 1) * 4, s);
@@ -454,9 +513,9 @@ __device__ __forceinline__ void put_cand(int* rec, int slot, int kind, int p, in
   r[0] = kind; r[1] = p; r[2] = a; r[3] = bb; r[4] = c; r[5] = d;
 }
 
-__global__ void k_expand_self(CandBufs c, const uint32_t* idx, const int2* pairs, int np) {
+__global__ void k_expand_self(CandBufs c, const uint32_t* idx, const int2* pairs, const uint32_t* dcnt) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= np) return;
+  if (i >= (int)dcnt[0]) return;
   const int tA = pairs[i].x, tB = pairs[i].y;
   const int A[3] = {(int)idx[tA * 3], (int)idx[tA * 3 + 1], (int)idx[tA * 3 + 2]};
   const int B[3] = {(int)idx[tB * 3], (int)idx[tB * 3 + 1], (int)idx[tB * 3 + 2]};
@@ -472,10 +531,11 @@ __global__ void k_expand_self(CandBufs c, const uint32_t* idx, const int2* pairs
     }
 }
 
-__global__ void k_expand_static(CandBufs c, const uint32_t* idx, const uint32_t* sidx, const int2* pairs, int np,
-                                int base) {
+__global__ void k_expand_static(CandBufs c, const uint32_t* idx, const uint32_t* sidx, const int2* pairs,
+                                const uint32_t* dcnt) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= np) return;
+  if (i >= (int)dcnt[1]) return;
+  const int base = 15 * (int)dcnt[0];
   const int ct = pairs[i].x, st = pairs[i].y;
   const int A[3] = {(int)idx[ct * 3], (int)idx[ct * 3 + 1], (int)idx[ct * 3 + 2]};
   const int B[3] = {(int)sidx[st * 3], (int)sidx[st * 3 + 1], (int)sidx[st * 3 + 2]};
@@ -487,12 +547,12 @@ __global__ void k_expand_static(CandBufs c, const uint32_t* idx, const uint32_t*
       put_cand(c.rec, slot++, 1, -1, A[E[e][0]], A[E[e][1]], -(B[E[f][0]] + 2), -(B[E[f][1]] + 2));
 }
 
-void expand_candidates(CandBufs& c, const uint32_t* idx, const uint32_t* sidx, int ns, const int2* selfPairs,
-                       int nSelf, const int2* staticPairs, int nStatic, cudaStream_t s, int64_t* launches) {
-  (void)ns;
-  if (nSelf) { k_expand_self<<<nb(nSelf), kBT, 0, s>>>(c, idx, selfPairs, nSelf); *launches += 1; }
-  if (nStatic) {
-    k_expand_static<<<nb(nStatic), kBT, 0, s>>>(c, idx, sidx, staticPairs, nStatic, nSelf * 15);
+void expand_candidates(CandBufs& c, const uint32_t* idx, const uint32_t* sidx, const int2* selfPairs, int selfCap,
+                       const int2* staticPairs, int staticCap, const uint32_t* dcnt, cudaStream_t s,
+                       int64_t* launches) {
+  if (selfCap) { k_expand_self<<<nb(selfCap), kBT, 0, s>>>(c, idx, selfPairs, dcnt); *launches += 1; }
+  if (staticCap) {
+    k_expand_static<<<nb(staticCap), kBT, 0, s>>>(c, idx, sidx, staticPairs, dcnt);
     *launches += 1;
   }
 }

@@ -64,6 +64,15 @@ void bvh_append_self(BvhBufs& b, cudaStream_t s, int64_t* launches);
 void bvh_append_static(BvhBufs& b, double pad, int2* out, uint32_t cap, uint32_t* cnt, cudaStream_t s,
                        int64_t* launches);
 void scan_counts(uint32_t* cnt, int n, uint32_t* total, cudaStream_t s, int64_t* launches);
+// Swept boxes of a new segment only (box64 / boxc / boxr / centroids), no refit.
+void bvh_boxes(BvhBufs& b, const double* x0, const double* x1, double pad, cudaStream_t s, int64_t* launches);
+// Exact query against a superset of pairs: keeps the self pairs whose current
+// f64 boxes overlap (adjacency was excluded when the superset was built) and
+// the static pairs whose cloth box overlaps the static box padded by `pad`;
+// appended through cnt[0] / scnt[0] (order arbitrary).
+void filter_pairs(const BvhBufs& b, const int2* sup, int nsup, int2* out, uint32_t cap, uint32_t* cnt,
+                  const int2* ssup, int nssup, double pad, int2* sout, uint32_t scap, uint32_t* scnt, cudaStream_t s,
+                  int64_t* launches);
 
 // Candidates: 15 per self pair (6 VT + 9 EE; void slots get kind 3), 12 per
 // static pair (3 VT + 9 EE). rec holds 6 ints per candidate in expansion order.
@@ -74,8 +83,12 @@ struct CandBufs {
   uint32_t* p0 = nullptr; uint32_t* p1 = nullptr;
   uint32_t* hist = nullptr;
 };
-void expand_candidates(CandBufs& c, const uint32_t* idx, const uint32_t* sidx, int ns, const int2* selfPairs,
-                       int nSelf, const int2* staticPairs, int nStatic, cudaStream_t s, int64_t* launches);
+// The exact pair counts stay on the device (dcnt[0] self, dcnt[1] static);
+// selfCap / staticCap bound them from the host. Static candidates start at 15
+// dcnt[0].
+void expand_candidates(CandBufs& c, const uint32_t* idx, const uint32_t* sidx, const int2* selfPairs, int selfCap,
+                       const int2* staticPairs, int staticCap, const uint32_t* dcnt, cudaStream_t s,
+                       int64_t* launches);
 
 // Order key of a candidate (contact-assembly.ts:118: kind, p, a, b, c, d),
 // packed as a 128-bit integer (w[0] most significant) with `bits` bits per id;

@@ -94,6 +94,29 @@ __device__ __forceinline__ T block_max(T v, T* smem) {
   return r;
 }
 
+// Block-wide minimum (identity +infinity; inputs must not be NaN).
+__device__ __forceinline__ double block_min(double v, double* smem) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_down_sync(0xffffffffu, v, o));
+  __syncthreads();
+  if (lane == 0) smem[warp] = v;
+  __syncthreads();
+  const int nw = (blockDim.x + 31) >> 5;
+  double r = INFINITY;
+  if (warp == 0) {
+    r = lane < nw ? smem[lane] : INFINITY;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) r = fmin(r, __shfl_down_sync(0xffffffffu, r, o));
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) smem[0] = r;
+  __syncthreads();
+  r = smem[0];
+  __syncthreads();
+  return r;
+}
+
 // Sum of nparts partials in a fixed order by one warp (every caller gets the
 // same bits), used after a grid-wide barrier.
 template <class T>

@@ -28,6 +28,7 @@ struct CView {  // kernel view of the contact host buffers
   const int* rec;              // candidates in expansion order (6 ints each)
   int ns, idBits;              // static vertex count, bits per id in the order key
   unsigned long long* badKey;  // [hi, lo] smallest (key, status) of a failing CCD candidate
+  const uint32_t* ccnt;        // [self pairs, static pairs] of the current query (device)
   uint32_t* cflag;
   uint32_t* fflag;
   double* cmin;
@@ -71,9 +72,15 @@ __device__ __forceinline__ void cand_closest(const CView& v, const double* x, co
   }
 }
 
-__global__ void k_cand_flags(CView v, const double* x, int C) {
+// Candidates of the current query: 15 per self pair, 12 per static pair.
+__device__ __forceinline__ int cand_count(const CView& v) { return 15 * (int)v.ccnt[0] + 12 * (int)v.ccnt[1]; }
+
+// Ccap bounds the candidate count from the host; slots past the device count
+// are cleared so scans and minima over Ccap see nothing there.
+__global__ void k_cand_flags(CView v, const double* x, int Ccap) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= C) return;
+  if (i >= Ccap) return;
+  if (i >= cand_count(v)) { v.cflag[i] = 0; v.cmin[i] = INFINITY; return; }
   const int* r = v.rec + (size_t)i * 6;
   if (r[0] == 3) { v.cflag[i] = 0; v.cmin[i] = INFINITY; return; }
   Closest cp;
@@ -419,12 +426,13 @@ __global__ void k_trial_reset(int* cint, unsigned long long* badKey) {
   badKey[1] = ~0ull;
 }
 
-__global__ void k_trial_cand(CView v, const double* xt, int C, double dMin) {
+__global__ void k_trial_cand(CView v, const double* xt, int Ccap, double dMin) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= C) return;
-  const int* r = v.rec + (size_t)i * 6;
+  if (i >= Ccap) return;
   v.cflag[i] = 0;
   v.ctoi[i] = INFINITY;
+  if (i >= cand_count(v)) { v.cmin[i] = INFINITY; return; }
+  const int* r = v.rec + (size_t)i * 6;
   if (r[0] == 3) { v.cmin[i] = INFINITY; return; }
   Closest cp;
   cand_closest(v, xt, r, cp);
@@ -593,6 +601,7 @@ static CView view(ContactHost& h, Solver& s) {
   v.ns = h.ns;
   v.idBits = h.idBits;
   v.badKey = h.badKey;
+  v.ccnt = (const uint32_t*)(h.cint + CI_SELF);
   v.cflag = h.cflag;
   v.fflag = h.fflag;
   v.cmin = h.cmin;
@@ -625,7 +634,8 @@ ContactHost::~ContactHost() {
                    (void**)&cg, (void**)&tc, (void**)&tf, (void**)&rk0, (void**)&rk1, (void**)&rp0, (void**)&rp1,
                    (void**)&rhist, (void**)&cOff, (void**)&lagFloor, (void**)&lagFloorOk, (void**)&lk0,
                    (void**)&lk1, (void**)&lp0, (void**)&lp1, (void**)&lhist, (void**)&lval, (void**)&lsorted,
-                   (void**)&probe, (void**)&diag, (void**)&cint, (void**)&minpart})
+                   (void**)&probe, (void**)&diag, (void**)&cint, (void**)&minpart, (void**)&supPairs,
+                   (void**)&supSPairs})
     if (*q) cudaFree(*q);
   if (hint) cudaFreeHost(hint);
   if (hdiag) cudaFreeHost(hdiag);
@@ -778,6 +788,38 @@ void ContactHost::read_ints(Solver& s) {
   CK(cudaStreamSynchronize(s.stream));
 }
 
+void ContactHost::build_superset(Solver& s, const double* x, double padSup) {
+  cudaStream_t st = s.stream;
+  int64_t& lc = launch_counter();
+  bvh_build(bvh, s.d.x0, x, padSup, false, st, &lc);
+  topoValid = true;
+  if (supCap == 0) { supCap = std::max<size_t>(pairCap, 1024); dalloc(supPairs, supCap); }
+  if (supSCap == 0) { supSCap = std::max<size_t>(spairCap, 64); dalloc(supSPairs, supSCap); }
+  for (int attempt = 0; attempt < 2; attempt++) {
+    CK(cudaMemsetAsync(cint, 0, CI_N * sizeof(int), st));
+    BvhBufs sb = bvh;
+    sb.cnt = (uint32_t*)(cint + CI_SELF);
+    sb.pairs = supPairs;
+    sb.pairCap = (uint32_t)supCap;
+    bvh_append_self(sb, st, &lc);
+    if (ms > 0) bvh_append_static(bvh, padSup, supSPairs, (uint32_t)supSCap, (uint32_t*)(cint + CI_STATIC), st, &lc);
+    read_ints(s);
+    if (hint[CI_OVERFLOW]) throw CapacityError("broadphase traversal aborted (stack deeper than 64 or malformed tree)");
+    const size_t P = (uint32_t)hint[CI_SELF], S = ms > 0 ? (uint32_t)hint[CI_STATIC] : 0u;
+    nSup = (int)P;
+    nSupS = (int)S;
+    if (P <= supCap && S <= supSCap) break;
+    if (attempt == 1) throw CapacityError("broadphase superset changed between identical traversals");
+    if (P > supCap) { supCap = P + P / 2 + 64; dalloc(supPairs, supCap); }
+    if (S > supSCap) { supSCap = S + S / 2 + 64; dalloc(supSPairs, supSCap); }
+  }
+  ensure_pairs((size_t)nSup, (size_t)nSupS);
+  const long Ccap = 15l * nSup + 12l * nSupS;
+  if (Ccap > INT_MAX / 8) throw CapacityError("too many contact candidates");
+  ensure_cands((size_t)Ccap);
+  CK(cudaMemsetAsync(cint, 0, CI_N * sizeof(int), st));
+}
+
 int ContactHost::build_candidates(Solver& s, const double* x, double pad) {
   struct Restore {
     Solver& s;
@@ -792,41 +834,62 @@ int ContactHost::build_candidates(Solver& s, const double* x, double pad) {
   cudaStream_t st = s.stream;
   int64_t& lc = launch_counter();
   CK(cudaMemsetAsync(cint, 0, CI_N * sizeof(int), st));
-  // The hierarchy is built once per step and refitted for every later segment:
-  // the exact pair set does not depend on the tree's shape.
-  if (!topoValid) {
-    bvh_build(bvh, s.d.x0, x, pad, false, st, &lc);
-    topoValid = true;
+  // Every position a step visits stays within newton_iters trust-region moves
+  // (|dx|_inf <= 2 mm each, newton.ts:163-179) of the segment x0 -> x of the
+  // step's first query, so a superset traversal with the pad widened by that
+  // distance contains every later query's pairs, which are then filtered
+  // exactly. Budgets that allow more than 2.5 cm of travel traverse per query.
+  const double travel = 0.002 * s.opts.newton_iters;
+  if (travel <= 0.025) {
+    if (!supValid) {
+      build_superset(s, x, std::max(p.dhat, p.dmin) + travel + 1e-9);
+      supValid = true;
+    }
+    // A query keeps a subset of the superset, so sizing every buffer for the
+    // superset lets the counts stay on the device (no host round trip here).
+    bvh_boxes(bvh, s.d.x0, x, pad, st, &lc);
+    filter_pairs(bvh, supPairs, nSup, bvh.pairs, (uint32_t)pairCap, (uint32_t*)(cint + CI_SELF), supSPairs, nSupS,
+                 pad, spairs, (uint32_t)spairCap, (uint32_t*)(cint + CI_STATIC), st, &lc);
+    const long Ccap = 15l * nSup + 12l * nSupS;
+    expand_candidates(cand, s.idx.p, sidx, bvh.pairs, nSup, spairs, ms > 0 ? nSupS : 0,
+                      (const uint32_t*)(cint + CI_SELF), st, &lc);
+    return (int)Ccap;
   } else {
-    bvh_refit(bvh, s.d.x0, x, pad, false, st, &lc);
-  }
-  for (int attempt = 0; attempt < 2; attempt++) {
-    BvhBufs sb = bvh;
-    sb.cnt = (uint32_t*)(cint + CI_SELF);
-    sb.pairCap = (uint32_t)pairCap;
-    bvh_append_self(sb, st, &lc);
-    if (ms > 0) bvh_append_static(bvh, pad, spairs, (uint32_t)spairCap, (uint32_t*)(cint + CI_STATIC), st, &lc);
-    read_ints(s);
-    if (hint[CI_OVERFLOW]) throw CapacityError("broadphase traversal aborted (stack deeper than 64 or malformed tree)");
-    const uint32_t P = (uint32_t)hint[CI_SELF], S = ms > 0 ? (uint32_t)hint[CI_STATIC] : 0u;
-    if (P <= pairCap && S <= spairCap) break;
-    if (attempt == 1) throw CapacityError("broadphase pair count changed between identical traversals");
-    ensure_pairs(P, S);
-    CK(cudaMemsetAsync(cint + CI_SELF, 0, 2 * sizeof(int), st));
+    // The hierarchy is built once per step and refitted for every later segment:
+    // the exact pair set does not depend on the tree's shape.
+    if (!topoValid) {
+      bvh_build(bvh, s.d.x0, x, pad, false, st, &lc);
+      topoValid = true;
+    } else {
+      bvh_refit(bvh, s.d.x0, x, pad, false, st, &lc);
+    }
+    for (int attempt = 0; attempt < 2; attempt++) {
+      BvhBufs sb = bvh;
+      sb.cnt = (uint32_t*)(cint + CI_SELF);
+      sb.pairCap = (uint32_t)pairCap;
+      bvh_append_self(sb, st, &lc);
+      if (ms > 0) bvh_append_static(bvh, pad, spairs, (uint32_t)spairCap, (uint32_t*)(cint + CI_STATIC), st, &lc);
+      read_ints(s);
+      if (hint[CI_OVERFLOW]) throw CapacityError("broadphase traversal aborted (stack deeper than 64 or malformed tree)");
+      const uint32_t P = (uint32_t)hint[CI_SELF], S = ms > 0 ? (uint32_t)hint[CI_STATIC] : 0u;
+      if (P <= pairCap && S <= spairCap) break;
+      if (attempt == 1) throw CapacityError("broadphase pair count changed between identical traversals");
+      ensure_pairs(P, S);
+      CK(cudaMemsetAsync(cint + CI_SELF, 0, 2 * sizeof(int), st));
+    }
   }
   const int P = hint[CI_SELF], S = ms > 0 ? hint[CI_STATIC] : 0;
   const long C = 15l * P + 12l * S;
   if (C > INT_MAX / 8) throw CapacityError("too many contact candidates");
   ensure_cands(C);
-  expand_candidates(cand, s.idx.p, sidx, ns, bvh.pairs, P, spairs, S, st, &lc);
+  expand_candidates(cand, s.idx.p, sidx, bvh.pairs, P, spairs, S, (const uint32_t*)(cint + CI_SELF), st, &lc);
   return (int)C;
 }
 
 void ContactHost::update_active_set(Solver& s, double* x) {
   cudaStream_t st = s.stream;
   int64_t& lc = launch_counter();
-  const int C = build_candidates(s, x, p.dhat);
-  candidatePairs = C;
+  const int C = build_candidates(s, x, p.dhat);  // an upper bound; the exact count is on the device
   CK(cudaMemsetAsync(cint + CI_NVT, 0, sizeof(int), st));
   CView v = view(*this, s);
   if (C > 0) {
@@ -841,6 +904,7 @@ void ContactHost::update_active_set(Solver& s, double* x) {
   else CK(cudaMemsetAsync(cint + CI_NCAND, 0, sizeof(int), st));
   scan_counts(fflag, n, (uint32_t*)(cint + CI_NFLOOR), st, &lc);
   read_ints(s);
+  candidatePairs = 15.0 * (uint32_t)hint[CI_SELF] + 12.0 * (uint32_t)(ms > 0 ? hint[CI_STATIC] : 0);
   nCand = hint[CI_NCAND];
   nFloor = hint[CI_NFLOOR];
   nVT = hint[CI_NVT];
@@ -913,8 +977,7 @@ void ContactHost::merit_energy(Solver& s, const double* x) {
 bool ContactHost::check_trial(Solver& s, const double* xt) {
   cudaStream_t st = s.stream;
   int64_t& lc = launch_counter();
-  const int C = build_candidates(s, xt, p.dmin);
-  candidatePairs = C;
+  const int C = build_candidates(s, xt, p.dmin);  // an upper bound; the exact count is on the device
   k_trial_reset<<<1, 1, 0, st>>>(cint, badKey);
   lc++;
   CView v = view(*this, s);
@@ -929,6 +992,7 @@ bool ContactHost::check_trial(Solver& s, const double* xt) {
   k_trial_final<<<1, 1, 0, st>>>(v, minpart, minpart + kMinBlocks, p.dmin);
   lc += 5;
   read_ints(s);
+  candidatePairs = 15.0 * (uint32_t)hint[CI_SELF] + 12.0 * (uint32_t)(ms > 0 ? hint[CI_STATIC] : 0);
   return hint[CI_VALID] != 0;
 }
 
@@ -983,6 +1047,7 @@ void ContactHost::begin_step_and_bisect(Solver& s) {
   commitNo = 0;
   rejections = 0;
   topoValid = false;
+  supValid = false;
   candidatePairs = activePairs = vtPairs = eePairs = floorPairs = 0;
   nCand = nFloor = nVT = 0;
   bind(s);

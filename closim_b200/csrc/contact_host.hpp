@@ -51,6 +51,15 @@ class ContactHost {
   unsigned long long* badKey = nullptr;  // smallest failing (key, status) of a trial
   int idBits = 24;             // bits per id in the candidate order key
   bool topoValid = false;      // hierarchy built for the current step
+  // Per-step superset of candidate pairs: every query of a step lies within
+  // the trust-region hull of the step's first segment, so one traversal with a
+  // widened pad serves all of them and each query filters it exactly.
+  int2* supPairs = nullptr;
+  int2* supSPairs = nullptr;
+  size_t supCap = 0, supSCap = 0;
+  int nSup = 0, nSupS = 0;
+  bool supValid = false;
+  void build_superset(Solver& s, const double* x, double padSup);
   size_t pairCap = 0, spairCap = 0;
   CandBufs cand;
   uint32_t* cflag = nullptr;   // per-candidate flag / offset / trial status (cand cap + 1)
@@ -91,6 +100,7 @@ class ContactHost {
   // the hierarchy is rebuilt at the next query.
   void begin_segment(Solver& s) {
     topoValid = false;
+    supValid = false;
     (void)s;
   }
   void update_active_set(Solver& s, double* x);

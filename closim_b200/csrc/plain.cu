@@ -697,6 +697,27 @@ __global__ void k_velocity(Dev d, double damp) {
   d.v[i] = ((d.x[i] - d.x0[i]) / d.h) * damp;
 }
 
+// ---- simulation-session hand-off -------------------------------------------------
+// flag = 1 when any coordinate of x is non-finite.
+__global__ void k_nonfinite(const double* x, int n3, int* flag) {
+  int bad = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += gridDim.x * blockDim.x)
+    if (!isfinite(x[i])) bad = 1;
+  if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(flag, 1);
+}
+// stable <- x when the flag is clear (the last NaN-free state stays on the device).
+__global__ void k_keep_if_finite(const double* x, double* stable, int n3, const int* flag) {
+  if (*flag) return;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += gridDim.x * blockDim.x) stable[i] = x[i];
+}
+
+void launch_session_check(const double* x, double* stable, int n3, int* flag, cudaStream_t s) {
+  cudaMemsetAsync(flag, 0, sizeof(int), s);
+  const int blocks = std::min(1184, std::max(1, (n3 + kThreads - 1) / kThreads));
+  k_nonfinite<<<blocks, kThreads, 0, s>>>(x, n3, flag);
+  k_keep_if_finite<<<blocks, kThreads, 0, s>>>(x, stable, n3, flag);
+}
+
 // ---- launchers ------------------------------------------------------------------
 
 void launch_predict(const Dev& d, cudaStream_t s) {

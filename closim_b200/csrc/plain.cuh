@@ -98,6 +98,9 @@ void launch_schwarz_factor(const Dev& d, cudaStream_t s);
 int launch_pcg(const Dev& d, int maxIters, double tol, int gridBlocks, cudaStream_t s);
 void launch_trial(const Dev& d, double alpha, cudaStream_t s);   // xt = x + alpha dx, pins
 void launch_velocity(const Dev& d, double damp, cudaStream_t s);
+// SimulationSession.doStep hand-off (sim-session.ts:132-150) on the device:
+// flag = any non-finite coordinate; stable <- x when finite.
+void launch_session_check(const double* x, double* stable, int n3, int* flag, cudaStream_t s);
 int pcg_grid_blocks(const Dev& d);
 // FD membrane HVP over device arrays (T: 3n terms, h: 1 double, elem: 18m scratch).
 void launch_membrane_hvp(const uint32_t* idx, const float4* inv, const float* area, const Mat<double>& mat, int n,

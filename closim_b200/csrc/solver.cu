@@ -196,6 +196,24 @@ int cs_adjoint_stats(cs_solver* h, double* out5) {
   });
 }
 
+int cs_session_step(cs_solver* h, double dt, double* positions_out, int32_t* nan_free) {
+  return guarded(h, [&] {
+    const bool ok = h->s.session_step(dt, positions_out);
+    if (nan_free) *nan_free = ok ? 1 : 0;
+  });
+}
+
+int cs_session_restore_stable(cs_solver* h, int32_t* stable_step) {
+  return guarded(h, [&] {
+    const bool ok = h->s.session_restore();
+    if (stable_step) *stable_step = ok ? h->s.stableStep : -1;
+  });
+}
+
+int cs_session_reset(cs_solver* h) {
+  return guarded(h, [&] { h->s.session_reset(); });
+}
+
 int cs_solver_info(cs_solver* h, int32_t* out, int32_t n) {
   return guarded(h, [&] {
     if (!out || n <= 0) throw std::invalid_argument("null output");

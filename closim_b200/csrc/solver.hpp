@@ -171,6 +171,7 @@ class Solver {
     if (pev0) cudaEventDestroy(pev0);
     if (pev1) cudaEventDestroy(pev1);
     if (hscal) cudaFreeHost(hscal);
+    if (hNan) cudaFreeHost(hNan);
     if (stream) cudaStreamDestroy(stream);
   }
 
@@ -615,6 +616,51 @@ class Solver {
     CK(cudaStreamSynchronize(stream));
     if (dtheta) for (int j = 0; j < 4; j++) dtheta[j] = acc[j];
     if (contact) contact->bind(*this);
+  }
+
+  // ---- SimulationSession hand-off (sim-session.ts:120-150) ----------------------
+  DBuf<double> stableX;
+  DBuf<int> nanFlag;
+  int* hNan = nullptr;  // pinned mirror of nanFlag
+  int stableStep = -1, sessionSteps = 0;
+
+  void session_reset() {
+    if (!ready) throw std::logic_error("CpuSolver not initialized");
+    const size_t n3 = 3 * (size_t)mesh.n;
+    if (stableX.n < n3) stableX.alloc(n3);
+    if (nanFlag.n < 1) nanFlag.alloc(1);
+    if (!hNan) CK(cudaMallocHost(&hNan, sizeof(int)));
+    CK(cudaMemcpyAsync(stableX.p, d.x, n3 * 8, cudaMemcpyDeviceToDevice, stream));
+    CK(cudaStreamSynchronize(stream));
+    stableStep = 0;
+    sessionSteps = 0;
+  }
+
+  // One step, the NaN check and the stable snapshot on the device, then the
+  // positions into `out` (pinned host memory is fastest) with one sync.
+  bool session_step(double h, double* out) {
+    if (stableStep < 0) session_reset();
+    step(h);
+    sessionSteps++;
+    const size_t n3 = 3 * (size_t)mesh.n;
+    launch_session_check(d.x, stableX.p, (int)n3, nanFlag.p, stream);
+    launch_counter() += 2;
+    CK(cudaMemcpyAsync(hNan, nanFlag.p, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    if (out) CK(cudaMemcpyAsync(out, d.x, n3 * 8, cudaMemcpyDeviceToHost, stream));
+    CK(cudaStreamSynchronize(stream));
+    const bool finite = *hNan == 0;
+    if (finite) stableStep = sessionSteps;
+    return finite;
+  }
+
+  // restoreStable: positions <- the last NaN-free state, velocities <- 0.
+  bool session_restore() {
+    if (stableStep < 0) return false;
+    const size_t n3 = 3 * (size_t)mesh.n;
+    CK(cudaMemcpyAsync(d.x, stableX.p, n3 * 8, cudaMemcpyDeviceToDevice, stream));
+    CK(cudaMemsetAsync(d.v, 0, n3 * 8, stream));
+    CK(cudaStreamSynchronize(stream));
+    return true;
   }
 
   void get(double* out, bool vel) {

@@ -153,6 +153,20 @@ int cs_profile_phases(cs_solver* s, double* out, int32_t n);
  * grid-wide mixed PCG, out[2] CTAs of the FP64 PCG, out[3] Schwarz domains. */
 int cs_solver_info(cs_solver* s, int32_t* out, int32_t n);
 
+/* ---- SimulationSession.doStep hand-off (src/view/sim-session.ts:132-150) ----
+ * cs_session_step: one step, then on the device the NaN scan of the new
+ * positions and, when they are finite, a device copy into the stable
+ * snapshot; the positions land in positions_out (3n doubles; pinned host
+ * memory avoids a staging copy; may be NULL) and *nan_free tells whether they
+ * are finite -- one stream synchronization per step, where the reference
+ * scans and copies on the host. cs_session_reset makes the current positions
+ * the stable snapshot (SimulationSession.attach); cs_session_restore_stable
+ * puts the snapshot back with zero velocities (restoreStable) and reports the
+ * session step it was taken at (-1 when there is none). */
+int cs_session_step(cs_solver* s, double dt, double* positions_out, int32_t* nan_free);
+int cs_session_reset(cs_solver* s);
+int cs_session_restore_stable(cs_solver* s, int32_t* stable_step);
+
 /* ---- differentiable rollout (no counterpart in the reference) ----
  * cs_forward runs `steps` implicit steps of size dt from the current state
  * (pins held fixed) and keeps (x, v) at every checkpoint_every-th step start.
