@@ -250,7 +250,7 @@ def run_batch(args, world, rank, local):
     import torch.distributed as dist
     from closim_b200 import configs
     from closim_b200.batch import BatchSolver
-    sheets = configs.batch_sheets()
+    sheets = configs.batch_sheets(count=args.sheets)
     h = sheets[0]["h"]
     bs = BatchSolver(sheets, device=local)
     threads = bs.autotune(h)
@@ -281,6 +281,25 @@ def run_batch(args, world, rank, local):
     ev1.synchronize()
     graph_ms = ev0.elapsed_time(ev1)
     st = bs.stats()
+    # the same sheets stepped one by one by the single-sheet mixed solver (a
+    # sample of 8, scaled to the batch by triangle count)
+    import closim_b200 as cb
+    sample = sheets[:: max(1, len(sheets) // 8)][:8]
+    single_ms, single_m = 0.0, 0
+    for cfg in sample:
+        sc = configs.make_scene(dict(cfg, contact=None))  # no self-contact search in the comparison
+        so = cb.CudaSolver("mixed", device=local, **dict(cfg["options"], precond="jacobi"))
+        so.initialize(sc)
+        so.advance(h, 2)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        so.advance(h, 3)
+        torch.cuda.synchronize()
+        single_ms += (time.perf_counter() - t0) * 1000.0 / 3
+        single_m += len(cfg["idx"]) // 3
+        so.close()
+    total_m = int(sum(len(c["idx"]) // 3 for c in sheets))
+    single_est_ms = single_ms * total_m / max(single_m, 1)
     t = torch.tensor([total, graph_ms], dtype=torch.float64, device=f"cuda:{local}")
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -294,10 +313,17 @@ def run_batch(args, world, rank, local):
                 "config": {"workload": "batch_sheets", "sheets": S, "n": bs.N,
                            "m": int(sum(len(c["idx"]) // 3 for c in sheets)), "h": h,
                            "parallelism": f"replicas x{world}", "threads_per_sheet": threads,
+                           "resident_blocks": bs.launchShape()["blocks"],
                            "l2": "flushed between timed steps (256 MiB write)"},
                 "sheet_steps_per_s": world * S * args.steps / (total / 1000.0),
                 "graph_replay": {"steps": args.steps, "ms_per_step": graph_ms / args.steps},
                 "converged_sheets_last_step": int(sum(1 for x in st if x["converged"] == 1)),
+                "mean_newton_iters": float(np.mean([x["newtonIters"] for x in st])),
+                "mean_pcg_iters": float(np.mean([x["pcgIters"] for x in st])),
+                "single_sheet_solver_ms_per_batch_step": single_est_ms,
+                "single_sheet_solver_note": "8 sheets stepped one by one by the single-sheet mixed solver (Jacobi, "
+                                            "no contact), scaled to the batch by triangle count",
+                "speedup_vs_single_sheet_solver": single_est_ms / (total / args.steps),
                 "gpu_launches": 2 * args.steps, "clocks": clocks}
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -356,6 +382,7 @@ def main():
     ap.add_argument("--workload", default="floor_drape",
                     choices=["floor_drape", "strip_pull", "sphere_drape", "batch_sheets", "material_fit"])
     ap.add_argument("--rollout-steps", type=int, default=40, help="material_fit: steps of the timed rollout")
+    ap.add_argument("--sheets", type=int, default=512, help="batch_sheets: number of sheets (512 in the workload)")
     ap.add_argument("--skip", type=int, default=0, help="extra untimed steps before the timed region")
     ap.add_argument("--phase-steps", type=int, default=3, help="extra steps for the per-phase wall-time breakdown")
     ap.add_argument("--small", action="store_true", help="32x32 floor drape (for profiler captures)")

@@ -58,7 +58,7 @@ EXPORTS = ["cs_create", "cs_destroy", "cs_last_error", "cs_initialize", "cs_set_
            "cs_set_adjoint_options", "cs_adjoint_stats", "cs_set_newton_mode", "cs_batch_create", "cs_batch_destroy",
            "cs_batch_last_error", "cs_batch_initialize", "cs_batch_set_contact", "cs_batch_set_stepper_options",
            "cs_batch_step", "cs_batch_get_positions", "cs_batch_get_velocities", "cs_batch_stats",
-           "cs_batch_autotune", "cs_batch_set_threads", "cs_batch_stream", "cs_session_step", "cs_session_reset",
+           "cs_batch_autotune", "cs_batch_set_threads", "cs_batch_stream", "cs_batch_launch_shape", "cs_session_step", "cs_session_reset",
            "cs_session_restore_stable", "cs_build_grid",
            "cs_preprocess", "cs_broadphase_create", "cs_broadphase_destroy", "cs_broadphase_last_error",
            "cs_broadphase_build", "cs_broadphase_diagnostics", "cs_broadphase_pairs", "cs_broadphase_state"]
@@ -118,6 +118,7 @@ def load():
         "cs_batch_autotune": (C.c_int, [vp, C.c_double, C.POINTER(C.c_int32)]),
         "cs_batch_set_threads": (C.c_int, [vp, C.c_int32]),
         "cs_batch_stream": (vp, [vp]),
+        "cs_batch_launch_shape": (C.c_int, [vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
         "cs_session_step": (C.c_int, [vp, C.c_double, vp, C.POINTER(C.c_int32)]),
         "cs_session_reset": (C.c_int, [vp]),
         "cs_session_restore_stable": (C.c_int, [vp, C.POINTER(C.c_int32)]),

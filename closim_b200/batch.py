@@ -92,6 +92,11 @@ class BatchSolver:
         self._check(self._lib.cs_batch_autotune(self._h, float(dt), C.byref(t)))
         return t.value
 
+    def launchShape(self) -> dict:
+        t, b = C.c_int32(0), C.c_int32(0)
+        self._check(self._lib.cs_batch_launch_shape(self._h, C.byref(t), C.byref(b)))
+        return dict(threads=t.value, blocks=b.value)
+
     def setThreads(self, threads: int) -> None:
         self._check(self._lib.cs_batch_set_threads(self._h, int(threads)))
 

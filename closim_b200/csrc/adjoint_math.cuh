@@ -117,4 +117,41 @@ CSHD void bend_hvp(const double* q, const double* v, double restAngle, double ed
   for (int a = 0; a < 12; a++) out[a] = g[a].d;
 }
 
+// Closed-form 9x9 membrane Hessian block of one triangle (the derivative of
+// membrane.ts:17-80's gradient), for the mixed path's Schwarz assembly:
+//   H_ab = s [ (K_a . S K_b) I3 + sum_{k,m} alpha_km F_k F_m^T ],
+//   alpha_00 = C00 Ka0 Kb0 + G Ka1 Kb1,   alpha_01 = C01 Ka0 Kb1 + G Ka1 Kb0,
+//   alpha_10 = C01 Ka1 Kb0 + G Ka0 Kb1,   alpha_11 = C11 Ka1 Kb1 + G Ka0 Kb0,
+// with F_k the columns of F, K_0 = -(a + c, b + d), K_1 = (a, b), K_2 = (c, d)
+// (the rows of the shape-function gradient) and s = thickness * area. Row-major
+// h[(3a + i) * 9 + 3b + p], stored as O (double, or float for the FP32 path).
+template <class O>
+CSHD void membrane_block9(const double* x0, const double* x1, const double* x2, double a, double b, double c,
+                          double d, double s, double C00, double C11, double C01, double G, O* h) {
+  const double K[3][2] = {{-(a + c), -(b + d)}, {a, b}, {c, d}};
+  double F0[3], F1[3];
+  for (int i = 0; i < 3; i++) {
+    const double e1 = x1[i] - x0[i], e2 = x2[i] - x0[i];
+    F0[i] = a * e1 + c * e2;
+    F1[i] = b * e1 + d * e2;
+  }
+  const double E00 = 0.5 * (F0[0] * F0[0] + F0[1] * F0[1] + F0[2] * F0[2] - 1);
+  const double E11 = 0.5 * (F1[0] * F1[0] + F1[1] * F1[1] + F1[2] * F1[2] - 1);
+  const double E01 = 0.5 * (F0[0] * F1[0] + F0[1] * F1[1] + F0[2] * F1[2]);
+  const double S00 = C00 * E00 + C01 * E11, S11 = C11 * E11 + C01 * E00, S01 = 2 * G * E01;
+  for (int A = 0; A < 3; A++)
+    for (int B = 0; B < 3; B++) {
+      const double ka0 = K[A][0], ka1 = K[A][1], kb0 = K[B][0], kb1 = K[B][1];
+      const double geo = ka0 * (S00 * kb0 + S01 * kb1) + ka1 * (S01 * kb0 + S11 * kb1);
+      const double a00 = C00 * ka0 * kb0 + G * ka1 * kb1, a01 = C01 * ka0 * kb1 + G * ka1 * kb0;
+      const double a10 = C01 * ka1 * kb0 + G * ka0 * kb1, a11 = C11 * ka1 * kb1 + G * ka0 * kb0;
+      for (int i = 0; i < 3; i++)
+        for (int p = 0; p < 3; p++) {
+          const double v = (i == p ? geo : 0.0) + a00 * F0[i] * F0[p] + a01 * F0[i] * F1[p] + a10 * F1[i] * F0[p] +
+                           a11 * F1[i] * F1[p];
+          h[(3 * A + i) * 9 + 3 * B + p] = (O)(s * v);
+        }
+    }
+}
+
 }  // namespace cs

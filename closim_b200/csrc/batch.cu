@@ -17,6 +17,7 @@
 #include "batch.cuh"
 #include "contact_math.cuh"
 #include "elem.cuh"
+#include "hvp32.cuh"
 
 namespace cs {
 
@@ -180,50 +181,26 @@ __device__ void sheet_tristate(const BatchDev& b, const Range& R, const Mat<doub
   }
 }
 
-// Ap = (M/h^2 + H_membrane + H_floor) p in FP32; returns p.Ap (FP64).
+// Ap = (M/h^2 + H_membrane + H_floor) p in FP32; returns p.Ap (FP64). Each
+// vertex adds the corner share of its incident triangles' HVP directly
+// (recomputed per corner from the stored FP32 state), so no per-triangle
+// result is written and read back and no barrier splits the product.
 __device__ double sheet_hvp(const BatchDev& b, const Range& R, float C00, float C11, float C01, float G,
                             double* sm) {
-  for (int t = R.t0 + threadIdx.x; t < R.t1; t += blockDim.x) {
-    const float* T = b.tris + (size_t)t * 16;
-    const float4 t0 = *(const float4*)T, t1 = *(const float4*)(T + 4), t2 = *(const float4*)(T + 8),
-                 t3 = *(const float4*)(T + 12);
-    const float F0[3] = {t0.x, t0.y, t0.z}, F1[3] = {t0.w, t1.x, t1.y};
-    const float S00 = t1.z, S11 = t1.w, S01 = t2.x;
-    const float a = t2.y, bb = t2.z, c = t2.w, dd = t3.x, s = t3.y;
-    const uint32_t i0 = b.idx[t * 3], i1 = b.idx[t * 3 + 1], i2 = b.idx[t * 3 + 2];
-    float w1[3], w2[3];
-    for (int q = 0; q < 3; q++) {
-      const float p0 = b.p[i0 * 3 + q];
-      w1[q] = b.p[i1 * 3 + q] - p0;
-      w2[q] = b.p[i2 * 3 + q] - p0;
-    }
-    float dF0[3], dF1[3];
-    for (int q = 0; q < 3; q++) { dF0[q] = a * w1[q] + c * w2[q]; dF1[q] = bb * w1[q] + dd * w2[q]; }
-    const float dE00 = F0[0] * dF0[0] + F0[1] * dF0[1] + F0[2] * dF0[2];
-    const float dE11 = F1[0] * dF1[0] + F1[1] * dF1[1] + F1[2] * dF1[2];
-    const float dE01 = 0.5f * (dF0[0] * F1[0] + F0[0] * dF1[0] + dF0[1] * F1[1] + F0[1] * dF1[1] + dF0[2] * F1[2] +
-                               F0[2] * dF1[2]);
-    const float dS00 = C00 * dE00 + C01 * dE11, dS11 = C11 * dE11 + C01 * dE00, dS01 = 2.f * G * dE01;
-    float* o = b.e32 + (size_t)t * 9;
-    for (int q = 0; q < 3; q++) {
-      const float P0 = dF0[q] * S00 + F0[q] * dS00 + dF1[q] * S01 + F1[q] * dS01;
-      const float P1 = dF0[q] * S01 + F0[q] * dS01 + dF1[q] * S11 + F1[q] * dS11;
-      const float g1 = s * (P0 * a + P1 * bb);
-      const float g2 = s * (P0 * c + P1 * dd);
-      o[q] = -(g1 + g2);
-      o[3 + q] = g1;
-      o[6 + q] = g2;
-    }
-  }
-  __syncthreads();
   double pAp = 0;
   const float invH2 = (float)b.invH2;
   for (int v = R.v0 + threadIdx.x; v < R.v1; v += blockDim.x) {
     float sp[3] = {0.f, 0.f, 0.f};
     for (uint32_t q = b.memOff[v]; q < b.memOff[v + 1]; q++) {
-      const uint32_t rec = b.memRec[q];
-      const float* e = b.e32 + (size_t)(rec >> 2) * 9 + (rec & 3) * 3;
-      sp[0] += e[0]; sp[1] += e[1]; sp[2] += e[2];
+      const uint32_t rec = __ldg(b.memRec + q);
+      const uint32_t t = rec >> 2;
+      const int i0 = (int)__ldg(b.idx + t * 3), i1 = (int)__ldg(b.idx + t * 3 + 1), i2 = (int)__ldg(b.idx + t * 3 + 2);
+      const float3 p0 = make_float3(b.p[i0 * 3], b.p[i0 * 3 + 1], b.p[i0 * 3 + 2]);
+      const float3 p1 = make_float3(b.p[i1 * 3], b.p[i1 * 3 + 1], b.p[i1 * 3 + 2]);
+      const float3 p2 = make_float3(b.p[i2 * 3], b.p[i2 * 3 + 1], b.p[i2 * 3 + 2]);
+      float o[3];
+      tri_hvp_corner(b.tris + (size_t)t * 16, p0, p1, p2, (int)(rec & 3), C00, C11, C01, G, o);
+      sp[0] += o[0]; sp[1] += o[1]; sp[2] += o[2];
     }
     float cy = 0.f;
     if (b.act[v]) {
@@ -256,8 +233,9 @@ __device__ int sheet_pcg(const BatchDev& b, const Range& R, float C00, float C11
     b.r[i] = ri;
     b.xs[i] = 0.f;
     rr += (double)ri * ri;
-    float zi = b.diag[i] > 1e-12 ? (float)((double)ri / b.diag[i]) : ri;
-    if (pin) zi = 0.f;
+    const float di = pin ? 0.f : b.diag[i] > 1e-12 ? (float)(1.0 / b.diag[i]) : 1.f;
+    b.dinv[i] = di;
+    const float zi = ri * di;
     b.z[i] = zi;
     b.p[i] = zi;
     rz += (double)ri * zi;
@@ -282,8 +260,7 @@ __device__ int sheet_pcg(const BatchDev& b, const Range& R, float C00, float C11
       b.xs[i] = xi;
       b.r[i] = ri;
       rrn += (double)ri * ri;
-      float zi = b.diag[i] > 1e-12 ? (float)((double)ri / b.diag[i]) : ri;
-      if (pin) zi = 0.f;
+      const float zi = ri * b.dinv[i];
       b.z[i] = zi;
       rzn += (double)ri * zi;
     }

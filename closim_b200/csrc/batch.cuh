@@ -38,8 +38,8 @@ struct BatchDev {
   double* helem;               // 12HG gradient terms
   // FP32 linear solve
   float *r, *z, *p, *Ap, *xs;  // 3N
+  float* dinv;                 // 3N inverse Jacobi diagonal of the current PCG (0 on pinned dofs)
   float* tris;                 // 16M: F (6), S (3), Dm^-1 (4), thickness * area, pad
-  float* e32;                  // 9M element HVP
   // floor contact, per vertex
   uint8_t* act;                // frozen active flag
   double* lagLam;              // lagged normal force

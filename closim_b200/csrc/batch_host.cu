@@ -63,7 +63,7 @@ struct Batch {
   Buf<double> hmeta, pinPos, mat;
   Buf<uint8_t> pinned, act, lagOk;
   Buf<double> x, v, x0, yHat, g, dx, xt, diag, elem, helem, lagLam, out;
-  Buf<float> r, z, p, Ap, xs, tris, e32;
+  Buf<float> r, z, p, Ap, xs, tris, dinv;
   Buf<unsigned int> work;
   BatchDev d{};
   cs_stepper_options opts{10, 60, 10, CS_PRECOND_JACOBI, 1e-5};
@@ -182,9 +182,8 @@ struct Batch {
     for (Buf<double>* b : {&x0, &yHat, &g, &dx, &xt, &diag}) b->alloc(n3);
     elem.alloc(9 * (size_t)M);
     helem.alloc(12 * (size_t)std::max(HG, 1));
-    for (Buf<float>* b : {&r, &z, &p, &Ap, &xs}) b->alloc(n3);
+    for (Buf<float>* b : {&r, &z, &p, &Ap, &xs, &dinv}) b->alloc(n3);
     tris.alloc(16 * (size_t)M);
-    e32.alloc(9 * (size_t)M);
     act.alloc(N);
     BK(cudaMemsetAsync(act.p, 0, N, st));
     lagOk.alloc(N);
@@ -207,7 +206,7 @@ struct Batch {
     d.pinned = pinned.p; d.pinPos = pinPos.p; d.mat = mat.p;
     d.x = x.p; d.v = v.p; d.x0 = x0.p; d.yHat = yHat.p; d.g = g.p; d.dx = dx.p; d.xt = xt.p; d.diag = diag.p;
     d.elem = elem.p; d.helem = helem.p;
-    d.r = r.p; d.z = z.p; d.p = p.p; d.Ap = Ap.p; d.xs = xs.p; d.tris = tris.p; d.e32 = e32.p;
+    d.r = r.p; d.z = z.p; d.p = p.p; d.Ap = Ap.p; d.xs = xs.p; d.tris = tris.p; d.dinv = dinv.p;
     d.act = act.p; d.lagLam = lagLam.p; d.lagOk = lagOk.p;
     d.hasFloor = floorOn; d.floorY = floorY;
     d.dHat = cp.dhat; d.kappa = cp.kappa; d.dMin = cp.dmin; d.mu = cp.mu; d.eps = cp.eps;
@@ -268,13 +267,17 @@ struct Batch {
     cudaEvent_t e0, e1;
     BK(cudaEventCreate(&e0));
     BK(cudaEventCreate(&e1));
+    // Candidates: block size x number of resident blocks. Fewer blocks keep
+    // fewer sheets in flight, so their working sets can stay in L2.
     const int cands[3] = {256, 512, 1024};
+    const int fracs[3] = {1, 2, 3};
     float best = 1e30f;
-    int bestT = threads;
+    int bestT = threads, bestC = ctas;
     drop_graph();
-    for (int T : cands) {
+    for (int ci = 0; ci < 9; ci++) {
+      const int T = cands[ci / 3];
       threads = T;
-      ctas = batch_max_ctas(T);
+      ctas = std::max(1, batch_max_ctas(T) / fracs[ci % 3]);
       BK(cudaMemcpyAsync(x.p, sx.p, n3 * 8, cudaMemcpyDeviceToDevice, stream));
       BK(cudaMemcpyAsync(v.p, sv.p, n3 * 8, cudaMemcpyDeviceToDevice, stream));
       BK(cudaMemcpyAsync(lagLam.p, sl.p, (size_t)N * 8, cudaMemcpyDeviceToDevice, stream));
@@ -285,7 +288,7 @@ struct Batch {
       BK(cudaEventSynchronize(e1));
       float ms = 0;
       BK(cudaEventElapsedTime(&ms, e0, e1));
-      if (ms < best) { best = ms; bestT = T; }
+      if (ms < best) { best = ms; bestT = T; bestC = ctas; }
     }
     BK(cudaMemcpyAsync(x.p, sx.p, n3 * 8, cudaMemcpyDeviceToDevice, stream));
     BK(cudaMemcpyAsync(v.p, sv.p, n3 * 8, cudaMemcpyDeviceToDevice, stream));
@@ -295,7 +298,7 @@ struct Batch {
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     threads = bestT;
-    ctas = batch_max_ctas(bestT);
+    ctas = bestC;
     return bestT;
   }
 };
@@ -423,6 +426,14 @@ int cs_batch_set_threads(cs_batch* h, int32_t threads) {
     b->threads = threads;
     b->ctas = b->ready ? cs::batch_max_ctas(threads) : 0;
     b->drop_graph();
+  });
+}
+
+int cs_batch_launch_shape(cs_batch* h, int32_t* threads, int32_t* blocks) {
+  cs::Batch* b = B(h);
+  return bguard(b, [&] {
+    if (threads) *threads = b->threads;
+    if (blocks) *blocks = b->ctas;
   });
 }
 

@@ -55,6 +55,14 @@ __device__ __forceinline__ double seq_sum(const double* t, int n) {
   return s;
 }
 
+// cint[CI_MOVED] = 1 when some coordinate moved more than `travel` from base.
+__global__ void k_moved(const double* x, const double* base, int n3, double travel, int* cint) {
+  int bad = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += gridDim.x * blockDim.x)
+    if (!(fabs(x[i] - base[i]) <= travel)) bad = 1;
+  if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(&cint[CI_MOVED], 1);
+}
+
 __global__ void k_lerp(double* out, const double* x0, const double* x, double t, int n3) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n3) out[i] = x0[i] + t * (x[i] - x0[i]);
@@ -75,20 +83,49 @@ __device__ __forceinline__ void cand_closest(const CView& v, const double* x, co
 // Candidates of the current query: 15 per self pair, 12 per static pair.
 __device__ __forceinline__ int cand_count(const CView& v) { return 15 * (int)v.ccnt[0] + 12 * (int)v.ccnt[1]; }
 
-// Ccap bounds the candidate count from the host; slots past the device count
-// are cleared so scans and minima over Ccap see nothing there.
-__global__ void k_cand_flags(CView v, const double* x, int Ccap) {
+// Distance of every candidate (for the minima) and the order keys of the active
+// ones, appended through a warp-aggregated counter (cint[CI_NCAND]): their
+// positions are arbitrary, the radix sort that follows imposes the reference's
+// (kind, p, a, b, c, d) order, and equal keys are identical records. Ccap bounds
+// the candidate count from the host; slots past the device count get +inf.
+__global__ void k_cand_flags(CView v, const double* x, int Ccap, Key<4>* keys, uint32_t* pay) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= Ccap) return;
-  if (i >= cand_count(v)) { v.cflag[i] = 0; v.cmin[i] = INFINITY; return; }
-  const int* r = v.rec + (size_t)i * 6;
-  if (r[0] == 3) { v.cflag[i] = 0; v.cmin[i] = INFINITY; return; }
-  Closest cp;
-  cand_closest(v, x, r, cp);
-  const bool act = !(cp.dist >= v.c.dHat || cp.dist < 1e-12);
-  v.cflag[i] = act ? 1u : 0u;
-  v.cmin[i] = cp.dist;
-  if (act && r[0] == 0) atomicAdd(&v.cint[CI_NVT], 1);
+  bool act = false;
+  CandKey k{0, 0};
+  if (i < Ccap) {
+    if (i >= cand_count(v)) {
+      v.cmin[i] = INFINITY;
+    } else {
+      const int* r = v.rec + (size_t)i * 6;
+      if (r[0] == 3) {
+        v.cmin[i] = INFINITY;
+      } else {
+        Closest cp;
+        cand_closest(v, x, r, cp);
+        act = !(cp.dist >= v.c.dHat || cp.dist < 1e-12);
+        v.cmin[i] = cp.dist;
+        if (act) {
+          k = cand_key(r, v.ns, v.idBits, 0, 0);
+          if (r[0] == 0) atomicAdd(&v.cint[CI_NVT], 1);
+        }
+      }
+    }
+  }
+  const uint32_t mask = __ballot_sync(0xffffffffu, act);
+  if (!mask) return;
+  const int lane = threadIdx.x & 31;
+  const int leader = __ffs(mask) - 1;
+  uint32_t base = 0;
+  if (lane == leader) base = atomicAdd((uint32_t*)&v.cint[CI_NCAND], (uint32_t)__popc(mask));
+  base = __shfl_sync(0xffffffffu, base, leader);
+  if (act) {
+    const uint32_t pos = base + __popc(mask & ((1u << lane) - 1u));
+    keys[pos].w[0] = (uint32_t)(k.hi >> 32);
+    keys[pos].w[1] = (uint32_t)k.hi;
+    keys[pos].w[2] = (uint32_t)(k.lo >> 32);
+    keys[pos].w[3] = (uint32_t)k.lo;
+    pay[pos] = (uint32_t)i;
+  }
 }
 
 __global__ void k_floor_flags(CView v, const double* x) {
@@ -103,20 +140,6 @@ __global__ void k_floor_flags(CView v, const double* x) {
 __device__ __forceinline__ bool cand_active(const CView& v, int i) {
   const double d = v.cmin[i];
   return !(d >= v.c.dHat || d < 1e-12);
-}
-
-// The active candidates' order keys at their compacted positions (cflag holds
-// the exclusive scan of the activity flags); the payload is the candidate.
-__global__ void k_cand_keys(CView v, int C, Key<4>* keys, uint32_t* pay) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= C || !cand_active(v, i)) return;
-  const CandKey k = cand_key(v.rec + (size_t)i * 6, v.ns, v.idBits, 0, 0);
-  const uint32_t pos = v.cflag[i];
-  keys[pos].w[0] = (uint32_t)(k.hi >> 32);
-  keys[pos].w[1] = (uint32_t)k.hi;
-  keys[pos].w[2] = (uint32_t)(k.lo >> 32);
-  keys[pos].w[3] = (uint32_t)k.lo;
-  pay[pos] = (uint32_t)i;
 }
 
 // Frozen record j of the active set from the j-th candidate in key order
@@ -635,7 +658,7 @@ ContactHost::~ContactHost() {
                    (void**)&rhist, (void**)&cOff, (void**)&lagFloor, (void**)&lagFloorOk, (void**)&lk0,
                    (void**)&lk1, (void**)&lp0, (void**)&lp1, (void**)&lhist, (void**)&lval, (void**)&lsorted,
                    (void**)&probe, (void**)&diag, (void**)&cint, (void**)&minpart, (void**)&supPairs,
-                   (void**)&supSPairs})
+                   (void**)&supSPairs, (void**)&supBase})
     if (*q) cudaFree(*q);
   if (hint) cudaFreeHost(hint);
   if (hdiag) cudaFreeHost(hdiag);
@@ -686,6 +709,7 @@ void ContactHost::init(Solver& s, const cs_contact_params* prm, int floor_on, do
   dalloc(bvh.visit, nn);
   dalloc(bvh.root, 1);
   dalloc(badKey, 2);
+  dalloc(supBase, 3 * (size_t)n);
   dalloc(fflag, (size_t)n + 1);
   dalloc(cOff, (size_t)n + 1);
   dalloc(lagFloor, (size_t)n);
@@ -791,6 +815,7 @@ void ContactHost::read_ints(Solver& s) {
 void ContactHost::build_superset(Solver& s, const double* x, double padSup) {
   cudaStream_t st = s.stream;
   int64_t& lc = launch_counter();
+  CK(cudaMemcpyAsync(supBase, x, 3 * (size_t)n * 8, cudaMemcpyDeviceToDevice, st));
   bvh_build(bvh, s.d.x0, x, padSup, false, st, &lc);
   topoValid = true;
   if (supCap == 0) { supCap = std::max<size_t>(pairCap, 1024); dalloc(supPairs, supCap); }
@@ -814,9 +839,6 @@ void ContactHost::build_superset(Solver& s, const double* x, double padSup) {
     if (S > supSCap) { supSCap = S + S / 2 + 64; dalloc(supSPairs, supSCap); }
   }
   ensure_pairs((size_t)nSup, (size_t)nSupS);
-  const long Ccap = 15l * nSup + 12l * nSupS;
-  if (Ccap > INT_MAX / 8) throw CapacityError("too many contact candidates");
-  ensure_cands((size_t)Ccap);
   CK(cudaMemsetAsync(cint, 0, CI_N * sizeof(int), st));
 }
 
@@ -834,49 +856,29 @@ int ContactHost::build_candidates(Solver& s, const double* x, double pad) {
   cudaStream_t st = s.stream;
   int64_t& lc = launch_counter();
   CK(cudaMemsetAsync(cint, 0, CI_N * sizeof(int), st));
-  // Every position a step visits stays within newton_iters trust-region moves
-  // (|dx|_inf <= 2 mm each, newton.ts:163-179) of the segment x0 -> x of the
-  // step's first query, so a superset traversal with the pad widened by that
-  // distance contains every later query's pairs, which are then filtered
-  // exactly. Budgets that allow more than 2.5 cm of travel traverse per query.
-  const double travel = 0.002 * s.opts.newton_iters;
-  if (travel <= 0.025) {
-    if (!supValid) {
-      build_superset(s, x, std::max(p.dhat, p.dmin) + travel + 1e-9);
-      supValid = true;
-    }
-    // A query keeps a subset of the superset, so sizing every buffer for the
-    // superset lets the counts stay on the device (no host round trip here).
+  // Queries filter a superset of pairs built for the segment x0 -> xBase with
+  // the pad widened by kSupTravel. A query whose positions all stay within
+  // kSupTravel (max norm) of xBase has its swept boxes inside the superset's,
+  // so filtering the superset by the query's own f64 boxes gives exactly the
+  // pairs a traversal would; otherwise the superset is rebuilt around the
+  // query. The buffers sized for the superset always hold a query, and the
+  // exact counts are read back so every later kernel runs over the query only.
+  const double padSup = std::max(p.dhat, p.dmin) + kSupTravel + 1e-9;
+  if (!supValid) {
+    build_superset(s, x, padSup);
+    supValid = true;
+  }
+  for (int attempt = 0; attempt < 2; attempt++) {
+    const int n3 = 3 * n;
+    k_moved<<<std::min(1184, (n3 + 255) / 256), 256, 0, st>>>(x, supBase, n3, kSupTravel, cint);
     bvh_boxes(bvh, s.d.x0, x, pad, st, &lc);
     filter_pairs(bvh, supPairs, nSup, bvh.pairs, (uint32_t)pairCap, (uint32_t*)(cint + CI_SELF), supSPairs, nSupS,
                  pad, spairs, (uint32_t)spairCap, (uint32_t*)(cint + CI_STATIC), st, &lc);
-    const long Ccap = 15l * nSup + 12l * nSupS;
-    expand_candidates(cand, s.idx.p, sidx, bvh.pairs, nSup, spairs, ms > 0 ? nSupS : 0,
-                      (const uint32_t*)(cint + CI_SELF), st, &lc);
-    return (int)Ccap;
-  } else {
-    // The hierarchy is built once per step and refitted for every later segment:
-    // the exact pair set does not depend on the tree's shape.
-    if (!topoValid) {
-      bvh_build(bvh, s.d.x0, x, pad, false, st, &lc);
-      topoValid = true;
-    } else {
-      bvh_refit(bvh, s.d.x0, x, pad, false, st, &lc);
-    }
-    for (int attempt = 0; attempt < 2; attempt++) {
-      BvhBufs sb = bvh;
-      sb.cnt = (uint32_t*)(cint + CI_SELF);
-      sb.pairCap = (uint32_t)pairCap;
-      bvh_append_self(sb, st, &lc);
-      if (ms > 0) bvh_append_static(bvh, pad, spairs, (uint32_t)spairCap, (uint32_t*)(cint + CI_STATIC), st, &lc);
-      read_ints(s);
-      if (hint[CI_OVERFLOW]) throw CapacityError("broadphase traversal aborted (stack deeper than 64 or malformed tree)");
-      const uint32_t P = (uint32_t)hint[CI_SELF], S = ms > 0 ? (uint32_t)hint[CI_STATIC] : 0u;
-      if (P <= pairCap && S <= spairCap) break;
-      if (attempt == 1) throw CapacityError("broadphase pair count changed between identical traversals");
-      ensure_pairs(P, S);
-      CK(cudaMemsetAsync(cint + CI_SELF, 0, 2 * sizeof(int), st));
-    }
+    lc++;
+    read_ints(s);
+    if (!hint[CI_MOVED]) break;
+    if (attempt == 1) throw CapacityError("broadphase superset rebuilt around the query does not cover it");
+    build_superset(s, x, padSup);
   }
   const int P = hint[CI_SELF], S = ms > 0 ? hint[CI_STATIC] : 0;
   const long C = 15l * P + 12l * S;
@@ -891,17 +893,16 @@ void ContactHost::update_active_set(Solver& s, double* x) {
   int64_t& lc = launch_counter();
   const int C = build_candidates(s, x, p.dhat);  // an upper bound; the exact count is on the device
   CK(cudaMemsetAsync(cint + CI_NVT, 0, sizeof(int), st));
+  CK(cudaMemsetAsync(cint + CI_NCAND, 0, sizeof(int), st));
   CView v = view(*this, s);
   if (C > 0) {
-    k_cand_flags<<<cnb(C), kCT, 0, st>>>(v, x, C);
+    k_cand_flags<<<cnb(C), kCT, 0, st>>>(v, x, C, cand.k0, cand.p0);
     lc++;
   }
   k_floor_flags<<<cnb(n), kCT, 0, st>>>(v, x);
   k_min_part<<<kMinBlocks, 256, 0, st>>>(cmin, C, v.vtmp, n, minpart);
   k_active_min<<<1, 1, 0, st>>>(v, minpart);
   lc += 3;
-  if (C > 0) scan_counts(cflag, C, (uint32_t*)(cint + CI_NCAND), st, &lc);
-  else CK(cudaMemsetAsync(cint + CI_NCAND, 0, sizeof(int), st));
   scan_counts(fflag, n, (uint32_t*)(cint + CI_NFLOOR), st, &lc);
   read_ints(s);
   candidatePairs = 15.0 * (uint32_t)hint[CI_SELF] + 12.0 * (uint32_t)(ms > 0 ? hint[CI_STATIC] : 0);
@@ -913,8 +914,6 @@ void ContactHost::update_active_set(Solver& s, double* x) {
   v = view(*this, s);
   if (nCand > 0) {
     // Only the active candidates are put in the reference's (kind, p, a, b, c, d) order.
-    k_cand_keys<<<cnb(C), kCT, 0, st>>>(v, C, cand.k0, cand.p0);
-    lc++;
     const bool flip = radix_sort<4>(cand.k0, cand.p0, cand.k1, cand.p1, nCand, cand_key_bits(idBits, 0), cand.hist,
                                     st, &lc);
     k_cand_active<<<cnb(nCand), kCT, 0, st>>>(v, x, flip ? cand.p1 : cand.p0, nCand);

@@ -28,7 +28,7 @@ struct DevDiag {
 };
 
 // Device counters read back by the host (int32).
-enum CInt { CI_SELF = 0, CI_STATIC, CI_OVERFLOW, CI_NCAND, CI_NFLOOR, CI_NVT, CI_VALID, CI_FIRSTNF,
+enum CInt { CI_SELF = 0, CI_STATIC, CI_OVERFLOW, CI_NCAND, CI_NFLOOR, CI_NVT, CI_VALID, CI_FIRSTNF, CI_MOVED,
             CI_FLOORBAD, CI_N = 16 };
 
 class ContactHost {
@@ -51,9 +51,12 @@ class ContactHost {
   unsigned long long* badKey = nullptr;  // smallest failing (key, status) of a trial
   int idBits = 24;             // bits per id in the candidate order key
   bool topoValid = false;      // hierarchy built for the current step
-  // Per-step superset of candidate pairs: every query of a step lies within
-  // the trust-region hull of the step's first segment, so one traversal with a
-  // widened pad serves all of them and each query filters it exactly.
+  // Superset of candidate pairs for the queries of a step: built for the
+  // segment x0 -> xBase with the pad widened by kSupTravel; a later query whose
+  // positions stay within kSupTravel (max norm) of xBase is covered and filters
+  // it exactly, one that moved further rebuilds it around its own positions.
+  static constexpr double kSupTravel = 0.004;
+  double* supBase = nullptr;   // 3n positions the superset was built around
   int2* supPairs = nullptr;
   int2* supSPairs = nullptr;
   size_t supCap = 0, supSCap = 0;

@@ -10,6 +10,7 @@
 // Schwarz preconditioner (src/solver/schwarz.ts) is assembled and factored in
 // FP64 and applied as an FP32 dense inverse per domain, one warp per domain.
 // Gradient, energies, contact and CCD stay on the FP64 kernels.
+#include "adjoint_math.cuh"
 #include "contact.cuh"
 #include "mixed.cuh"
 
@@ -55,10 +56,8 @@ __global__ void __launch_bounds__(kThreads) k_mx_h9(Dev d, MixBufs mb) {
   double x0[3], x1[3], x2[3];
   ld3(d.x, d.idx[t * 3], x0); ld3(d.x, d.idx[t * 3 + 1], x1); ld3(d.x, d.idx[t * 3 + 2], x2);
   const float4 iv = d.inv[t];
-  double h[81];
-  tri_hessian9_rows<double>(x0, x1, x2, iv.x, iv.y, iv.z, iv.w, d.area[t], d.mat, 0, 9, h);
-  float* o = mb.h9 + (size_t)t * 81;
-  for (int k = 0; k < 81; k++) o[k] = (float)h[k];
+  membrane_block9<float>(x0, x1, x2, iv.x, iv.y, iv.z, iv.w, d.mat.thickness * (double)d.area[t], d.mat.C00,
+                         d.mat.C11, d.mat.C01, d.mat.G, mb.h9 + (size_t)t * 81);
 }
 
 // Schwarz factor: assemble (FP64 sums of the stored blocks + Jacobi diagonal),

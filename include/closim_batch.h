@@ -14,8 +14,10 @@
  * from a work list ordered largest first and runs that sheet's whole implicit
  * step with block barriers only. cs_batch_step with steps > 1 captures the
  * sequence once into a CUDA graph and replays it. cs_batch_autotune times the
- * candidate block sizes (256, 512, 1024 threads) on the batch's own state
- * (restored afterwards) and keeps the fastest.
+ * candidate launch shapes (256, 512 or 1024 threads per block, all resident
+ * blocks or a half or a third of them) on the batch's own state (restored
+ * afterwards) and keeps the fastest: fewer blocks keep fewer sheets in flight,
+ * whose working sets then stay in L2.
  */
 #ifndef CLOSIM_BATCH_H
 #define CLOSIM_BATCH_H
@@ -51,6 +53,8 @@ int cs_batch_get_velocities(cs_batch* b, double* out);
 int cs_batch_stats(cs_batch* b, double* out);  /* CS_BATCH_STATS doubles per sheet */
 int cs_batch_autotune(cs_batch* b, double dt, int32_t* threads);
 int cs_batch_set_threads(cs_batch* b, int32_t threads);
+/* The launch shape in use: threads per block and resident blocks. */
+int cs_batch_launch_shape(cs_batch* b, int32_t* threads, int32_t* blocks);
 void* cs_batch_stream(cs_batch* b);
 
 #ifdef __cplusplus

@@ -29,4 +29,7 @@ double hc_bend_grad(const double* q, const double* meta, double k, double* g) {
 void hc_bend_hvp(const double* q, const double* v, const double* meta, double k, double* o) {
   cs::bend_hvp(q, v, meta[0], meta[1], meta[2], k, o);
 }
+void hc_membrane_block9(const double* x9, const double* inv4, double s, const double* C4, double* h) {
+  cs::membrane_block9<double>(x9, x9 + 3, x9 + 6, inv4[0], inv4[1], inv4[2], inv4[3], s, C4[0], C4[1], C4[2], C4[3], h);
+}
 }

@@ -137,3 +137,25 @@ def test_bending_gradient_and_hvp(hc):
     assert worst_e < 1e-7, worst_e
     assert worst_g < 1e-4, worst_g
     assert worst_h < 1e-6, worst_h
+
+
+def test_membrane_block9_matches_oracle(hc):
+    """The mixed path's closed-form 9x9 membrane block against the oracle's
+    restatement of membrane-blocks.ts:21-98 (same Hessian, different algebra)."""
+    p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+    hc.hc_membrane_block9.restype = None
+    hc.hc_membrane_block9.argtypes = [p, p, C.c_double, p, p]
+    rng = np.random.default_rng(21)
+    worst = 0.0
+    for trial in range(40):
+        x9 = np.array([0, 0, 0, 0.02, 0, 0, 0, 0, 0.02]) + rng.uniform(-4e-3, 4e-3, 9)
+        inv = np.array([50.0, 0.0, 0.0, 50.0]) + rng.uniform(-5, 5, 4)
+        area = 2e-4 * (1 + 0.1 * rng.uniform())
+        mat = dict(arealDensity=0.2, thickness=1.0, C00=rng.uniform(2e3, 1e4), C11=rng.uniform(2e3, 1e4),
+                   C01=rng.uniform(0, 500), G=rng.uniform(5e2, 2e3), bendWarp=1e-4, bendWeft=1e-4, damping=0)
+        ref = O.tri_hessian9(x9, inv, np.float32(area), mat)
+        h = np.zeros(81)
+        hc.hc_membrane_block9(x9, inv, mat["thickness"] * float(np.float32(area)),
+                              np.array([mat["C00"], mat["C11"], mat["C01"], mat["G"]]), h)
+        worst = max(worst, np.max(np.abs(h.reshape(9, 9) - ref)) / np.max(np.abs(ref)))
+    assert worst < 1e-12, worst
