@@ -206,6 +206,8 @@ def run_precision(cfg, precision, local, args, ext_stream_cb, flush, sampler=Non
     if sampler:
         sampler.start()
     launches0 = solver.kernelLaunches()
+    if args.profiler_range:
+        torch.cuda.profiler.start()  # ncu --profile-from-start off captures the timed steps only
     solver.profile(True)
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
@@ -223,6 +225,8 @@ def run_precision(cfg, precision, local, args, ext_stream_cb, flush, sampler=Non
         total += ev0.elapsed_time(ev1)
         step_bytes += step_algorithmic_bytes(solver.lastStats, mesh, precision, cfg)
     torch.cuda.synchronize()
+    if args.profiler_range:
+        torch.cuda.profiler.stop()
     if prof_out is not None:
         prof_out.update(solver.profileRead())
     solver.profile(False)
@@ -388,6 +392,8 @@ def main():
     ap.add_argument("--small", action="store_true", help="32x32 floor drape (for profiler captures)")
     ap.add_argument("--precision", default="both", choices=["both", "fp64", "mixed"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profiler-range", action="store_true",
+                    help="mark the timed steps for ncu --profile-from-start off")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 

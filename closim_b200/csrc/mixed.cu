@@ -47,6 +47,16 @@ __global__ void __launch_bounds__(kThreads) k_mx_tristate(Dev d, MixBufs mb) {
   o[9] = iv.x; o[10] = iv.y; o[11] = iv.z; o[12] = iv.w;
   o[13] = (float)(m.thickness * (double)d.area[t]);
   o[14] = 0.f; o[15] = 0.f;
+  if (mb.vrec) {
+    const float4 r0 = make_float4(o[0], o[1], o[2], o[3]), r1 = make_float4(o[4], o[5], o[6], o[7]),
+                 r2 = make_float4(o[8], o[9], o[10], o[11]), r3 = make_float4(o[12], o[13], 0.f, 0.f);
+    for (int c = 0; c < 3; c++) {
+      float4* q = mb.vrec + (size_t)mb.triSlot[t * 3 + c] * 5;
+      q[0] = r0; q[1] = r1; q[2] = r2; q[3] = r3;
+      q[4] = make_float4(__int_as_float((int)d.idx[t * 3]), __int_as_float((int)d.idx[t * 3 + 1]),
+                         __int_as_float((int)d.idx[t * 3 + 2]), __int_as_float(c));
+    }
+  }
 }
 
 // Full 9x9 membrane block per triangle (FP64 closed form), stored FP32.

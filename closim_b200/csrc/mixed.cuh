@@ -10,6 +10,12 @@ struct MixBufs {
   float* tris;                 // 16m per-triangle F, S, Dm^-1, thickness * area
   float* h9;                   // 81m 9x9 blocks (Schwarz assembly)
   float* Linv;                 // D x 576 dense inverses
+  // Vertex-major copies of the triangle state for the one-cluster PCG: record q
+  // of the membrane incidence (tri << 2 | corner) holds that triangle's 16-float
+  // state, its three vertex ids and the corner (5 float4, 80 B), so a vertex
+  // reads its incident triangles contiguously with no index indirection.
+  float4* vrec;                // 5 x 3m (null when unused)
+  const uint32_t* triSlot;     // 3m: incidence record of (triangle, corner)
   float C00, C11, C01, G;
 };
 

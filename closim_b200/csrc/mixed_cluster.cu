@@ -118,12 +118,16 @@ __device__ __forceinline__ void cl_domain(const Dev& d, const MixBufs& mb, const
     rv = ri;
     rr += (double)ri * ri;
   }
-  const float* Li = mb.Linv + (size_t)dom * 576 + lane * 24;
+  // row `lane` of the 24x24 inverse: 96 bytes, six 16-byte loads
+  const float4* Li = reinterpret_cast<const float4*>(mb.Linv + (size_t)dom * 576) + lane * 6;
   float z = 0.f;
 #pragma unroll
-  for (int j = 0; j < 24; j++) {
-    const float rj = __shfl_sync(0xffffffffu, rv, j);
-    if (lane < dw) z = fmaf(__ldg(Li + j), rj, z);
+  for (int j4 = 0; j4 < 6; j4++) {
+    const float4 l = lane < dw ? __ldg(Li + j4) : make_float4(0.f, 0.f, 0.f, 0.f);
+    z = fmaf(l.x, __shfl_sync(0xffffffffu, rv, 4 * j4), z);
+    z = fmaf(l.y, __shfl_sync(0xffffffffu, rv, 4 * j4 + 1), z);
+    z = fmaf(l.z, __shfl_sync(0xffffffffu, rv, 4 * j4 + 2), z);
+    z = fmaf(l.w, __shfl_sync(0xffffffffu, rv, 4 * j4 + 3), z);
   }
   if (lane < dw) {
     if (pin) z = 0.f;
@@ -214,14 +218,17 @@ __global__ void __launch_bounds__(kClT, 1) k_mx_pcg_cluster(ClArgs A) {
     for (int v = tid; v < d.n; v += nth) {
       const float3 pv = ld_p(mb.z, pc, beta, first, v);
       float sp[3] = {0.f, 0.f, 0.f};
-      for (uint32_t q = d.memOff[v]; q < d.memOff[v + 1]; q++) {
-        const uint32_t rec = __ldg(d.memRec + q);
-        const uint32_t t = rec >> 2;
-        const int i0 = (int)__ldg(d.idx + t * 3), i1 = (int)__ldg(d.idx + t * 3 + 1), i2 = (int)__ldg(d.idx + t * 3 + 2);
-        const float3 p0 = ld_p(mb.z, pc, beta, first, i0), p1 = ld_p(mb.z, pc, beta, first, i1),
-                     p2 = ld_p(mb.z, pc, beta, first, i2);
+      const uint32_t q0 = d.memOff[v], q1 = d.memOff[v + 1];
+      for (uint32_t q = q0; q < q1; q++) {
+        // record q = (triangle << 2 | corner): state + vertex ids, read contiguously
+        const float4* R = mb.vrec + (size_t)q * 5;
+        const float4 ids = __ldg(R + 4);
+        const int corner = __float_as_int(ids.w);
+        const float3 p0 = ld_p(mb.z, pc, beta, first, __float_as_int(ids.x));
+        const float3 p1 = ld_p(mb.z, pc, beta, first, __float_as_int(ids.y));
+        const float3 p2 = ld_p(mb.z, pc, beta, first, __float_as_int(ids.z));
         float o[3];
-        tri_hvp_corner(mb.tris + (size_t)t * 16, p0, p1, p2, (int)(rec & 3), C00, C11, C01, G, o);
+        tri_hvp_corner(reinterpret_cast<const float*>(R), p0, p1, p2, corner, C00, C11, C01, G, o);
         sp[0] += o[0]; sp[1] += o[1]; sp[2] += o[2];
       }
       double ch[3] = {0, 0, 0};

@@ -104,6 +104,8 @@ class Solver {
   int pcgBlocks = 1;
   // mixed-precision path
   DBuf<float> fr, fz, fp, fAp, fx, felem, ftris, fh9, fLinv, fp2;
+  DBuf<float4> fvrec;
+  DBuf<uint32_t> triSlot;
   MixBufs mb{};
   int mxBlocks = 1;
   int mxCluster = 0;  // CTAs of the one-cluster PCG (0: grid-wide cooperative PCG)
@@ -290,7 +292,18 @@ class Solver {
       const char* env = std::getenv("CLOSIM_MX_PCG");
       const bool wantCluster = env ? std::string(env) == "cluster" : mesh.n <= 20000;
       mxCluster = wantCluster && mesh.maxDomain <= 8 ? mx_cluster_size() : 0;
-      if (mxCluster > 0) fp2.alloc(n3);
+      if (mxCluster > 0) {
+        fp2.alloc(n3);
+        std::vector<uint32_t> slot(3 * (size_t)cm.m);
+        for (size_t q = 0; q < mesh.memRec.size(); q++) {
+          const uint32_t rec = mesh.memRec[q];
+          slot[(rec >> 2) * 3 + (rec & 3)] = (uint32_t)q;
+        }
+        triSlot.upload(slot.data(), slot.size(), stream);
+        fvrec.alloc(5 * 3 * (size_t)cm.m);
+        mb.vrec = fvrec.p;
+        mb.triSlot = triSlot.p;
+      }
     }
     upload_pins();
     contact.reset();
