@@ -30,6 +30,23 @@ sys.path.insert(0, ROOT)
 HBM_FALLBACK_GBS = 6650.0
 
 
+def max_over_ranks(values, device, world):
+    """Max of each timing over all ranks (the job is as slow as its slowest
+    replica); identity when world == 1."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor(list(values), dtype=torch.float64, device=device)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.tolist()
+
+
+def replica_throughput(world, steps, ms):
+    """Whole-job steps/s of `world` independent replicas that each ran `steps`
+    steps, timed as the slowest rank's `ms`."""
+    return world * steps / (ms / 1000.0)
+
+
 def measured_peak():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -304,13 +321,10 @@ def run_batch(args, world, rank, local):
         so.close()
     total_m = int(sum(len(c["idx"]) // 3 for c in sheets))
     single_est_ms = single_ms * total_m / max(single_m, 1)
-    t = torch.tensor([total, graph_ms], dtype=torch.float64, device=f"cuda:{local}")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    total, graph_ms = t.tolist()
+    total, graph_ms = max_over_ranks([total, graph_ms], f"cuda:{local}", world)
     if rank == 0:
         S = len(sheets)
-        line = {"metric": "sim steps/s", "value": world * args.steps / (total / 1000.0), "unit": "steps/s",
+        line = {"metric": "sim steps/s", "value": replica_throughput(world, args.steps, total), "unit": "steps/s",
                 "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": total / args.steps,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
                 "data": "synthetic (seeded)", "impl": "cuda",
@@ -460,13 +474,11 @@ def main():
     d2h = 2 * n * 3 * 8
 
     times = [res[headline]["ms"], e2e_ms, res.get("fp64", {}).get("ms", 0.0)]
-    t = torch.tensor(times, dtype=torch.float64, device=f"cuda:{local}")
+    total_ms, e2e_ms, fp64_ms = max_over_ranks(times, f"cuda:{local}", world)
     if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
         dist.barrier()
-    total_ms, e2e_ms, fp64_ms = t.tolist()
-    value = world * args.steps / (total_ms / 1000.0)
-    e2e_value = world * e_steps / (e2e_ms / 1000.0)
+    value = replica_throughput(world, args.steps, total_ms)
+    e2e_value = replica_throughput(world, e_steps, e2e_ms)
 
     if rank == 0:
         peak, peak_kind = measured_peak()

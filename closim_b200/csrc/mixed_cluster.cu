@@ -64,7 +64,34 @@ __device__ __forceinline__ void cl_totals(cg::cluster_group& cl, double* red, do
   __syncthreads();
 #pragma unroll
   for (int k = 0; k < K; k++) out[k] = bc[k];
+  // no trailing barrier: consecutive calls alternate between two bc banks
+}
+
+// This CTA's sums of K per-thread values into out[0..K) (thread 0 writes):
+// warp shuffle trees, one block barrier, warp 0 adds the warp partials in a
+// fixed order. wsm holds K x 32 doubles; it is rewritten only after the next
+// cluster barrier, by which time warp 0 has read it.
+template <int K>
+__device__ __forceinline__ void block_partials(const double* v, double* out, double* wsm) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < K; k++) {
+    double w = v[k];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) w += __shfl_down_sync(0xffffffffu, w, o);
+    if (lane == 0) wsm[k * 32 + warp] = w;
+  }
   __syncthreads();
+  if (warp == 0) {
+    const int nw = blockDim.x >> 5;
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+      double t = lane < nw ? wsm[k * 32 + lane] : 0.0;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+      if (lane == 0) out[k] = t;
+    }
+  }
 }
 
 __device__ __forceinline__ float3 ld_p(const float* z, const float* pc, float beta, bool first, int v) {
@@ -163,8 +190,10 @@ __global__ void __launch_bounds__(kClT, 1) k_mx_pcg_cluster(ClArgs A) {
   // Partials alternate between two banks: a bank is rewritten only after the
   // cluster barrier that follows every CTA's read of it.
   __shared__ double red[2][4];
-  __shared__ double bc[4];
+  __shared__ double bcs[2][4];   // broadcast banks of cl_totals, alternating per call
+  __shared__ double wsm[3 * 32];
   int round = 0;
+#define BC (bcs[round & 1])
   const Dev& d = A.d;
   const MixBufs& mb = A.mb;
   const int n3 = d.n * 3;
@@ -194,12 +223,12 @@ __global__ void __launch_bounds__(kClT, 1) k_mx_pcg_cluster(ClArgs A) {
     }
   }
   {
-    const double s0 = block_sum(bb, sm), s1 = block_sum(rr, sm), s2 = block_sum(rz, sm);
-    if (threadIdx.x == 0) { red[round & 1][0] = s0; red[round & 1][1] = s1; red[round & 1][2] = s2; }
+    const double v3[3] = {bb, rr, rz};
+    block_partials<3>(v3, red[round & 1], wsm);
   }
   cl.sync();
   double tot[3];
-  cl_totals<3>(cl, red[round & 1], tot, bc);
+  cl_totals<3>(cl, red[round & 1], tot, BC);
   round++;
   double rzCur = tot[2];
   const double bNorm = sqrt(tot[0]);
@@ -255,12 +284,9 @@ __global__ void __launch_bounds__(kClT, 1) k_mx_pcg_cluster(ClArgs A) {
         pAp += (double)pvv[q] * ap;
       }
     }
-    {
-      const double s = block_sum(pAp, sm);
-      if (threadIdx.x == 0) red[round & 1][0] = s;
-    }
+    block_partials<1>(&pAp, red[round & 1], wsm);
     cl.sync();
-    cl_totals<1>(cl, red[round & 1], tot, bc);
+    cl_totals<1>(cl, red[round & 1], tot, BC);
     round++;
     const double pApT = tot[0];
     if (!(pApT > 1e-30)) { iters = k; done = true; break; }
@@ -274,12 +300,12 @@ __global__ void __launch_bounds__(kClT, 1) k_mx_pcg_cluster(ClArgs A) {
       for (int dom = gwarp; dom < d.D; dom += nwarps) cl_domain(d, mb, pn, alpha, false, dom, rr, rz);
     }
     {
-      const double s0 = block_sum(rr, sm), s1 = block_sum(rz, sm);
-      if (threadIdx.x == 0) { red[round & 1][0] = s0; red[round & 1][1] = s1; }
+      const double v2[2] = {rr, rz};
+      block_partials<2>(v2, red[round & 1], wsm);
     }
     cl.sync();
     double t2[2];
-    cl_totals<2>(cl, red[round & 1], t2, bc);
+    cl_totals<2>(cl, red[round & 1], t2, BC);
     round++;
     residual = sqrt(t2[0]);
     if (residual < absTol) { iters = k + 1; done = true; break; }
@@ -299,13 +325,10 @@ __global__ void __launch_bounds__(kClT, 1) k_mx_pcg_cluster(ClArgs A) {
     d.dx[i] = di;
     gt += d.g[i] * di;
   }
-  {
-    const double s = block_sum(gt, sm);
-    if (threadIdx.x == 0) red[round & 1][0] = s;
-  }
+  block_partials<1>(&gt, red[round & 1], wsm);
   cl.sync();
   double t1[1];
-  cl_totals<1>(cl, red[round & 1], t1, bc);
+  cl_totals<1>(cl, red[round & 1], t1, BC);
   round++;
   double gtdx = t1[0];
   bool fallback = false;
@@ -317,10 +340,9 @@ __global__ void __launch_bounds__(kClT, 1) k_mx_pcg_cluster(ClArgs A) {
       d.dx[i] = di;
       gt += d.g[i] * di;
     }
-    const double s = block_sum(gt, sm);
-    if (threadIdx.x == 0) red[round & 1][0] = s;
+    block_partials<1>(&gt, red[round & 1], wsm);
     cl.sync();
-    cl_totals<1>(cl, red[round & 1], t1, bc);
+    cl_totals<1>(cl, red[round & 1], t1, BC);
     round++;
     gtdx = t1[0];
   }
@@ -333,12 +355,12 @@ __global__ void __launch_bounds__(kClT, 1) k_mx_pcg_cluster(ClArgs A) {
     if (threadIdx.x == 0) {
       double r = 0;
       for (int q = 0; q < nrank; q++) r = fmax(r, *cl.map_shared_rank(&red[round & 1][0], q));
-      bc[0] = r;
+      BC[0] = r;
     }
     __syncthreads();
-    round++;
   }
-  const double maxDx = bc[0];
+  const double maxDx = BC[0];
+  round++;
   if (maxDx > 0.002) {
     const double s = 0.002 / maxDx;
     for (int i = tid; i < n3; i += nth) d.dx[i] *= s;
@@ -352,6 +374,7 @@ __global__ void __launch_bounds__(kClT, 1) k_mx_pcg_cluster(ClArgs A) {
     d.scal[S_MAXDX] = maxDx;
   }
   cl.sync();  // no CTA leaves while a peer may still read its shared memory
+#undef BC
 }
 
 // Largest cluster (16, then 8, 4, 2, 1 CTAs) the device can co-schedule for
