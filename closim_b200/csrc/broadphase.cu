@@ -507,54 +507,4 @@ void bvh_append_static(BvhBufs& b, double pad, int2* out, uint32_t cap, uint32_t
   *launches += 1;
 }
 
-// ---- candidates (contact-assembly.ts:87-121, self-collision.ts:23-41) -----------
-__device__ __forceinline__ void put_cand(int* rec, int slot, int kind, int p, int a, int bb, int c, int d) {
-  int* r = rec + (size_t)slot * 6;
-  r[0] = kind; r[1] = p; r[2] = a; r[3] = bb; r[4] = c; r[5] = d;
-}
-
-__global__ void k_expand_self(CandBufs c, const uint32_t* idx, const int2* pairs, const uint32_t* dcnt) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= (int)dcnt[0]) return;
-  const int tA = pairs[i].x, tB = pairs[i].y;
-  const int A[3] = {(int)idx[tA * 3], (int)idx[tA * 3 + 1], (int)idx[tA * 3 + 2]};
-  const int B[3] = {(int)idx[tB * 3], (int)idx[tB * 3 + 1], (int)idx[tB * 3 + 2]};
-  int slot = i * 15;
-  for (int k = 0; k < 3; k++) put_cand(c.rec, slot++, 0, A[k], B[0], B[1], B[2], -1);
-  for (int k = 0; k < 3; k++) put_cand(c.rec, slot++, 0, B[k], A[0], A[1], A[2], -1);
-  const int TE[3][2] = {{0, 1}, {1, 2}, {2, 0}};
-  for (int ea = 0; ea < 3; ea++)
-    for (int eb = 0; eb < 3; eb++) {
-      const int a = A[TE[ea][0]], bb = A[TE[ea][1]], cc = B[TE[eb][0]], d = B[TE[eb][1]];
-      if (a == cc || a == d || bb == cc || bb == d) put_cand(c.rec, slot++, 3, 0, 0, 0, 0, 0);
-      else put_cand(c.rec, slot++, 1, -1, a, bb, cc, d);
-    }
-}
-
-__global__ void k_expand_static(CandBufs c, const uint32_t* idx, const uint32_t* sidx, const int2* pairs,
-                                const uint32_t* dcnt) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= (int)dcnt[1]) return;
-  const int base = 15 * (int)dcnt[0];
-  const int ct = pairs[i].x, st = pairs[i].y;
-  const int A[3] = {(int)idx[ct * 3], (int)idx[ct * 3 + 1], (int)idx[ct * 3 + 2]};
-  const int B[3] = {(int)sidx[st * 3], (int)sidx[st * 3 + 1], (int)sidx[st * 3 + 2]};
-  int slot = base + i * 12;
-  for (int k = 0; k < 3; k++) put_cand(c.rec, slot++, 0, A[k], -(B[0] + 2), -(B[1] + 2), -(B[2] + 2), -2);
-  const int E[3][2] = {{0, 1}, {1, 2}, {2, 0}};
-  for (int e = 0; e < 3; e++)
-    for (int f = 0; f < 3; f++)
-      put_cand(c.rec, slot++, 1, -1, A[E[e][0]], A[E[e][1]], -(B[E[f][0]] + 2), -(B[E[f][1]] + 2));
-}
-
-void expand_candidates(CandBufs& c, const uint32_t* idx, const uint32_t* sidx, const int2* selfPairs, int selfCap,
-                       const int2* staticPairs, int staticCap, const uint32_t* dcnt, cudaStream_t s,
-                       int64_t* launches) {
-  if (selfCap) { k_expand_self<<<nb(selfCap), kBT, 0, s>>>(c, idx, selfPairs, dcnt); *launches += 1; }
-  if (staticCap) {
-    k_expand_static<<<nb(staticCap), kBT, 0, s>>>(c, idx, sidx, staticPairs, dcnt);
-    *launches += 1;
-  }
-}
-
 }  // namespace cs

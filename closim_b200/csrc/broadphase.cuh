@@ -74,21 +74,14 @@ void filter_pairs(const BvhBufs& b, const int2* sup, int nsup, int2* out, uint32
                   const int2* ssup, int nssup, double pad, int2* sout, uint32_t scap, uint32_t* scnt, cudaStream_t s,
                   int64_t* launches);
 
-// Candidates: 15 per self pair (6 VT + 9 EE; void slots get kind 3), 12 per
-// static pair (3 VT + 9 EE). rec holds 6 ints per candidate in expansion order.
+// Sort buffers for the order keys of candidates (15 per self pair, 12 per
+// static pair; the records are decoded from the pairs where they are used).
 struct CandBufs {
   int cap = 0;
-  int* rec = nullptr;       // 6 ints per candidate (kind, p, a, b, c, d)
   Key<4>* k0 = nullptr; Key<4>* k1 = nullptr;
   uint32_t* p0 = nullptr; uint32_t* p1 = nullptr;
   uint32_t* hist = nullptr;
 };
-// The exact pair counts stay on the device (dcnt[0] self, dcnt[1] static);
-// selfCap / staticCap bound them from the host. Static candidates start at 15
-// dcnt[0].
-void expand_candidates(CandBufs& c, const uint32_t* idx, const uint32_t* sidx, const int2* selfPairs, int selfCap,
-                       const int2* staticPairs, int staticCap, const uint32_t* dcnt, cudaStream_t s,
-                       int64_t* launches);
 
 // Order key of a candidate (contact-assembly.ts:118: kind, p, a, b, c, d),
 // packed as a 128-bit integer (w[0] most significant) with `bits` bits per id;

@@ -25,16 +25,21 @@ struct CView {  // kernel view of the contact host buffers
   Contact c;
   int nCand, nFloor, n;
   const double* x0;  // xStep
-  const int* rec;              // candidates in expansion order (6 ints each)
+  // Candidate pairs of the current query (counts in ccnt): self triangle
+  // pairs and (cloth triangle, static triangle) pairs, and the index buffers.
+  const int2* selfPairs;
+  const int2* staticPairs;
+  const uint32_t* idx;
+  const uint32_t* sidx;
   int ns, idBits;              // static vertex count, bits per id in the order key
   unsigned long long* badKey;  // [hi, lo] smallest (key, status) of a failing CCD candidate
+  // Minima as order-preserving 64-bit images of doubles (ord_of):
+  // [0] trial distance, [1] trial TOI, [2] active-set distance.
+  unsigned long long* omin;
+  int* badList;                // indices of failing trial candidates (first kBadCap)
   const uint32_t* ccnt;        // [self pairs, static pairs] of the current query (device)
   uint32_t* cflag;
   uint32_t* fflag;
-  double* cmin;
-  double* ctoi;
-  double* vtmp;
-  double* vtmp2;
   Frozen* active;
   double* dd;
   double* cg;
@@ -53,6 +58,48 @@ __device__ __forceinline__ double seq_sum(const double* t, int n) {
   double s = 0.0;
   for (int i = 0; i < n; i++) s = s + t[i];
   return s;
+}
+
+// Order-preserving map of a non-NaN double onto an unsigned 64-bit integer
+// (negative values bit-flipped, non-negative ones with the sign bit set), so
+// that an atomicMin on the image is a minimum of the doubles.
+__device__ __forceinline__ unsigned long long ord_of(double d) {
+  const unsigned long long b = (unsigned long long)__double_as_longlong(d);
+  return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+}
+__device__ __forceinline__ double dbl_of(unsigned long long o) {
+  return __longlong_as_double((long long)((o >> 63) ? (o & 0x7fffffffffffffffull) : ~o));
+}
+constexpr unsigned long long kOrdInf = 0xfff0000000000000ull;  // ord_of(+inf)
+
+// Block minima of two per-thread values (NaN-free: callers keep a value only
+// when it is below the running +inf start, the reference's `if (d < m) m = d`)
+// folded into dst0 / dst1 with one atomicMin each. Every thread of the block calls it.
+__device__ __forceinline__ void block_min_into(double a, double b, unsigned long long* dst0,
+                                               unsigned long long* dst1) {
+  __shared__ double sa[32], sb[32];
+  for (int o = 16; o > 0; o >>= 1) {
+    const double ta = __shfl_down_sync(0xffffffffu, a, o), tb = __shfl_down_sync(0xffffffffu, b, o);
+    if (ta < a) a = ta;
+    if (tb < b) b = tb;
+  }
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) { sa[w] = a; sb[w] = b; }
+  __syncthreads();
+  if (w == 0) {
+    const int nw = (int)(blockDim.x >> 5);
+    a = l < nw ? sa[l] : INFINITY;
+    b = l < nw ? sb[l] : INFINITY;
+    for (int o = 16; o > 0; o >>= 1) {
+      const double ta = __shfl_down_sync(0xffffffffu, a, o), tb = __shfl_down_sync(0xffffffffu, b, o);
+      if (ta < a) a = ta;
+      if (tb < b) b = tb;
+    }
+    if (l == 0) {
+      if (a < INFINITY) atomicMin(dst0, ord_of(a));
+      if (dst1 && b < INFINITY) atomicMin(dst1, ord_of(b));
+    }
+  }
 }
 
 // cint[CI_MOVED] = 1 when some coordinate moved more than `travel` from base.
@@ -83,6 +130,51 @@ __device__ __forceinline__ void cand_closest(const CView& v, const double* x, co
 // Candidates of the current query: 15 per self pair, 12 per static pair.
 __device__ __forceinline__ int cand_count(const CView& v) { return 15 * (int)v.ccnt[0] + 12 * (int)v.ccnt[1]; }
 
+// Record (kind, p, a, b, c, d) of candidate i, decoded from its pair
+// (expandTriPair, contact-assembly.ts:91-115). Candidates are slot-major: slot s
+// of self pair k is s * P + k, slot s of static pair k is 15 P + s * Q + k (P self
+// pairs, Q static pairs), so a warp evaluates one kind for 32 pairs. Self slots
+// 0-2: VT of A's vertices against B, 3-5: VT of B's vertices against A, 6-14:
+// EE of edge ea of A against edge eb of B (void, kind 3, when the edges share a
+// vertex). Static slots 0-2: VT of A's vertices against the static triangle,
+// 3-11: EE. Static ids are stored as -(id + 2). The order of the records is
+// free: every consumer orders them by key.
+__device__ __forceinline__ void cand_rec(const CView& v, int i, int* r) {
+  const int P = (int)v.ccnt[0];
+  const int e0[3] = {0, 1, 2}, e1[3] = {1, 2, 0};
+  if (i < 15 * P) {
+    const int slot = i / P, k = i - slot * P;
+    const int2 pr = v.selfPairs[k];
+    const int A[3] = {(int)v.idx[pr.x * 3], (int)v.idx[pr.x * 3 + 1], (int)v.idx[pr.x * 3 + 2]};
+    const int B[3] = {(int)v.idx[pr.y * 3], (int)v.idx[pr.y * 3 + 1], (int)v.idx[pr.y * 3 + 2]};
+    if (slot < 3) {
+      r[0] = 0; r[1] = A[slot]; r[2] = B[0]; r[3] = B[1]; r[4] = B[2]; r[5] = -1;
+    } else if (slot < 6) {
+      r[0] = 0; r[1] = B[slot - 3]; r[2] = A[0]; r[3] = A[1]; r[4] = A[2]; r[5] = -1;
+    } else {
+      const int ea = (slot - 6) / 3, eb = (slot - 6) - 3 * ea;
+      const int a = A[e0[ea]], b = A[e1[ea]], c = B[e0[eb]], d = B[e1[eb]];
+      if (a == c || a == d || b == c || b == d) {
+        r[0] = 3; r[1] = r[2] = r[3] = r[4] = r[5] = 0;
+      } else {
+        r[0] = 1; r[1] = -1; r[2] = a; r[3] = b; r[4] = c; r[5] = d;
+      }
+    }
+    return;
+  }
+  const int Q = (int)v.ccnt[1];
+  const int j = i - 15 * P, slot = j / Q, k = j - slot * Q;
+  const int2 pr = v.staticPairs[k];
+  const int A[3] = {(int)v.idx[pr.x * 3], (int)v.idx[pr.x * 3 + 1], (int)v.idx[pr.x * 3 + 2]};
+  const int B[3] = {-((int)v.sidx[pr.y * 3] + 2), -((int)v.sidx[pr.y * 3 + 1] + 2), -((int)v.sidx[pr.y * 3 + 2] + 2)};
+  if (slot < 3) {
+    r[0] = 0; r[1] = A[slot]; r[2] = B[0]; r[3] = B[1]; r[4] = B[2]; r[5] = -2;
+  } else {
+    const int ea = (slot - 3) / 3, eb = (slot - 3) - 3 * ea;
+    r[0] = 1; r[1] = -1; r[2] = A[e0[ea]]; r[3] = A[e1[ea]]; r[4] = B[e0[eb]]; r[5] = B[e1[eb]];
+  }
+}
+
 // Distance of every candidate (for the minima) and the order keys of the active
 // ones, appended through a warp-aggregated counter (cint[CI_NCAND]): their
 // positions are arbitrary, the radix sort that follows imposes the reference's
@@ -92,25 +184,22 @@ __global__ void k_cand_flags(CView v, const double* x, int Ccap, Key<4>* keys, u
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   bool act = false;
   CandKey k{0, 0};
-  if (i < Ccap) {
-    if (i >= cand_count(v)) {
-      v.cmin[i] = INFINITY;
-    } else {
-      const int* r = v.rec + (size_t)i * 6;
-      if (r[0] == 3) {
-        v.cmin[i] = INFINITY;
-      } else {
-        Closest cp;
-        cand_closest(v, x, r, cp);
-        act = !(cp.dist >= v.c.dHat || cp.dist < 1e-12);
-        v.cmin[i] = cp.dist;
-        if (act) {
-          k = cand_key(r, v.ns, v.idBits, 0, 0);
-          if (r[0] == 0) atomicAdd(&v.cint[CI_NVT], 1);
-        }
+  double dmin = INFINITY;
+  if (i < Ccap && i < cand_count(v)) {
+    int r[6];
+    cand_rec(v, i, r);
+    if (r[0] != 3) {
+      Closest cp;
+      cand_closest(v, x, r, cp);
+      act = !(cp.dist >= v.c.dHat || cp.dist < 1e-12);
+      if (cp.dist < dmin) dmin = cp.dist;
+      if (act) {
+        k = cand_key(r, v.ns, v.idBits, 0, 0);
+        if (r[0] == 0) atomicAdd(&v.cint[CI_NVT], 1);
       }
     }
   }
+  block_min_into(dmin, INFINITY, &v.omin[2], nullptr);
   const uint32_t mask = __ballot_sync(0xffffffffu, act);
   if (!mask) return;
   const int lane = threadIdx.x & 31;
@@ -128,18 +217,21 @@ __global__ void k_cand_flags(CView v, const double* x, int Ccap, Key<4>* keys, u
   }
 }
 
+// Floor flags, and the floor distances folded into the active-set minimum
+// (contact-assembly.ts:200-215).
 __global__ void k_floor_flags(CView v, const double* x) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= v.n) return;
-  if (!v.c.hasFloor) { v.fflag[i] = 0; v.vtmp[i] = INFINITY; return; }
-  const double d = x[i * 3 + 1] - v.c.floorY;
-  v.vtmp[i] = d;
-  v.fflag[i] = d >= v.c.dHat ? 0u : 1u;
-}
-
-__device__ __forceinline__ bool cand_active(const CView& v, int i) {
-  const double d = v.cmin[i];
-  return !(d >= v.c.dHat || d < 1e-12);
+  double dmin = INFINITY;
+  if (i < v.n) {
+    if (!v.c.hasFloor) {
+      v.fflag[i] = 0;
+    } else {
+      const double d = x[i * 3 + 1] - v.c.floorY;
+      if (d < dmin) dmin = d;
+      v.fflag[i] = d >= v.c.dHat ? 0u : 1u;
+    }
+  }
+  block_min_into(dmin, INFINITY, &v.omin[2], nullptr);
 }
 
 // Frozen record j of the active set from the j-th candidate in key order
@@ -147,7 +239,8 @@ __device__ __forceinline__ bool cand_active(const CView& v, int i) {
 __global__ void k_cand_active(CView v, const double* x, const uint32_t* order, int nAct) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= nAct) return;
-  const int* r = v.rec + (size_t)order[j] * 6;
+  int r[6];
+  cand_rec(v, (int)order[j], r);
   Closest cp;
   cand_closest(v, x, r, cp);
   Frozen f;
@@ -175,46 +268,13 @@ __global__ void k_floor_compact(CView v, const double* x) {
   v.active[v.nCand + v.fflag[i]] = f;
 }
 
-// Minimum ignoring NaN (the reference's `if (d < minD) minD = d`) over two arrays.
-__device__ double block_min2(const double* a, int na, const double* b, int nb) {
-  __shared__ double sm[1024];
-  double m = INFINITY;
-  for (int i = threadIdx.x; i < na; i += blockDim.x) if (a[i] < m) m = a[i];
-  for (int i = threadIdx.x; i < nb; i += blockDim.x) if (b[i] < m) m = b[i];
-  sm[threadIdx.x] = m;
-  __syncthreads();
-  for (int off = blockDim.x / 2; off > 0; off >>= 1) {
-    if ((int)threadIdx.x < off && sm[threadIdx.x + off] < sm[threadIdx.x]) sm[threadIdx.x] = sm[threadIdx.x + off];
-    __syncthreads();
-  }
-  const double r = sm[0];
-  __syncthreads();
-  return r;
+__global__ void k_active_reset(CView v) {
+  v.cint[CI_NVT] = 0;
+  v.cint[CI_NCAND] = 0;
+  v.omin[2] = kOrdInf;
 }
-
-// Per-block minima (NaN ignored) of a[0..na) and b[0..nb) into part[blockIdx].
-constexpr int kMinBlocks = 128;
-__global__ void __launch_bounds__(256) k_min_part(const double* a, int na, const double* b, int nb, double* part) {
-  __shared__ double sm[256];
-  double m = INFINITY;
-  const int stride = gridDim.x * blockDim.x;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < na; i += stride) if (a[i] < m) m = a[i];
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += stride) if (b[i] < m) m = b[i];
-  sm[threadIdx.x] = m;
-  __syncthreads();
-  for (int off = 128; off > 0; off >>= 1) {
-    if ((int)threadIdx.x < off && sm[threadIdx.x + off] < sm[threadIdx.x]) sm[threadIdx.x] = sm[threadIdx.x + off];
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) part[blockIdx.x] = sm[0];
-}
-__device__ __forceinline__ double min_of_parts(const double* part) {
-  double m = INFINITY;
-  for (int i = 0; i < kMinBlocks; i++) if (part[i] < m) m = part[i];
-  return m;
-}
-__global__ void k_active_min(CView v, const double* part) {
-  const double m = min_of_parts(part);
+__global__ void k_active_min(CView v) {
+  const double m = dbl_of(v.omin[2]);
   if (m < v.diag->minDistance) v.diag->minDistance = m;
 }
 
@@ -441,25 +501,28 @@ __global__ void k_gather_vals(const double4* src, const uint32_t* order, int n, 
 }
 
 // ---- trial validation (contact-assembly.ts:489-553) ----------------------------------
-__global__ void k_trial_reset(int* cint, unsigned long long* badKey) {
-  cint[CI_FIRSTNF] = INT_MAX;
-  cint[CI_FLOORBAD] = 0;
-  cint[CI_VALID] = 0;
-  badKey[0] = ~0ull;
-  badKey[1] = ~0ull;
+__global__ void k_trial_reset(CView v) {
+  v.cint[CI_FIRSTNF] = INT_MAX;
+  v.cint[CI_FLOORBAD] = 0;
+  v.cint[CI_VALID] = 0;
+  v.cint[CI_NBAD] = 0;
+  v.badKey[0] = ~0ull;
+  v.badKey[1] = ~0ull;
+  v.omin[0] = kOrdInf;
+  v.omin[1] = kOrdInf;
 }
 
-__global__ void k_trial_cand(CView v, const double* xt, int Ccap, double dMin) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= Ccap) return;
+// Trial distance and CCD of candidate i; returns its distance and TOI for the
+// minima (+inf when it has none).
+__device__ __forceinline__ void trial_one(const CView& v, const double* xt, int i, double dMin, double& dOut,
+                                          double& tOut) {
   v.cflag[i] = 0;
-  v.ctoi[i] = INFINITY;
-  if (i >= cand_count(v)) { v.cmin[i] = INFINITY; return; }
-  const int* r = v.rec + (size_t)i * 6;
-  if (r[0] == 3) { v.cmin[i] = INFINITY; return; }
+  int r[6];
+  cand_rec(v, i, r);
+  if (r[0] == 3) return;
   Closest cp;
   cand_closest(v, xt, r, cp);
-  v.cmin[i] = cp.dist;
+  dOut = cp.dist;
   if (!isfinite(cp.dist)) atomicMin(&v.cint[CI_FIRSTNF], i);
   int ids[4];
   if (r[0] == 0) {
@@ -474,48 +537,70 @@ __global__ void k_trial_cand(CView v, const double* xt, int Ccap, double dMin) {
     cpos(v.c, v.x0, ids[k], P0 + k * 3);
     cpos(v.c, xt, ids[k], P1 + k * 3);
   }
-  const double toi = r[0] == 0 ? vt_ccd(P0, P1, dMin) : ee_ccd(P0, P1, dMin);
-  v.ctoi[i] = toi;
+  const double toi = trial_ccd(r[0] == 0 ? 0 : 1, P0, P1, cp.dist, dMin);
+  tOut = toi;
   uint32_t st = 0;
   if (isnan(toi)) st = 2;
   else if (toi > 0 && toi < 1 - 1e-9) st = 1;
+  if (!st) return;
   v.cflag[i] = st;
   // The reference stops at the first failing candidate in key order; its
   // status (NaN or crossing) is the low two bits of the smallest (key, status).
-  if (st) atomicMin(&v.badKey[0], (unsigned long long)cand_key(r, v.ns, v.idBits, 2, st).hi);
+  atomicMin(&v.badKey[0], (unsigned long long)cand_key(r, v.ns, v.idBits, 2, st).hi);
+  const int j = atomicAdd(&v.cint[CI_NBAD], 1);
+  if (j < kBadCap) v.badList[j] = i;
+}
+
+// checkTrial's candidate loops (contact-assembly.ts:498-535): exact distances at
+// the trial, CCD of the segment, and their minima.
+__global__ void __launch_bounds__(kCT) k_trial_cand(CView v, const double* xt, int Ccap, double dMin) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double d = INFINITY, t = INFINITY, dOut = INFINITY, tOut = INFINITY;
+  if (i < Ccap && i < cand_count(v)) trial_one(v, xt, i, dMin, dOut, tOut);
+  if (dOut < d) d = dOut;
+  if (tOut < t) t = tOut;
+  block_min_into(d, t, &v.omin[0], &v.omin[1]);
 }
 
 // Second half of the smallest failing (key, status): the low word among the
-// failing candidates whose high word is the minimum.
+// failing candidates whose high word is the minimum. Walks the list of failing
+// indices, or every candidate when more failed than the list holds.
 __global__ void k_trial_bad_lo(CView v, int C) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= C) return;
-  const uint32_t st = v.cflag[i];
-  if (!st) return;
-  const CandKey k = cand_key(v.rec + (size_t)i * 6, v.ns, v.idBits, 2, st);
-  if (k.hi == v.badKey[0]) atomicMin(&v.badKey[1], (unsigned long long)k.lo);
+  const int nbad = v.cint[CI_NBAD];
+  if (nbad == 0) return;
+  const bool listed = nbad <= kBadCap;
+  const int cnt = listed ? nbad : C;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < cnt; j += gridDim.x * blockDim.x) {
+    const int i = listed ? v.badList[j] : j;
+    const uint32_t st = v.cflag[i];
+    if (!st) continue;
+    int r[6];
+    cand_rec(v, i, r);
+    const CandKey k = cand_key(r, v.ns, v.idBits, 2, st);
+    if (k.hi == v.badKey[0]) atomicMin(&v.badKey[1], (unsigned long long)k.lo);
+  }
 }
 
 __global__ void k_trial_floor(CView v, const double* xt, double dMin) {
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= v.n) return;
-  v.vtmp2[q] = INFINITY;
-  if (!v.c.hasFloor) { v.vtmp[q] = INFINITY; return; }
-  const double dd = xt[q * 3 + 1] - v.c.floorY;
-  v.vtmp[q] = dd;
-  const double y0 = v.x0[q * 3 + 1] - v.c.floorY;
-  const double yT = xt[q * 3 + 1] - v.c.floorY;
-  if (y0 - fabs(yT - y0) > dMin) return;
-  if (y0 > dMin && yT <= dMin && y0 > yT) {
-    const double toi = (y0 - dMin) / (y0 - yT);
-    v.vtmp2[q] = toi;
-    if (toi < 1 - 1e-9) atomicOr(&v.cint[CI_FLOORBAD], 1);
+  double d = INFINITY, t = INFINITY;
+  if (q < v.n && v.c.hasFloor) {
+    const double dd = xt[q * 3 + 1] - v.c.floorY;
+    if (dd < d) d = dd;
+    const double y0 = v.x0[q * 3 + 1] - v.c.floorY;
+    const double yT = xt[q * 3 + 1] - v.c.floorY;
+    if (!(y0 - fabs(yT - y0) > dMin) && y0 > dMin && yT <= dMin && y0 > yT) {
+      const double toi = (y0 - dMin) / (y0 - yT);
+      if (toi < t) t = toi;
+      if (toi < 1 - 1e-9) atomicOr(&v.cint[CI_FLOORBAD], 1);
+    }
   }
+  block_min_into(d, t, &v.omin[0], &v.omin[1]);
 }
 
-__global__ void k_trial_final(CView v, const double* partDist, const double* partToi, double dMin) {
-  const double minDist = min_of_parts(partDist);
-  const double minTOI = min_of_parts(partToi);
+__global__ void k_trial_final(CView v, double dMin) {
+  const double minDist = dbl_of(v.omin[0]);
+  const double minTOI = dbl_of(v.omin[1]);
   int valid = 0;
   DevDiag* dg = v.diag;
   if (v.cint[CI_FIRSTNF] != INT_MAX) {
@@ -535,62 +620,112 @@ __global__ void k_trial_final(CView v, const double* partDist, const double* par
 }
 
 // ---- restitution-0 filter (newton.ts:238-303) -----------------------------------------
+// Restitution-0 impulse of one VT or EE contact (newton.ts:246-301).
+__device__ __forceinline__ void kill_one(const Frozen& c, double* vel) {
+  if (c.kind == 0) {
+    const double vp[3] = {vel[c.p * 3], vel[c.p * 3 + 1], vel[c.p * 3 + 2]};
+    double tx = 0, ty = 0, tz = 0;
+    const double ws[3] = {c.w0, c.w1, c.w2};
+    const int vs[3] = {c.a, c.b, c.c};
+    for (int k = 0; k < 3; k++) {
+      if (vs[k] < 0) continue;
+      tx += ws[k] * vel[vs[k] * 3];
+      ty += ws[k] * vel[vs[k] * 3 + 1];
+      tz += ws[k] * vel[vs[k] * 3 + 2];
+    }
+    const double rel = (vp[0] - tx) * c.nx + (vp[1] - ty) * c.ny + (vp[2] - tz) * c.nz;
+    if (rel < 0) {
+      const double j = -0.5 * rel;
+      vel[c.p * 3] += j * c.nx;
+      vel[c.p * 3 + 1] += j * c.ny;
+      vel[c.p * 3 + 2] += j * c.nz;
+      for (int k = 0; k < 3; k++) {
+        if (vs[k] < 0) continue;
+        vel[vs[k] * 3] -= j * ws[k] * c.nx;
+        vel[vs[k] * 3 + 1] -= j * ws[k] * c.ny;
+        vel[vs[k] * 3 + 2] -= j * ws[k] * c.nz;
+      }
+    }
+    return;
+  }
+  double A[3] = {0, 0, 0}, B[3] = {0, 0, 0};
+  {
+    double xa[3] = {0, 0, 0}, xb[3] = {0, 0, 0};
+    if (c.a >= 0) for (int k = 0; k < 3; k++) xa[k] = vel[c.a * 3 + k];
+    if (c.b >= 0) for (int k = 0; k < 3; k++) xb[k] = vel[c.b * 3 + k];
+    for (int k = 0; k < 3; k++) A[k] = (xa[k] + xb[k]) / 2;
+    double xc[3] = {0, 0, 0}, xd[3] = {0, 0, 0};
+    if (c.c >= 0) for (int k = 0; k < 3; k++) xc[k] = vel[c.c * 3 + k];
+    if (c.d >= 0) for (int k = 0; k < 3; k++) xd[k] = vel[c.d * 3 + k];
+    for (int k = 0; k < 3; k++) B[k] = (xc[k] + xd[k]) / 2;
+  }
+  const double rel = (A[0] - B[0]) * c.nx + (A[1] - B[1]) * c.ny + (A[2] - B[2]) * c.nz;
+  if (rel < 0) {
+    const double j = -0.25 * rel;
+    const int up[2] = {c.a, c.b}, dn[2] = {c.c, c.d};
+    for (int q = 0; q < 2; q++) {
+      if (up[q] < 0) continue;
+      vel[up[q] * 3] += j * c.nx; vel[up[q] * 3 + 1] += j * c.ny; vel[up[q] * 3 + 2] += j * c.nz;
+    }
+    for (int q = 0; q < 2; q++) {
+      if (dn[q] < 0) continue;
+      vel[dn[q] * 3] -= j * c.nx; vel[dn[q] * 3 + 1] -= j * c.ny; vel[dn[q] * 3 + 2] -= j * c.nz;
+    }
+  }
+}
+
 // VT/EE impulses in list order by one thread (each sees the earlier updates).
 __global__ void k_kill_vtee(CView v, double* vel, int nve) {
   if (blockIdx.x != 0 || threadIdx.x != 0) return;
-  for (int i = 0; i < nve; i++) {
-    const Frozen c = v.active[i];
-    if (c.kind == 0) {
-      const double vp[3] = {vel[c.p * 3], vel[c.p * 3 + 1], vel[c.p * 3 + 2]};
-      double tx = 0, ty = 0, tz = 0;
-      const double ws[3] = {c.w0, c.w1, c.w2};
-      const int vs[3] = {c.a, c.b, c.c};
-      for (int k = 0; k < 3; k++) {
-        if (vs[k] < 0) continue;
-        tx += ws[k] * vel[vs[k] * 3];
-        ty += ws[k] * vel[vs[k] * 3 + 1];
-        tz += ws[k] * vel[vs[k] * 3 + 2];
-      }
-      const double rel = (vp[0] - tx) * c.nx + (vp[1] - ty) * c.ny + (vp[2] - tz) * c.nz;
-      if (rel < 0) {
-        const double j = -0.5 * rel;
-        vel[c.p * 3] += j * c.nx;
-        vel[c.p * 3 + 1] += j * c.ny;
-        vel[c.p * 3 + 2] += j * c.nz;
-        for (int k = 0; k < 3; k++) {
-          if (vs[k] < 0) continue;
-          vel[vs[k] * 3] -= j * ws[k] * c.nx;
-          vel[vs[k] * 3 + 1] -= j * ws[k] * c.ny;
-          vel[vs[k] * 3 + 2] -= j * ws[k] * c.nz;
-        }
-      }
-      continue;
+  for (int i = 0; i < nve; i++) kill_one(v.active[i], vel);
+}
+
+// Predecessor of each VT/EE contact on each of its cloth vertices: the previous
+// contact in that vertex's list (the vertex -> (contact, slot) CSR is in contact
+// order), -1 for none or a static vertex.
+__global__ void k_kill_pred(CView v, const Key<1>* rk, const uint32_t* rp, const uint32_t* off, int nrec, int nve,
+                            int* pred) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= nrec) return;
+  const uint32_t vert = rk[q].w[0];
+  const uint32_t pay = rp[q];
+  const int c = (int)(pay >> 2), slot = (int)(pay & 3);
+  if (c >= nve) return;
+  pred[c * 4 + slot] = (vert != 0xffffffffu && q > (int)off[vert]) ? (int)(rp[q - 1] >> 2) : -1;
+}
+
+// The same pass by one block in rounds: a contact is applied once its
+// predecessor on each of its vertices has been. Contacts applied in one round
+// share no vertex, and every vertex receives its contacts' impulses in list
+// order, so the velocities equal the one-thread pass bit for bit. The smallest
+// pending contact is always ready, so each round applies at least one and
+// nve + 1 rounds bound the loop; diag->killStall is set if it ever runs out.
+constexpr int kKillThreads = 1024;
+__global__ void __launch_bounds__(kKillThreads) k_kill_vtee_rounds(CView v, double* vel, int nve,
+                                                                   const int* pred) {
+  extern __shared__ uint32_t doneBits[];
+  const int words = (nve + 31) >> 5;
+  for (int w = threadIdx.x; w < words; w += blockDim.x) doneBits[w] = 0;
+  __syncthreads();
+  int cur = threadIdx.x;
+  auto done = [&](int c) { return c < 0 || c == cur || ((doneBits[c >> 5] >> (c & 31)) & 1u); };
+  bool pending = cur < nve;
+  for (int round = 0; round <= nve; round++) {
+    bool ready = false;
+    if (pending) {
+      const int4 pr = reinterpret_cast<const int4*>(pred)[cur];
+      ready = done(pr.x) && done(pr.y) && done(pr.z) && done(pr.w);
+      if (ready) kill_one(v.active[cur], vel);
     }
-    double A[3] = {0, 0, 0}, B[3] = {0, 0, 0};
-    {
-      double xa[3] = {0, 0, 0}, xb[3] = {0, 0, 0};
-      if (c.a >= 0) for (int k = 0; k < 3; k++) xa[k] = vel[c.a * 3 + k];
-      if (c.b >= 0) for (int k = 0; k < 3; k++) xb[k] = vel[c.b * 3 + k];
-      for (int k = 0; k < 3; k++) A[k] = (xa[k] + xb[k]) / 2;
-      double xc[3] = {0, 0, 0}, xd[3] = {0, 0, 0};
-      if (c.c >= 0) for (int k = 0; k < 3; k++) xc[k] = vel[c.c * 3 + k];
-      if (c.d >= 0) for (int k = 0; k < 3; k++) xd[k] = vel[c.d * 3 + k];
-      for (int k = 0; k < 3; k++) B[k] = (xc[k] + xd[k]) / 2;
+    __syncthreads();
+    if (ready) {
+      atomicOr(&doneBits[cur >> 5], 1u << (cur & 31));
+      cur += blockDim.x;
+      pending = cur < nve;
     }
-    const double rel = (A[0] - B[0]) * c.nx + (A[1] - B[1]) * c.ny + (A[2] - B[2]) * c.nz;
-    if (rel < 0) {
-      const double j = -0.25 * rel;
-      const int up[2] = {c.a, c.b}, dn[2] = {c.c, c.d};
-      for (int q = 0; q < 2; q++) {
-        if (up[q] < 0) continue;
-        vel[up[q] * 3] += j * c.nx; vel[up[q] * 3 + 1] += j * c.ny; vel[up[q] * 3 + 2] += j * c.nz;
-      }
-      for (int q = 0; q < 2; q++) {
-        if (dn[q] < 0) continue;
-        vel[dn[q] * 3] -= j * c.nx; vel[dn[q] * 3 + 1] -= j * c.ny; vel[dn[q] * 3 + 2] -= j * c.nz;
-      }
-    }
+    if (!__syncthreads_or(pending)) return;
   }
+  if (threadIdx.x == 0) v.diag->killStall = 1;
 }
 
 __global__ void k_kill_floor(CView v, double* vel, int base, int nf) {
@@ -620,17 +755,18 @@ static CView view(ContactHost& h, Solver& s) {
   v.nFloor = h.nFloor;
   v.n = h.n;
   v.x0 = s.d.x0;
-  v.rec = h.cand.rec;
+  v.selfPairs = h.bvh.pairs;
+  v.staticPairs = h.spairs;
+  v.idx = s.idx.p;
+  v.sidx = h.sidx;
   v.ns = h.ns;
   v.idBits = h.idBits;
   v.badKey = h.badKey;
   v.ccnt = (const uint32_t*)(h.cint + CI_SELF);
   v.cflag = h.cflag;
   v.fflag = h.fflag;
-  v.cmin = h.cmin;
-  v.ctoi = h.ctoi;
-  v.vtmp = h.probe + 3 * (size_t)h.n;
-  v.vtmp2 = h.probe + 4 * (size_t)h.n;
+  v.omin = h.omin;
+  v.badList = h.badList;
   v.active = h.active;
   v.dd = h.dd;
   v.cg = h.cg;
@@ -651,13 +787,13 @@ ContactHost::~ContactHost() {
                    (void**)&bvh.cent, (void**)&bvh.scene, (void**)&bvh.k0, (void**)&bvh.k1, (void**)&bvh.p0,
                    (void**)&bvh.p1, (void**)&bvh.hist, (void**)&bvh.left, (void**)&bvh.right, (void**)&bvh.parent,
                    (void**)&bvh.depth, (void**)&bvh.nbox, (void**)&bvh.rec, (void**)&bvh.visit, (void**)&bvh.root,
-                   (void**)&bvh.pairs, (void**)&badKey, (void**)&spairs, (void**)&cand.rec,
+                   (void**)&bvh.pairs, (void**)&badKey, (void**)&spairs,
                    (void**)&cand.k0, (void**)&cand.k1, (void**)&cand.p0, (void**)&cand.p1, (void**)&cand.hist,
-                   (void**)&cflag, (void**)&fflag, (void**)&cmin, (void**)&ctoi, (void**)&active, (void**)&dd,
+                   (void**)&cflag, (void**)&fflag, (void**)&omin, (void**)&badList, (void**)&active, (void**)&dd,
                    (void**)&cg, (void**)&tc, (void**)&tf, (void**)&rk0, (void**)&rk1, (void**)&rp0, (void**)&rp1,
-                   (void**)&rhist, (void**)&cOff, (void**)&lagFloor, (void**)&lagFloorOk, (void**)&lk0,
+                   (void**)&rhist, (void**)&kpred, (void**)&cOff, (void**)&lagFloor, (void**)&lagFloorOk, (void**)&lk0,
                    (void**)&lk1, (void**)&lp0, (void**)&lp1, (void**)&lhist, (void**)&lval, (void**)&lsorted,
-                   (void**)&probe, (void**)&diag, (void**)&cint, (void**)&minpart, (void**)&supPairs,
+                   (void**)&probe, (void**)&diag, (void**)&cint, (void**)&supPairs,
                    (void**)&supSPairs, (void**)&supBase})
     if (*q) cudaFree(*q);
   if (hint) cudaFreeHost(hint);
@@ -709,14 +845,15 @@ void ContactHost::init(Solver& s, const cs_contact_params* prm, int floor_on, do
   dalloc(bvh.visit, nn);
   dalloc(bvh.root, 1);
   dalloc(badKey, 2);
+  dalloc(omin, 3);
+  dalloc(badList, kBadCap);
   dalloc(supBase, 3 * (size_t)n);
   dalloc(fflag, (size_t)n + 1);
   dalloc(cOff, (size_t)n + 1);
   dalloc(lagFloor, (size_t)n);
   dalloc(lagFloorOk, (size_t)n);
-  dalloc(probe, 5 * (size_t)n);
+  dalloc(probe, 3 * (size_t)n);
   dalloc(diag, 1);
-  dalloc(minpart, 2 * kMinBlocks);
   dalloc(cint, CI_N);
   CK(cudaMallocHost(&hint, CI_N * sizeof(int)));
   CK(cudaMallocHost(&hdiag, sizeof(DevDiag)));
@@ -736,15 +873,12 @@ void ContactHost::ensure_cands(size_t nc) {
   if ((int)nc <= cand.cap) return;
   const size_t c = nc + nc / 2 + 256;
   cand.cap = (int)c;
-  dalloc(cand.rec, 6 * c);
   dalloc(cand.k0, c);
   dalloc(cand.k1, c);
   dalloc(cand.p0, c);
   dalloc(cand.p1, c);
   dalloc(cand.hist, 256 * ((c + kSortTile - 1) / kSortTile) + 1);
   dalloc(cflag, c + 1);
-  dalloc(cmin, c);
-  dalloc(ctoi, c);
 }
 void ContactHost::ensure_active(Solver& s, size_t na) {
   if (na <= actCap) return;
@@ -760,6 +894,7 @@ void ContactHost::ensure_active(Solver& s, size_t na) {
   dalloc(rp0, 4 * c);
   dalloc(rp1, 4 * c);
   dalloc(rhist, 256 * ((4 * c + kSortTile - 1) / kSortTile) + 1);
+  dalloc(kpred, 4 * c);
   (void)s;
 }
 void ContactHost::ensure_lag(size_t nl) {
@@ -884,7 +1019,6 @@ int ContactHost::build_candidates(Solver& s, const double* x, double pad) {
   const long C = 15l * P + 12l * S;
   if (C > INT_MAX / 8) throw CapacityError("too many contact candidates");
   ensure_cands(C);
-  expand_candidates(cand, s.idx.p, sidx, bvh.pairs, P, spairs, S, (const uint32_t*)(cint + CI_SELF), st, &lc);
   return (int)C;
 }
 
@@ -892,17 +1026,16 @@ void ContactHost::update_active_set(Solver& s, double* x) {
   cudaStream_t st = s.stream;
   int64_t& lc = launch_counter();
   const int C = build_candidates(s, x, p.dhat);  // an upper bound; the exact count is on the device
-  CK(cudaMemsetAsync(cint + CI_NVT, 0, sizeof(int), st));
-  CK(cudaMemsetAsync(cint + CI_NCAND, 0, sizeof(int), st));
   CView v = view(*this, s);
+  k_active_reset<<<1, 1, 0, st>>>(v);
+  lc++;
   if (C > 0) {
     k_cand_flags<<<cnb(C), kCT, 0, st>>>(v, x, C, cand.k0, cand.p0);
     lc++;
   }
   k_floor_flags<<<cnb(n), kCT, 0, st>>>(v, x);
-  k_min_part<<<kMinBlocks, 256, 0, st>>>(cmin, C, v.vtmp, n, minpart);
-  k_active_min<<<1, 1, 0, st>>>(v, minpart);
-  lc += 3;
+  k_active_min<<<1, 1, 0, st>>>(v);
+  lc += 2;
   scan_counts(fflag, n, (uint32_t*)(cint + CI_NFLOOR), st, &lc);
   read_ints(s);
   candidatePairs = 15.0 * (uint32_t)hint[CI_SELF] + 12.0 * (uint32_t)(ms > 0 ? hint[CI_STATIC] : 0);
@@ -977,19 +1110,17 @@ bool ContactHost::check_trial(Solver& s, const double* xt) {
   cudaStream_t st = s.stream;
   int64_t& lc = launch_counter();
   const int C = build_candidates(s, xt, p.dmin);  // an upper bound; the exact count is on the device
-  k_trial_reset<<<1, 1, 0, st>>>(cint, badKey);
-  lc++;
   CView v = view(*this, s);
+  k_trial_reset<<<1, 1, 0, st>>>(v);
+  lc++;
   if (C > 0) {
     k_trial_cand<<<cnb(C), kCT, 0, st>>>(v, xt, C, p.dmin);
-    k_trial_bad_lo<<<cnb(C), kCT, 0, st>>>(v, C);
+    k_trial_bad_lo<<<std::min(cnb(C), 4 * 148), kCT, 0, st>>>(v, C);
     lc += 2;
   }
   k_trial_floor<<<cnb(n), kCT, 0, st>>>(v, xt, p.dmin);
-  k_min_part<<<kMinBlocks, 256, 0, st>>>(cmin, C, v.vtmp, n, minpart);
-  k_min_part<<<kMinBlocks, 256, 0, st>>>(ctoi, C, v.vtmp2, n, minpart + kMinBlocks);
-  k_trial_final<<<1, 1, 0, st>>>(v, minpart, minpart + kMinBlocks, p.dmin);
-  lc += 5;
+  k_trial_final<<<1, 1, 0, st>>>(v, p.dmin);
+  lc += 2;
   read_ints(s);
   candidatePairs = 15.0 * (uint32_t)hint[CI_SELF] + 12.0 * (uint32_t)(ms > 0 ? hint[CI_STATIC] : 0);
   return hint[CI_VALID] != 0;
@@ -1026,8 +1157,18 @@ void ContactHost::kill_approach_velocity(Solver& s) {
   update_active_set(s, s.d.x);
   CView v = view(*this, s);
   if (nCand > 0) {
-    k_kill_vtee<<<1, 1, 0, s.stream>>>(v, s.d.v, nCand);
-    launch_counter()++;
+    const size_t smem = 4 * (((size_t)nCand + 31) / 32);
+    if (smem <= 48 * 1024) {
+      // The vertex -> (contact, slot) CSR of update_active_set gives each
+      // contact's predecessors; the rounds kernel applies them in parallel.
+      k_kill_pred<<<cnb(4l * (nCand + nFloor)), kCT, 0, s.stream>>>(v, rk0, rp0, cOff, 4 * (nCand + nFloor), nCand,
+                                                                     kpred);
+      k_kill_vtee_rounds<<<1, kKillThreads, smem, s.stream>>>(v, s.d.v, nCand, kpred);
+      launch_counter() += 2;
+    } else {
+      k_kill_vtee<<<1, 1, 0, s.stream>>>(v, s.d.v, nCand);
+      launch_counter()++;
+    }
   }
   if (nFloor > 0) {
     k_kill_floor<<<cnb(nFloor), kCT, 0, s.stream>>>(v, s.d.v, nCand, nFloor);
@@ -1071,6 +1212,7 @@ void ContactHost::begin_step_and_bisect(Solver& s) {
 void ContactHost::fill_stats(Solver& s, cs_step_stats& out) {
   CK(cudaMemcpyAsync(hdiag, diag, sizeof(DevDiag), cudaMemcpyDeviceToHost, s.stream));
   CK(cudaStreamSynchronize(s.stream));
+  if (hdiag->killStall != 0) throw std::runtime_error("restitution pass did not complete");
   out.candidate_pairs = candidatePairs;
   out.active_pairs = activePairs;
   out.vt_pairs = vtPairs;

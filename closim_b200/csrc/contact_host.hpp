@@ -24,12 +24,14 @@ struct CapacityError : std::runtime_error {
 struct DevDiag {
   double minDistance, minTOI, barrierEnergy, frictionWork, ccdFailures;
   double trialMinDist, trialMinTOI;
-  double pad;
+  double killStall;  // set if the restitution rounds ran out (never expected)
 };
 
 // Device counters read back by the host (int32).
 enum CInt { CI_SELF = 0, CI_STATIC, CI_OVERFLOW, CI_NCAND, CI_NFLOOR, CI_NVT, CI_VALID, CI_FIRSTNF, CI_MOVED,
-            CI_FLOORBAD, CI_N = 16 };
+            CI_FLOORBAD, CI_NBAD, CI_N = 16 };
+// Failing trial candidates listed by index for the second key pass.
+constexpr int kBadCap = 4096;
 
 class ContactHost {
  public:
@@ -67,8 +69,8 @@ class ContactHost {
   CandBufs cand;
   uint32_t* cflag = nullptr;   // per-candidate flag / offset / trial status (cand cap + 1)
   uint32_t* fflag = nullptr;   // per-vertex floor flag / offset (n + 1)
-  double* cmin = nullptr;      // per-candidate distance (cand cap)
-  double* ctoi = nullptr;      // per-candidate toi
+  unsigned long long* omin = nullptr;  // ordered images of the trial / active-set minima (3)
+  int* badList = nullptr;      // failing trial candidates (kBadCap)
   // frozen set
   size_t actCap = 0;
   Frozen* active = nullptr;
@@ -79,6 +81,7 @@ class ContactHost {
   Key<1>* rk0 = nullptr; Key<1>* rk1 = nullptr;
   uint32_t* rp0 = nullptr; uint32_t* rp1 = nullptr; uint32_t* rhist = nullptr;
   uint32_t* cOff = nullptr;    // n + 1
+  int* kpred = nullptr;        // 4 per contact: predecessor on each vertex (restitution pass)
   // lagged normals / multipliers
   double* lagFloor = nullptr;  // n
   uint8_t* lagFloorOk = nullptr;
@@ -90,7 +93,6 @@ class ContactHost {
   // probes
   double* probe = nullptr;
   DevDiag* diag = nullptr;
-  double* minpart = nullptr;   // per-block minima (2 x 128)
   int* cint = nullptr;
   int* hint = nullptr;         // pinned mirror of cint
   DevDiag* hdiag = nullptr;    // pinned mirror of diag

@@ -204,14 +204,50 @@ CSHD double stencil_dev(const double* P0, const double* P1) {
   return dev;
 }
 
+// Largest Euclidean motion of a stencil vertex relative to the stencil's mean
+// motion. Every point of either primitive (VT or EE) is a convex combination of
+// its vertices, so the gap vector between two such points changes by at most
+// twice this between P0 and P1: the distance at P0 is at least the distance at
+// P1 minus twice this.
+CSHD double stencil_rel_motion(const double* P0, const double* P1) {
+  double mx = 0, my = 0, mz = 0;
+  for (int v = 0; v < 4; v++) {
+    mx += P1[v * 3] - P0[v * 3];
+    my += P1[v * 3 + 1] - P0[v * 3 + 1];
+    mz += P1[v * 3 + 2] - P0[v * 3 + 2];
+  }
+  mx /= 4; my /= 4; mz /= 4;
+  double e = 0;
+  for (int v = 0; v < 4; v++) {
+    const double dx = P1[v * 3] - P0[v * 3] - mx;
+    const double dy = P1[v * 3 + 1] - P0[v * 3 + 1] - my;
+    const double dz = P1[v * 3 + 2] - P0[v * 3 + 2] - mz;
+    e = js_max(e, sqrt(dx * dx + dy * dy + dz * dz));
+  }
+  return e;
+}
+
+// Sweep bound for the CCD: with d0, d1 the distances at the ends of the
+// segment and E = stencil_rel_motion, the distance at time t is at least
+// max(d0 - 2 E t, d1 - 2 E (1 - t)) >= (d0 + d1) / 2 - E. When that exceeds the
+// thickness, no root and no sample of the CCD below can come within it, so the
+// CCD returns +inf; the 1e-6 relative margin covers the rounding of the
+// computed distances and sample positions. d1 = NaN disables the test.
+CSHD bool sweep_clear(double d0, double d1, double E, double thickness) {
+  return (d0 + d1) / 2 - E > thickness * (1 + 1e-6);
+}
+
 // Earliest time of impact in [0,1] of vertex p against triangle abc moving
-// linearly P0 -> P1 (stencil order p, a, b, c), or +inf when safe.
-CSHD double vt_ccd(const double* P0, const double* P1, double thickness) {
+// linearly P0 -> P1 (stencil order p, a, b, c), or +inf when safe. d1 and E
+// (the distance at P1 and stencil_rel_motion) feed sweep_clear, which returns
+// the same +inf sooner.
+CSHD double vt_ccd(const double* P0, const double* P1, double thickness, double d1 = NAN, double E = 0) {
   const double* p0 = P0; const double* a0 = P0 + 3; const double* b0 = P0 + 6; const double* c0 = P0 + 9;
   const double d0 = closest_vt(p0, a0, b0, c0).dist;
   if (d0 <= thickness) return 0;
   const double dev = stencil_dev(P0, P1);
   if (d0 - 4 * dev > thickness) return INFINITY;
+  if (sweep_clear(d0, d1, E, thickness)) return INFINITY;
   double dp[3], da[3], db[3], dc[3];
   for (int i = 0; i < 3; i++) {
     dp[i] = P1[i] - P0[i]; da[i] = P1[3 + i] - P0[3 + i];
@@ -267,8 +303,8 @@ CSHD Closest ee_at(const double* a0, const double* da, const double* b0, const d
   return closest_ee(A, B, C, D);
 }
 
-// Edge ab vs edge cd (stencil order a, b, c, d).
-CSHD double ee_ccd(const double* P0, const double* P1, double thickness) {
+// Edge ab vs edge cd (stencil order a, b, c, d); d1, E as for vt_ccd.
+CSHD double ee_ccd(const double* P0, const double* P1, double thickness, double d1 = NAN, double E = 0) {
   const double* a0 = P0; const double* b0 = P0 + 3; const double* c0 = P0 + 6; const double* d0 = P0 + 9;
   double da[3], db[3], dc[3], dd[3];
   for (int i = 0; i < 3; i++) {
@@ -279,6 +315,7 @@ CSHD double ee_ccd(const double* P0, const double* P1, double thickness) {
   if (q0 <= thickness) return 0;
   const double dev = stencil_dev(P0, P1);
   if (q0 - 4 * dev > thickness) return INFINITY;
+  if (sweep_clear(q0, d1, E, thickness)) return INFINITY;
   double e10[3], de1[3], e20[3], de2[3], r0[3], dr[3];
   for (int i = 0; i < 3; i++) {
     e10[i] = b0[i] - a0[i]; de1[i] = db[i] - da[i];
@@ -309,6 +346,16 @@ CSHD double ee_ccd(const double* P0, const double* P1, double thickness) {
   }
   if (minD <= thickness) return minT;
   return INFINITY;
+}
+
+// CCD of a trial candidate (kind 0 VT, 1 EE) whose distance at P1 is dT: equal
+// to vt_ccd / ee_ccd. The step-start distance d0 >= dT - 2E, so the sweep bound
+// (d0 + dT) / 2 - E is at least dT - 2E: when that clears the thickness, the
+// CCD's +inf is known without its closest-point query at P0.
+CSHD double trial_ccd(int kind, const double* P0, const double* P1, double dT, double thickness) {
+  const double E = stencil_rel_motion(P0, P1);
+  if (sweep_clear(dT - 2 * E, dT, E, thickness)) return INFINITY;
+  return kind == 0 ? vt_ccd(P0, P1, thickness, dT, E) : ee_ccd(P0, P1, thickness, dT, E);
 }
 
 CSHD double barrier_value(double d, double dHat) {

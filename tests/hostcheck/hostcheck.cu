@@ -19,6 +19,12 @@ void hc_closest_ee(const double* q, double* o) {
 }
 double hc_vt_ccd(const double* P0, const double* P1, double th) { return cs::vt_ccd(P0, P1, th); }
 double hc_ee_ccd(const double* P0, const double* P1, double th) { return cs::ee_ccd(P0, P1, th); }
+// The trial kernel's gated CCD: distance at P1 first, then trial_ccd.
+double hc_trial_ccd(const double* P0, const double* P1, double th, int kind) {
+  const double dT = kind == 0 ? cs::closest_vt(P1, P1 + 3, P1 + 6, P1 + 9).dist
+                              : cs::closest_ee(P1, P1 + 3, P1 + 6, P1 + 9).dist;
+  return cs::trial_ccd(kind, P0, P1, dT, th);
+}
 int hc_solve_cubic01(double a3, double a2, double a1, double a0, double* o) { return cs::solve_cubic01(a3, a2, a1, a0, o); }
 double hc_barrier_value(double d, double dh) { return cs::barrier_value(d, dh); }
 double hc_barrier_grad(double d, double dh, double k) { return cs::barrier_grad_scalar(d, dh, k, 1); }

@@ -17,14 +17,14 @@ LIB = os.path.join(HERE, "hostcheck", "libhostcheck.so")
 
 @pytest.fixture(scope="module")
 def hc():
-    if not os.path.exists(LIB):
-        subprocess.run(["make", "-s", "-C", os.path.join(HERE, "hostcheck")], check=True)
+    subprocess.run(["make", "-s", "-C", os.path.join(HERE, "hostcheck")], check=True)
     L = C.CDLL(LIB)
     d = C.c_double
     p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
     for name, res, args in [("hc_js_acos", d, [d]), ("hc_js_log", d, [d]), ("hc_js_cbrt", d, [d]),
                             ("hc_hypot3", d, [d, d, d]), ("hc_closest_vt", None, [p, p]),
                             ("hc_closest_ee", None, [p, p]), ("hc_vt_ccd", d, [p, p, d]), ("hc_ee_ccd", d, [p, p, d]),
+                            ("hc_trial_ccd", d, [p, p, d, C.c_int]),
                             ("hc_solve_cubic01", C.c_int, [d, d, d, d, p]), ("hc_barrier_value", d, [d, d]),
                             ("hc_barrier_grad", d, [d, d, d]), ("hc_barrier_curv", d, [d, d, d])]:
         f = getattr(L, name)
@@ -85,6 +85,61 @@ def test_ccd_matches_oracle(hc):
             assert same(c, d), (c, d)
             hits += (0 < a < 1) + (0 < c < 1)
     assert hits > 0
+
+
+def _stencil_dist(P, kind):
+    q = P.reshape(4, 3)
+    o = O.closest_vt(q[0], q[1], q[2], q[3]) if kind == 0 else O.closest_ee(q[0], q[1], q[2], q[3])
+    return float(o[2])
+
+
+def test_trial_ccd_gate_matches_oracle(hc):
+    """The trial kernel's CCD skips the root search when the sweep bound
+    (d0 + dT) / 2 - E, or its lower bound dT - 2E, clears the thickness. It must
+    return exactly the reference's CCD: random stencils, cloth-like near-parallel
+    layers closing in, and thicknesses placed on and around each gate's
+    threshold (relative offsets down to 1e-9)."""
+    rng = np.random.default_rng(11)
+    checked = gated = 0
+
+    def check(P0, P1, th):
+        nonlocal checked
+        for kind, ref in ((0, O.vt_ccd), (1, O.ee_ccd)):
+            a = hc.hc_trial_ccd(P0, P1, th, kind)
+            b = ref(P0, P1, th)
+            assert same(a, b), (kind, th, a, b, P0.tolist(), P1.tolist())
+            checked += 1
+
+    for it in range(1500):
+        if it % 2 == 0:
+            P0, P1 = _random_stencils(rng, 1, 0.01)
+            P0 = np.ascontiguousarray(P0.ravel())
+            P1 = np.ascontiguousarray(P1.ravel())
+        else:
+            # two cloth layers: a triangle and a vertex (or edges) a few dHat apart, closing in
+            h = 4e-3
+            tri = np.array([[0, 0, 0], [h, 0, 0], [0, 0, h]]) + rng.normal(0, 2e-4, (3, 3))
+            top = np.array([h / 3, 0, h / 3]) + rng.normal(0, 2e-4, 3)
+            top[1] = rng.uniform(1e-4, 2e-3)
+            P0 = np.concatenate([top, tri.ravel()]) + rng.uniform(-1, 1)
+            P1 = P0 + rng.normal(0, 1, 12) * 10 ** rng.uniform(-6, -3)
+            P1 += np.tile(rng.normal(0, 1e-2, 3), 4)  # common translation
+        for kind in (0, 1):
+            dT = _stencil_dist(P1, kind)
+            d0 = _stencil_dist(P0, kind)
+            m0 = P1.reshape(4, 3) - P0.reshape(4, 3)
+            E = float(np.max(np.linalg.norm(m0 - m0.mean(axis=0), axis=1)))
+            dev = float(np.max(np.abs(m0 - m0.mean(axis=0))))
+            for crit in (dT - 2 * E, (d0 + dT) / 2 - E, d0 - 4 * dev, d0):
+                if not (crit > 0):
+                    continue
+                for rel in (-1e-5, -1e-7, -1e-9, 0.0, 1e-9, 1e-7, 1e-5):
+                    th = crit * (1 + rel)
+                    gated += dT - 2 * E > th
+                    check(P0, P1, th)
+        for th in (1e-4, 2e-3):
+            check(P0, P1, th)
+    assert checked > 40000 and gated > 1000, (checked, gated)
 
 
 def test_cubic_and_barrier_match_oracle(hc):
