@@ -5,11 +5,13 @@
 // trip through L2 and every SM) with an on-GPC one, and fuses each iteration
 // into two phases:
 //
-//   A  per vertex: p_k = z + beta p_{k-1} formed on the fly for the vertex and
-//      its element neighbours, the membrane HVP of every incident triangle
-//      (corner share only) from the stored FP32 (F, S), the frozen-contact
-//      HVP, Ap = M/h^2 p + H p; partial p.Ap          -- cluster barrier --
-//   B  per Schwarz domain (one warp, lane = local dof) or per dof (Jacobi):
+//   A  per vertex (T lanes splitting its incident triangles): p_k = z + beta
+//      p_{k-1} formed on the fly for the vertex and its element neighbours,
+//      the membrane HVP of every incident triangle (corner share only) from the
+//      stored FP32 (F, S), the frozen-contact HVP, Ap = M/h^2 p + H p; partial
+//      p.Ap                                            -- cluster barrier --
+//   B  per Schwarz domain (one warp, lane = local dof, up to three domains
+//      per warp in flight together) or per dof (Jacobi):
 //      alpha, x += alpha p, r -= alpha Ap, z = M^-1 r; partial r.r and r.z
 //                                                      -- cluster barrier --
 //
@@ -120,46 +122,81 @@ __device__ __forceinline__ double cl_jvp(const Frozen& f, const float* z, const 
   return f.w0 * nv[0] + f.w1 * nv[1] + f.w2 * nv[2] + f.w3 * nv[3];
 }
 
-// Phase B on one Schwarz domain: lane = local dof. Returns (r.r, r.z) shares.
-__device__ __forceinline__ void cl_domain(const Dev& d, const MixBufs& mb, const float* pn, float alpha, bool init,
-                                          int dom, double& rr, double& rz) {
+// Phase B on K Schwarz domains dom0, dom0 + step, ... at once (one warp, lane =
+// local dof): the loads of all K are issued before any product, so their
+// latencies overlap. Adds the (r.r, r.z) shares.
+template <int K>
+__device__ __forceinline__ void cl_domains(const Dev& d, const MixBufs& mb, const float* pn, float alpha, bool init,
+                                           int dom0, int step, double& rr, double& rz) {
   const int lane = threadIdx.x & 31;
-  const int start = d.domStart[dom], dw = (d.domStart[dom + 1] - start) * 3;
-  float rv = 0.f;
-  int gi = -1;
-  bool pin = false;
-  if (lane < dw) {
-    gi = d.domVerts[start + lane / 3] * 3 + lane % 3;
-    pin = d.pinned[gi / 3];
-    float xi, ri;
-    if (init) {
-      xi = 0.f;
-      ri = (float)(-d.g[gi]);
-    } else {
-      xi = mb.x[gi] + alpha * pn[gi];
-      ri = mb.r[gi] - alpha * mb.Ap[gi];
-    }
-    if (pin) { xi = 0.f; ri = 0.f; }
-    mb.x[gi] = xi;
-    mb.r[gi] = ri;
-    rv = ri;
-    rr += (double)ri * ri;
-  }
-  // row `lane` of the 24x24 inverse: 96 bytes, six 16-byte loads
-  const float4* Li = reinterpret_cast<const float4*>(mb.Linv + (size_t)dom * 576) + lane * 6;
-  float z = 0.f;
+  float rv[K];
+  int gi[K];
+  bool pin[K], act[K];
 #pragma unroll
-  for (int j4 = 0; j4 < 6; j4++) {
-    const float4 l = lane < dw ? __ldg(Li + j4) : make_float4(0.f, 0.f, 0.f, 0.f);
-    z = fmaf(l.x, __shfl_sync(0xffffffffu, rv, 4 * j4), z);
-    z = fmaf(l.y, __shfl_sync(0xffffffffu, rv, 4 * j4 + 1), z);
-    z = fmaf(l.z, __shfl_sync(0xffffffffu, rv, 4 * j4 + 2), z);
-    z = fmaf(l.w, __shfl_sync(0xffffffffu, rv, 4 * j4 + 3), z);
+  for (int u = 0; u < K; u++) {
+    const int dom = dom0 + u * step;
+    rv[u] = 0.f;
+    gi[u] = -1;
+    pin[u] = false;
+    act[u] = false;
+    if (dom < d.D) {
+      const int start = d.domStart[dom], dw = (d.domStart[dom + 1] - start) * 3;
+      act[u] = lane < dw;
+      if (act[u]) {
+        gi[u] = d.domVerts[start + lane / 3] * 3 + lane % 3;
+        pin[u] = d.pinned[gi[u] / 3];
+        float xi, ri;
+        if (init) {
+          xi = 0.f;
+          ri = (float)(-d.g[gi[u]]);
+        } else {
+          xi = mb.x[gi[u]] + alpha * pn[gi[u]];
+          ri = mb.r[gi[u]] - alpha * mb.Ap[gi[u]];
+        }
+        if (pin[u]) { xi = 0.f; ri = 0.f; }
+        mb.x[gi[u]] = xi;
+        mb.r[gi[u]] = ri;
+        rv[u] = ri;
+        rr += (double)ri * ri;
+      }
+    }
   }
-  if (lane < dw) {
-    if (pin) z = 0.f;
-    mb.z[gi] = z;
-    rz += (double)rv * z;
+  // row `lane` of each 24x24 inverse: 96 bytes, six 16-byte loads
+  float4 L[K][6];
+#pragma unroll
+  for (int u = 0; u < K; u++) {
+    const float4* Li = reinterpret_cast<const float4*>(mb.Linv + (size_t)(dom0 + u * step) * 576) + lane * 6;
+#pragma unroll
+    for (int j4 = 0; j4 < 6; j4++) L[u][j4] = act[u] ? __ldg(Li + j4) : make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+#pragma unroll
+  for (int u = 0; u < K; u++) {
+    float z = 0.f;
+#pragma unroll
+    for (int j4 = 0; j4 < 6; j4++) {
+      z = fmaf(L[u][j4].x, __shfl_sync(0xffffffffu, rv[u], 4 * j4), z);
+      z = fmaf(L[u][j4].y, __shfl_sync(0xffffffffu, rv[u], 4 * j4 + 1), z);
+      z = fmaf(L[u][j4].z, __shfl_sync(0xffffffffu, rv[u], 4 * j4 + 2), z);
+      z = fmaf(L[u][j4].w, __shfl_sync(0xffffffffu, rv[u], 4 * j4 + 3), z);
+    }
+    if (act[u]) {
+      if (pin[u]) z = 0.f;
+      mb.z[gi[u]] = z;
+      rz += (double)rv[u] * z;
+    }
+  }
+}
+
+// Phase B over every domain, K = ceil(D / warps) (at most 3) per warp at once.
+__device__ __forceinline__ void cl_all_domains(const Dev& d, const MixBufs& mb, const float* pn, float alpha,
+                                               bool init, int gwarp, int nwarps, double& rr, double& rz) {
+  const int per = (d.D + nwarps - 1) / nwarps;
+  if (per <= 1) {
+    if (gwarp < d.D) cl_domains<1>(d, mb, pn, alpha, init, gwarp, nwarps, rr, rz);
+  } else if (per == 2) {
+    cl_domains<2>(d, mb, pn, alpha, init, gwarp, nwarps, rr, rz);
+  } else {
+    for (int dom = gwarp; dom < d.D; dom += 3 * nwarps) cl_domains<3>(d, mb, pn, alpha, init, dom, nwarps, rr, rz);
   }
 }
 
@@ -203,6 +240,10 @@ __global__ void __launch_bounds__(kClT, 1) k_mx_pcg_cluster(ClArgs A) {
   const bool jacobi = d.precond == 0;
   const float invH2 = (float)d.invH2;
   const float C00 = mb.C00, C11 = mb.C11, C01 = mb.C01, G = mb.G;
+  // lanes per vertex in phase A: 4, 2 or 1 as the cluster's threads allow
+  const int T = nth >= 4 * d.n ? 4 : nth >= 2 * d.n ? 2 : 1;
+  const int lane = threadIdx.x & (T - 1);
+  const int vStride = nth / T, vRounds = (d.n + vStride - 1) / vStride;
 
   // ---- init: r = -g (filtered), x = 0, z = M^-1 r; |b|^2, r.r, r.z -------------------
   double bb = 0, rr = 0, rz = 0;
@@ -213,7 +254,7 @@ __global__ void __launch_bounds__(kClT, 1) k_mx_pcg_cluster(ClArgs A) {
   if (jacobi) {
     for (int i = tid; i < n3; i += nth) cl_dof(d, mb, nullptr, 0.f, true, i, rr, rz);
   } else {
-    for (int dom = gwarp; dom < d.D; dom += nwarps) cl_domain(d, mb, nullptr, 0.f, true, dom, rr, rz);
+    cl_all_domains(d, mb, nullptr, 0.f, true, gwarp, nwarps, rr, rz);
   }
   if (d.hasContact) {
     const Contact& c = d.c;
@@ -243,23 +284,53 @@ __global__ void __launch_bounds__(kClT, 1) k_mx_pcg_cluster(ClArgs A) {
   int k = 0;
   for (; !done && k < A.maxIters; k++) {
     // ---- phase A: p_k, Ap_k, p.Ap ------------------------------------------------
+    // T consecutive lanes share a vertex and split its incident records; each
+    // lane issues the loads of up to three records before using any, so the
+    // gathers overlap. The T shares are summed with a fixed xor tree.
     double pAp = 0;
-    for (int v = tid; v < d.n; v += nth) {
-      const float3 pv = ld_p(mb.z, pc, beta, first, v);
+    for (int it = 0; it < vRounds; it++) {
+      const int v = tid / T + it * vStride;
+      const bool valid = v < d.n;
       float sp[3] = {0.f, 0.f, 0.f};
-      const uint32_t q0 = d.memOff[v], q1 = d.memOff[v + 1];
-      for (uint32_t q = q0; q < q1; q++) {
-        // record q = (triangle << 2 | corner): state + vertex ids, read contiguously
-        const float4* R = mb.vrec + (size_t)q * 5;
-        const float4 ids = __ldg(R + 4);
-        const int corner = __float_as_int(ids.w);
-        const float3 p0 = ld_p(mb.z, pc, beta, first, __float_as_int(ids.x));
-        const float3 p1 = ld_p(mb.z, pc, beta, first, __float_as_int(ids.y));
-        const float3 p2 = ld_p(mb.z, pc, beta, first, __float_as_int(ids.z));
-        float o[3];
-        tri_hvp_corner(reinterpret_cast<const float*>(R), p0, p1, p2, corner, C00, C11, C01, G, o);
-        sp[0] += o[0]; sp[1] += o[1]; sp[2] += o[2];
+      if (valid) {
+        const uint32_t q1 = d.memOff[v + 1];
+        for (uint32_t qb = d.memOff[v] + lane; qb < q1; qb += 3 * T) {
+          float4 ids[3];
+#pragma unroll
+          for (int u = 0; u < 3; u++) {
+            const uint32_t q = qb + u * T;
+            // record q = (triangle << 2 | corner): state + vertex ids, read contiguously
+            ids[u] = q < q1 ? __ldg(mb.vrec + (size_t)q * 5 + 4) : make_float4(0.f, 0.f, 0.f, 0.f);
+          }
+          float3 P[3][3];
+#pragma unroll
+          for (int u = 0; u < 3; u++) {
+            if (qb + u * T < q1) {
+              P[u][0] = ld_p(mb.z, pc, beta, first, __float_as_int(ids[u].x));
+              P[u][1] = ld_p(mb.z, pc, beta, first, __float_as_int(ids[u].y));
+              P[u][2] = ld_p(mb.z, pc, beta, first, __float_as_int(ids[u].z));
+            }
+          }
+#pragma unroll
+          for (int u = 0; u < 3; u++) {
+            const uint32_t q = qb + u * T;
+            if (q < q1) {
+              float o[3];
+              tri_hvp_corner(reinterpret_cast<const float*>(mb.vrec + (size_t)q * 5), P[u][0], P[u][1], P[u][2],
+                             __float_as_int(ids[u].w), C00, C11, C01, G, o);
+              sp[0] += o[0]; sp[1] += o[1]; sp[2] += o[2];
+            }
+          }
+        }
       }
+#pragma unroll
+      for (int o = 1; o < T; o <<= 1) {
+        sp[0] += __shfl_xor_sync(0xffffffffu, sp[0], o);
+        sp[1] += __shfl_xor_sync(0xffffffffu, sp[1], o);
+        sp[2] += __shfl_xor_sync(0xffffffffu, sp[2], o);
+      }
+      if (!valid || lane != 0) continue;
+      const float3 pv = ld_p(mb.z, pc, beta, first, v);
       double ch[3] = {0, 0, 0};
       if (d.hasContact) {
         const Contact& c = d.c;
@@ -297,7 +368,7 @@ __global__ void __launch_bounds__(kClT, 1) k_mx_pcg_cluster(ClArgs A) {
     if (jacobi) {
       for (int i = tid; i < n3; i += nth) cl_dof(d, mb, pn, alpha, false, i, rr, rz);
     } else {
-      for (int dom = gwarp; dom < d.D; dom += nwarps) cl_domain(d, mb, pn, alpha, false, dom, rr, rz);
+      cl_all_domains(d, mb, pn, alpha, false, gwarp, nwarps, rr, rz);
     }
     {
       const double v2[2] = {rr, rz};
