@@ -178,43 +178,49 @@ __device__ __forceinline__ void cand_rec(const CView& v, int i, int* r) {
 // Distance of every candidate (for the minima) and the order keys of the active
 // ones, appended through a warp-aggregated counter (cint[CI_NCAND]): their
 // positions are arbitrary, the radix sort that follows imposes the reference's
-// (kind, p, a, b, c, d) order, and equal keys are identical records. Ccap bounds
-// the candidate count from the host; slots past the device count get +inf.
-__global__ void k_cand_flags(CView v, const double* x, int Ccap, Key<4>* keys, uint32_t* pay) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  bool act = false;
-  CandKey k{0, 0};
+// (kind, p, a, b, c, d) order, and equal keys are identical records. The grid
+// strides over the candidate count on the device; keys past `cap` are counted
+// but not stored (the host grows the buffers and repeats the query).
+__global__ void __launch_bounds__(kCT) k_cand_flags(CView v, const double* x, int cap, Key<4>* keys, uint32_t* pay) {
+  const int total = cand_count(v);
   double dmin = INFINITY;
-  if (i < Ccap && i < cand_count(v)) {
-    int r[6];
-    cand_rec(v, i, r);
-    if (r[0] != 3) {
-      Closest cp;
-      cand_closest(v, x, r, cp);
-      act = !(cp.dist >= v.c.dHat || cp.dist < 1e-12);
-      if (cp.dist < dmin) dmin = cp.dist;
-      if (act) {
-        k = cand_key(r, v.ns, v.idBits, 0, 0);
-        if (r[0] == 0) atomicAdd(&v.cint[CI_NVT], 1);
+  for (int base = blockIdx.x * blockDim.x; base < total; base += gridDim.x * blockDim.x) {
+    const int i = base + threadIdx.x;
+    bool act = false;
+    CandKey k{0, 0};
+    if (i < total) {
+      int r[6];
+      cand_rec(v, i, r);
+      if (r[0] != 3) {
+        Closest cp;
+        cand_closest(v, x, r, cp);
+        act = !(cp.dist >= v.c.dHat || cp.dist < 1e-12);
+        if (cp.dist < dmin) dmin = cp.dist;
+        if (act) {
+          k = cand_key(r, v.ns, v.idBits, 0, 0);
+          if (r[0] == 0) atomicAdd(&v.cint[CI_NVT], 1);
+        }
+      }
+    }
+    const uint32_t mask = __ballot_sync(0xffffffffu, act);
+    if (!mask) continue;
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(mask) - 1;
+    uint32_t pbase = 0;
+    if (lane == leader) pbase = atomicAdd((uint32_t*)&v.cint[CI_NCAND], (uint32_t)__popc(mask));
+    pbase = __shfl_sync(0xffffffffu, pbase, leader);
+    if (act) {
+      const uint32_t pos = pbase + __popc(mask & ((1u << lane) - 1u));
+      if (pos < (uint32_t)cap) {
+        keys[pos].w[0] = (uint32_t)(k.hi >> 32);
+        keys[pos].w[1] = (uint32_t)k.hi;
+        keys[pos].w[2] = (uint32_t)(k.lo >> 32);
+        keys[pos].w[3] = (uint32_t)k.lo;
+        pay[pos] = (uint32_t)i;
       }
     }
   }
   block_min_into(dmin, INFINITY, &v.omin[2], nullptr);
-  const uint32_t mask = __ballot_sync(0xffffffffu, act);
-  if (!mask) return;
-  const int lane = threadIdx.x & 31;
-  const int leader = __ffs(mask) - 1;
-  uint32_t base = 0;
-  if (lane == leader) base = atomicAdd((uint32_t*)&v.cint[CI_NCAND], (uint32_t)__popc(mask));
-  base = __shfl_sync(0xffffffffu, base, leader);
-  if (act) {
-    const uint32_t pos = base + __popc(mask & ((1u << lane) - 1u));
-    keys[pos].w[0] = (uint32_t)(k.hi >> 32);
-    keys[pos].w[1] = (uint32_t)k.hi;
-    keys[pos].w[2] = (uint32_t)(k.lo >> 32);
-    keys[pos].w[3] = (uint32_t)k.lo;
-    pay[pos] = (uint32_t)i;
-  }
 }
 
 // Floor flags, and the floor distances folded into the active-set minimum
@@ -274,6 +280,7 @@ __global__ void k_active_reset(CView v) {
   v.omin[2] = kOrdInf;
 }
 __global__ void k_active_min(CView v) {
+  if (v.cint[CI_MOVED]) return;  // the query is repeated on a rebuilt superset
   const double m = dbl_of(v.omin[2]);
   if (m < v.diag->minDistance) v.diag->minDistance = m;
 }
@@ -553,23 +560,26 @@ __device__ __forceinline__ void trial_one(const CView& v, const double* xt, int 
 
 // checkTrial's candidate loops (contact-assembly.ts:498-535): exact distances at
 // the trial, CCD of the segment, and their minima.
-__global__ void __launch_bounds__(kCT) k_trial_cand(CView v, const double* xt, int Ccap, double dMin) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  double d = INFINITY, t = INFINITY, dOut = INFINITY, tOut = INFINITY;
-  if (i < Ccap && i < cand_count(v)) trial_one(v, xt, i, dMin, dOut, tOut);
-  if (dOut < d) d = dOut;
-  if (tOut < t) t = tOut;
+__global__ void __launch_bounds__(kCT) k_trial_cand(CView v, const double* xt, double dMin) {
+  const int total = cand_count(v);
+  double d = INFINITY, t = INFINITY;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+    double dOut = INFINITY, tOut = INFINITY;
+    trial_one(v, xt, i, dMin, dOut, tOut);
+    if (dOut < d) d = dOut;
+    if (tOut < t) t = tOut;
+  }
   block_min_into(d, t, &v.omin[0], &v.omin[1]);
 }
 
 // Second half of the smallest failing (key, status): the low word among the
 // failing candidates whose high word is the minimum. Walks the list of failing
 // indices, or every candidate when more failed than the list holds.
-__global__ void k_trial_bad_lo(CView v, int C) {
+__global__ void k_trial_bad_lo(CView v) {
   const int nbad = v.cint[CI_NBAD];
   if (nbad == 0) return;
   const bool listed = nbad <= kBadCap;
-  const int cnt = listed ? nbad : C;
+  const int cnt = listed ? nbad : cand_count(v);
   for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < cnt; j += gridDim.x * blockDim.x) {
     const int i = listed ? v.badList[j] : j;
     const uint32_t st = v.cflag[i];
@@ -601,6 +611,10 @@ __global__ void k_trial_floor(CView v, const double* xt, double dMin) {
 __global__ void k_trial_final(CView v, double dMin) {
   const double minDist = dbl_of(v.omin[0]);
   const double minTOI = dbl_of(v.omin[1]);
+  if (v.cint[CI_MOVED]) {  // the query is repeated on a rebuilt superset
+    v.cint[CI_VALID] = -1;
+    return;
+  }
   int valid = 0;
   DevDiag* dg = v.diag;
   if (v.cint[CI_FIRSTNF] != INT_MAX) {
@@ -859,6 +873,12 @@ void ContactHost::init(Solver& s, const cs_contact_params* prm, int floor_on, do
   CK(cudaMallocHost(&hdiag, sizeof(DevDiag)));
   ensure_pairs(1024, 64);
   ensure_cands(1024);
+  ensure_flags(1024);
+  {
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&smCount, cudaDevAttrMultiProcessorCount, dev));
+  }
   ensure_active(s, std::max(1024, n + 64));
   ensure_lag(1024);
   bvh.flags = cint + CI_OVERFLOW;
@@ -878,7 +898,11 @@ void ContactHost::ensure_cands(size_t nc) {
   dalloc(cand.p0, c);
   dalloc(cand.p1, c);
   dalloc(cand.hist, 256 * ((c + kSortTile - 1) / kSortTile) + 1);
-  dalloc(cflag, c + 1);
+}
+void ContactHost::ensure_flags(size_t nc) {
+  if (nc + 1 <= flagCap) return;
+  flagCap = nc + nc / 2 + 256;
+  dalloc(cflag, flagCap);
 }
 void ContactHost::ensure_active(Solver& s, size_t na) {
   if (na <= actCap) return;
@@ -974,10 +998,22 @@ void ContactHost::build_superset(Solver& s, const double* x, double padSup) {
     if (S > supSCap) { supSCap = S + S / 2 + 64; dalloc(supSPairs, supSCap); }
   }
   ensure_pairs((size_t)nSup, (size_t)nSupS);
+  const size_t bound = 15 * (size_t)nSup + 12 * (size_t)nSupS;
+  if (bound > (size_t)INT_MAX / 8) throw CapacityError("too many contact candidates");
+  ensure_flags(bound);
   CK(cudaMemsetAsync(cint, 0, CI_N * sizeof(int), st));
 }
 
-int ContactHost::build_candidates(Solver& s, const double* x, double pad) {
+// Launches one broadphase query (no host synchronization): the pairs of the
+// segment xStep -> x padded by `pad`, counted on the device (cint[CI_SELF],
+// cint[CI_STATIC]). Queries filter a superset of pairs built for the segment
+// x0 -> xBase with the pad widened by kSupTravel: a query whose positions all
+// stay within kSupTravel (max norm) of xBase has its swept boxes inside the
+// superset's, so filtering the superset by the query's own f64 boxes gives
+// exactly the pairs a traversal would. A query that moved further raises
+// cint[CI_MOVED]; the kernels that follow then leave no trace, and the caller
+// rebuilds the superset around the query and repeats it.
+void ContactHost::launch_query(Solver& s, const double* x, double pad) {
   struct Restore {
     Solver& s;
     int prev;
@@ -990,61 +1026,53 @@ int ContactHost::build_candidates(Solver& s, const double* x, double pad) {
   } restore{s, s.phase(PH_BROADPHASE)};
   cudaStream_t st = s.stream;
   int64_t& lc = launch_counter();
-  CK(cudaMemsetAsync(cint, 0, CI_N * sizeof(int), st));
-  // Queries filter a superset of pairs built for the segment x0 -> xBase with
-  // the pad widened by kSupTravel. A query whose positions all stay within
-  // kSupTravel (max norm) of xBase has its swept boxes inside the superset's,
-  // so filtering the superset by the query's own f64 boxes gives exactly the
-  // pairs a traversal would; otherwise the superset is rebuilt around the
-  // query. The buffers sized for the superset always hold a query, and the
-  // exact counts are read back so every later kernel runs over the query only.
-  const double padSup = std::max(p.dhat, p.dmin) + kSupTravel + 1e-9;
   if (!supValid) {
-    build_superset(s, x, padSup);
+    build_superset(s, x, sup_pad());
     supValid = true;
   }
-  for (int attempt = 0; attempt < 2; attempt++) {
-    const int n3 = 3 * n;
-    k_moved<<<std::min(1184, (n3 + 255) / 256), 256, 0, st>>>(x, supBase, n3, kSupTravel, cint);
-    bvh_boxes(bvh, s.d.x0, x, pad, st, &lc);
-    filter_pairs(bvh, supPairs, nSup, bvh.pairs, (uint32_t)pairCap, (uint32_t*)(cint + CI_SELF), supSPairs, nSupS,
-                 pad, spairs, (uint32_t)spairCap, (uint32_t*)(cint + CI_STATIC), st, &lc);
-    lc++;
-    read_ints(s);
-    if (!hint[CI_MOVED]) break;
-    if (attempt == 1) throw CapacityError("broadphase superset rebuilt around the query does not cover it");
-    build_superset(s, x, padSup);
-  }
-  const int P = hint[CI_SELF], S = ms > 0 ? hint[CI_STATIC] : 0;
-  const long C = 15l * P + 12l * S;
-  if (C > INT_MAX / 8) throw CapacityError("too many contact candidates");
-  ensure_cands(C);
-  return (int)C;
+  CK(cudaMemsetAsync(cint, 0, CI_N * sizeof(int), st));
+  const int n3 = 3 * n;
+  k_moved<<<std::min(1184, (n3 + 255) / 256), 256, 0, st>>>(x, supBase, n3, kSupTravel, cint);
+  bvh_boxes(bvh, s.d.x0, x, pad, st, &lc);
+  filter_pairs(bvh, supPairs, nSup, bvh.pairs, (uint32_t)pairCap, (uint32_t*)(cint + CI_SELF), supSPairs, nSupS,
+               pad, spairs, (uint32_t)spairCap, (uint32_t*)(cint + CI_STATIC), st, &lc);
+  lc++;
+}
+
+// Blocks for the grid-stride candidate kernels: enough for the superset's
+// bound, at most 8 per SM.
+int ContactHost::cand_blocks() const {
+  const long bound = 15l * nSup + 12l * nSupS;
+  return (int)std::max(1l, std::min((bound + kCT - 1) / kCT, 8l * smCount));
 }
 
 void ContactHost::update_active_set(Solver& s, double* x) {
   cudaStream_t st = s.stream;
   int64_t& lc = launch_counter();
-  const int C = build_candidates(s, x, p.dhat);  // an upper bound; the exact count is on the device
-  CView v = view(*this, s);
-  k_active_reset<<<1, 1, 0, st>>>(v);
-  lc++;
-  if (C > 0) {
-    k_cand_flags<<<cnb(C), kCT, 0, st>>>(v, x, C, cand.k0, cand.p0);
-    lc++;
+  // One host read per query: the counts, and whether the superset covered it.
+  for (int attempt = 0;; attempt++) {
+    launch_query(s, x, p.dhat);
+    CView v = view(*this, s);
+    k_active_reset<<<1, 1, 0, st>>>(v);
+    k_cand_flags<<<cand_blocks(), kCT, 0, st>>>(v, x, cand.cap, cand.k0, cand.p0);
+    k_floor_flags<<<cnb(n), kCT, 0, st>>>(v, x);
+    k_active_min<<<1, 1, 0, st>>>(v);
+    lc += 4;
+    scan_counts(fflag, n, (uint32_t*)(cint + CI_NFLOOR), st, &lc);
+    read_ints(s);
+    const bool moved = hint[CI_MOVED] != 0, overflow = hint[CI_NCAND] > cand.cap;
+    if (!moved && !overflow) break;
+    if (attempt >= 2) throw CapacityError("active-set query repeated without settling");
+    if (moved) build_superset(s, x, sup_pad());
+    if (overflow) ensure_cands((size_t)hint[CI_NCAND]);
   }
-  k_floor_flags<<<cnb(n), kCT, 0, st>>>(v, x);
-  k_active_min<<<1, 1, 0, st>>>(v);
-  lc += 2;
-  scan_counts(fflag, n, (uint32_t*)(cint + CI_NFLOOR), st, &lc);
-  read_ints(s);
   candidatePairs = 15.0 * (uint32_t)hint[CI_SELF] + 12.0 * (uint32_t)(ms > 0 ? hint[CI_STATIC] : 0);
   nCand = hint[CI_NCAND];
   nFloor = hint[CI_NFLOOR];
   nVT = hint[CI_NVT];
   const int na = nCand + nFloor;
   ensure_active(s, na);
-  v = view(*this, s);
+  CView v = view(*this, s);
   if (nCand > 0) {
     // Only the active candidates are put in the reference's (kind, p, a, b, c, d) order.
     const bool flip = radix_sort<4>(cand.k0, cand.p0, cand.k1, cand.p1, nCand, cand_key_bits(idBits, 0), cand.hist,
@@ -1106,24 +1134,49 @@ void ContactHost::merit_energy(Solver& s, const double* x) {
   launch_counter()++;
 }
 
-bool ContactHost::check_trial(Solver& s, const double* xt) {
+// checkTrial (contact-assembly.ts:489-553) launched without a host read: the
+// candidate and floor kernels, then an asynchronous copy of the counters that
+// trial_result reads after the caller's next synchronization.
+void ContactHost::trial_launch(Solver& s, const double* xt) {
   cudaStream_t st = s.stream;
   int64_t& lc = launch_counter();
-  const int C = build_candidates(s, xt, p.dmin);  // an upper bound; the exact count is on the device
+  launch_query(s, xt, p.dmin);
   CView v = view(*this, s);
   k_trial_reset<<<1, 1, 0, st>>>(v);
-  lc++;
-  if (C > 0) {
-    k_trial_cand<<<cnb(C), kCT, 0, st>>>(v, xt, C, p.dmin);
-    k_trial_bad_lo<<<std::min(cnb(C), 4 * 148), kCT, 0, st>>>(v, C);
-    lc += 2;
-  }
+  k_trial_cand<<<cand_blocks(), kCT, 0, st>>>(v, xt, p.dmin);
+  k_trial_bad_lo<<<4 * smCount, kCT, 0, st>>>(v);
   k_trial_floor<<<cnb(n), kCT, 0, st>>>(v, xt, p.dmin);
   k_trial_final<<<1, 1, 0, st>>>(v, p.dmin);
-  lc += 2;
-  read_ints(s);
+  lc += 5;
+  CK(cudaMemcpyAsync(hint, cint, CI_N * sizeof(int), cudaMemcpyDeviceToHost, st));
+}
+
+// After a synchronization: 1 valid, 0 invalid, -1 when the query fell outside
+// the superset (nothing was recorded; rebuild and repeat).
+int ContactHost::trial_result() {
   candidatePairs = 15.0 * (uint32_t)hint[CI_SELF] + 12.0 * (uint32_t)(ms > 0 ? hint[CI_STATIC] : 0);
-  return hint[CI_VALID] != 0;
+  return hint[CI_VALID];
+}
+
+// A trial whose query fell outside the superset: rebuild around it and check again.
+bool ContactHost::trial_redo(Solver& s, const double* xt) {
+  build_superset(s, xt, sup_pad());
+  trial_launch(s, xt);
+  CK(cudaStreamSynchronize(s.stream));
+  const int r = trial_result();
+  if (r < 0) throw CapacityError("broadphase superset rebuilt around the query does not cover it");
+  return r != 0;
+}
+
+bool ContactHost::check_trial(Solver& s, const double* xt) {
+  for (int attempt = 0;; attempt++) {
+    trial_launch(s, xt);
+    CK(cudaStreamSynchronize(s.stream));
+    const int r = trial_result();
+    if (r >= 0) return r != 0;
+    if (attempt >= 1) throw CapacityError("broadphase superset rebuilt around the query does not cover it");
+    build_superset(s, xt, sup_pad());
+  }
 }
 
 void ContactHost::commit(Solver& s, const double* x) {

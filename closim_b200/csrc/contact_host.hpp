@@ -4,6 +4,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <stdexcept>
 #include <vector>
@@ -67,7 +68,9 @@ class ContactHost {
   void build_superset(Solver& s, const double* x, double padSup);
   size_t pairCap = 0, spairCap = 0;
   CandBufs cand;
-  uint32_t* cflag = nullptr;   // per-candidate flag / offset / trial status (cand cap + 1)
+  uint32_t* cflag = nullptr;   // per-candidate trial status (flagCap, the superset's candidate bound + 1)
+  size_t flagCap = 0;
+  int smCount = 148;
   uint32_t* fflag = nullptr;   // per-vertex floor flag / offset (n + 1)
   unsigned long long* omin = nullptr;  // ordered images of the trial / active-set minima (3)
   int* badList = nullptr;      // failing trial candidates (kBadCap)
@@ -111,17 +114,26 @@ class ContactHost {
   void update_active_set(Solver& s, double* x);
   void merit_energy(Solver& s, const double* x);
   void gradient_terms(Solver& s);
+  // Trial validity with one host synchronization (bisection, commit).
   bool check_trial(Solver& s, const double* xt);
+  // The same split around the caller's own synchronization: trial_launch
+  // enqueues the check and the copy of its counters, trial_result reads them.
+  void trial_launch(Solver& s, const double* xt);
+  int trial_result();
+  bool trial_redo(Solver& s, const double* xt);
   void commit(Solver& s, const double* x);
   void kill_approach_velocity(Solver& s);
   void fill_stats(Solver& s, cs_step_stats& st);
-  // broadphase stage only: candidate count for a segment xStep -> x with pad
-  int build_candidates(Solver& s, const double* x, double pad);
+  // broadphase stage only: the pairs of a segment xStep -> x with pad, counted on the device
+  void launch_query(Solver& s, const double* x, double pad);
   void bind(Solver& s);  // refresh the Contact view inside the solver's Dev
  private:
   void read_ints(Solver& s);
   void ensure_pairs(size_t np, size_t nsp);
   void ensure_cands(size_t nc);
+  void ensure_flags(size_t nc);
+  int cand_blocks() const;
+  double sup_pad() const { return std::max(p.dhat, p.dmin) + kSupTravel + 1e-9; }
   void ensure_active(Solver& s, size_t na);
   void ensure_lag(size_t nl);
 };

@@ -414,15 +414,23 @@ class Solver {
         phase(PH_TRIAL);
         launch_trial(d, alpha, stream);
         lc += 1 + (d.npins > 0);
-        if (contact && !contact->check_trial(*this, d.xt)) {
-          contact->rejections++;
-          alpha *= 0.5;
-          continue;
-        }
+        // The trial's validity check and its energy are enqueued together and
+        // read with one synchronization; the energy has no side effects and is
+        // used only when the trial is valid, as in the reference.
+        if (contact) contact->trial_launch(*this, d.xt);
         phase(PH_ENERGY);
         if (contact) contact->merit_energy(*this, d.xt);
         energy_of(d.xt);
         read_scalars();
+        if (contact) {
+          int r = contact->trial_result();
+          if (r < 0) r = contact->trial_redo(*this, d.xt) ? 1 : 0;
+          if (!r) {
+            contact->rejections++;
+            alpha *= 0.5;
+            continue;
+          }
+        }
         if (!haveSlope) {
           gtdx = hscal[S_GTDX];
           pcgTotal += (int)hscal[S_PCG_ITERS];
