@@ -805,7 +805,7 @@ ContactHost::~ContactHost() {
                    (void**)&cand.k0, (void**)&cand.k1, (void**)&cand.p0, (void**)&cand.p1, (void**)&cand.hist,
                    (void**)&cflag, (void**)&fflag, (void**)&omin, (void**)&badList, (void**)&active, (void**)&dd,
                    (void**)&cg, (void**)&tc, (void**)&tf, (void**)&rk0, (void**)&rk1, (void**)&rp0, (void**)&rp1,
-                   (void**)&rhist, (void**)&kpred, (void**)&cOff, (void**)&lagFloor, (void**)&lagFloorOk, (void**)&lk0,
+                   (void**)&rhist, (void**)&kpred, (void**)&recScratch, (void**)&cOff, (void**)&lagFloor, (void**)&lagFloorOk, (void**)&lk0,
                    (void**)&lk1, (void**)&lp0, (void**)&lp1, (void**)&lhist, (void**)&lval, (void**)&lsorted,
                    (void**)&probe, (void**)&diag, (void**)&cint, (void**)&supPairs,
                    (void**)&supSPairs, (void**)&supBase})
@@ -919,6 +919,7 @@ void ContactHost::ensure_active(Solver& s, size_t na) {
   dalloc(rp1, 4 * c);
   dalloc(rhist, 256 * ((4 * c + kSortTile - 1) / kSortTile) + 1);
   dalloc(kpred, 4 * c);
+  dalloc(recScratch, 12 * c);
   (void)s;
 }
 void ContactHost::ensure_lag(size_t nl) {
@@ -962,6 +963,7 @@ void ContactHost::bind(Solver& s) {
   c.cg = cg;
   c.cOff = cOff;
   c.cRec = rp0;
+  c.recScratch = recScratch;
   s.d.Tc = tc;
   s.d.hasContact = 1;
 }

@@ -291,6 +291,28 @@ __global__ void __launch_bounds__(kClT, 1) k_mx_pcg_cluster(ClArgs A) {
     for (int it = 0; it < vRounds; it++) {
       const int v = tid / T + it * vStride;
       const bool valid = v < d.n;
+      if (d.hasContact) {
+        // Frozen-contact shares of this CTA's vertices [v0, v1) for this round,
+        // one record per thread (a vertex may sit in many contacts), written to
+        // the record scratch and summed per vertex below in record order. Later
+        // rounds cover other vertices, hence other records; the next iteration
+        // rewrites these only after two cluster barriers.
+        const Contact& c = d.c;
+        const int v0 = min(d.n, rank * (kClT / T) + it * vStride), v1 = min(d.n, v0 + kClT / T);
+        const uint32_t r0 = c.cOff[v0], r1 = c.cOff[v1];
+        for (uint32_t q = r0 + threadIdx.x; q < r1; q += blockDim.x) {
+          const uint32_t rec = c.cRec[q];
+          const double g = A.coef[rec >> 2];
+          double ch[3] = {0, 0, 0};
+          if (g != 0) {
+            const Frozen f = c.active[rec >> 2];
+            dist_grad_slot(f, rec & 3, g * cl_jvp(f, mb.z, pc, beta, first), ch);
+          }
+          double* o = c.recScratch + (size_t)q * 3;
+          o[0] = ch[0]; o[1] = ch[1]; o[2] = ch[2];
+        }
+        __syncthreads();
+      }
       float sp[3] = {0.f, 0.f, 0.f};
       if (valid) {
         const uint32_t q1 = d.memOff[v + 1];
@@ -335,11 +357,8 @@ __global__ void __launch_bounds__(kClT, 1) k_mx_pcg_cluster(ClArgs A) {
       if (d.hasContact) {
         const Contact& c = d.c;
         for (uint32_t q = c.cOff[v]; q < c.cOff[v + 1]; q++) {
-          const uint32_t rec = c.cRec[q];
-          const double g = A.coef[rec >> 2];
-          if (g == 0) continue;
-          const Frozen f = c.active[rec >> 2];
-          dist_grad_slot(f, rec & 3, g * cl_jvp(f, mb.z, pc, beta, first), ch);
+          const double* o = c.recScratch + (size_t)q * 3;
+          ch[0] += o[0]; ch[1] += o[1]; ch[2] += o[2];
         }
       }
       const float M = d.mass[v];
