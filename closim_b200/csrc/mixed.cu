@@ -72,61 +72,70 @@ __global__ void __launch_bounds__(kThreads) k_mx_h9(Dev d, MixBufs mb) {
 
 // Schwarz factor: assemble (FP64 sums of the stored blocks + Jacobi diagonal),
 // symmetrize, Cholesky; store A^-1 = L^-T L^-1 as FP32 (Jacobi inverse on failure).
+// One warp per domain, lane = local dof:
+// - assembly: lane (vertex, component) owns one row and adds its incident
+//   triangles' block rows in incidence order;
+// - right-looking Cholesky: per pivot, every row below scales its entry and
+//   updates its own part of the trailing lower triangle, in parallel;
+// - L^-1 column by column (lane = column) by forward substitution in registers;
+// - A^-1 row by row (lane = row).
+// Rows are padded to 25 doubles so a column read by the warp spreads over banks.
 constexpr int kMxWarps = 4;
+constexpr int kFS = 25;
 __global__ void __launch_bounds__(kMxWarps * 32) k_mx_schwarz_factor(Dev d, MixBufs mb) {
-  __shared__ double A[kMxWarps][24 * 24];
+  __shared__ double A[kMxWarps][24 * kFS];
+  __shared__ int dvs[kMxWarps][8];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int dom = blockIdx.x * kMxWarps + wib;
   if (dom >= d.D) return;
   double* a = A[wib];
   const int start = d.domStart[dom], dv = d.domStart[dom + 1] - start, dw = dv * 3;
-  for (int i = lane; i < 24 * 24; i += 32) a[i] = 0;
+  for (int i = lane; i < 24 * kFS; i += 32) a[i] = 0;
+  if (lane < dv) dvs[wib][lane] = d.domVerts[start + lane];
   __syncwarp();
-  if (lane < dv) {
-    const int v = d.domVerts[start + lane];
+  if (lane < dw) {
+    const int lv = lane / 3, aa = lane % 3;
+    const int v = dvs[wib][lv];
+    double* row = a + lane * kFS;
     for (int k = d.v2tOff[v]; k < d.v2tOff[v + 1]; k++) {
       const int t = d.v2t[k];
       const int cvs[3] = {(int)d.idx[t * 3], (int)d.idx[t * 3 + 1], (int)d.idx[t * 3 + 2]};
       const int ci = cvs[0] == v ? 0 : cvs[1] == v ? 1 : 2;
-      const float* h = mb.h9 + (size_t)t * 81;
+      const float* h = mb.h9 + (size_t)t * 81 + (ci * 3 + aa) * 9;
       for (int cj = 0; cj < 3; cj++) {
         int lw = -1;
         for (int q = 0; q < dv; q++)
-          if (d.domVerts[start + q] == cvs[cj]) { lw = q; break; }
+          if (dvs[wib][q] == cvs[cj]) { lw = q; break; }
         if (lw < 0) continue;
-        for (int aa = 0; aa < 3; aa++)
-          for (int bb = 0; bb < 3; bb++) a[(lane * 3 + aa) * dw + lw * 3 + bb] += h[(ci * 3 + aa) * 9 + cj * 3 + bb];
+        for (int bb = 0; bb < 3; bb++) row[lw * 3 + bb] += h[cj * 3 + bb];
       }
     }
+    row[lane] += d.diag[v * 3 + aa];
   }
-  __syncwarp();
-  if (lane < dw) a[lane * dw + lane] += d.diag[d.domVerts[start + lane / 3] * 3 + lane % 3];
   __syncwarp();
   for (int i = lane; i < dw; i += 32)
     for (int j = i + 1; j < dw; j++) {
-      const double s = 0.5 * (a[i * dw + j] + a[j * dw + i]);
-      a[i * dw + j] = s;
-      a[j * dw + i] = s;
+      const double sv = 0.5 * (a[i * kFS + j] + a[j * kFS + i]);
+      a[i * kFS + j] = sv;
+      a[j * kFS + i] = sv;
     }
   __syncwarp();
   double scale = 0;
-  for (int i = 0; i < dw; i++) scale = fmax(scale, fabs(a[i * dw + i]));
+  for (int i = 0; i < dw; i++) scale = fmax(scale, fabs(a[i * kFS + i]));
   const double tiny = 1e-20 * (1 + scale);
   bool ok = true;
   for (int k = 0; k < dw; k++) {
-    if (lane == 0) {
-      double sum = a[k * dw + k];
-      for (int s = 0; s < k; s++) sum -= a[k * dw + s] * a[k * dw + s];
-      ok = sum > tiny;
-      if (ok) a[k * dw + k] = sqrt(sum);
-    }
-    ok = __shfl_sync(0xffffffffu, ok, 0);
-    __syncwarp();
+    const double piv = a[k * kFS + k];  // the same value in every lane
+    ok = piv > tiny;
     if (!ok) break;
+    const double lkk = sqrt(piv);
+    __syncwarp();
+    if (lane == k) a[k * kFS + k] = lkk;
+    if (lane > k && lane < dw) a[lane * kFS + k] /= lkk;
+    __syncwarp();
     if (lane > k && lane < dw) {
-      double s2 = a[lane * dw + k];
-      for (int s = 0; s < k; s++) s2 -= a[lane * dw + s] * a[k * dw + s];
-      a[lane * dw + k] = s2 / a[k * dw + k];
+      const double lik = a[lane * kFS + k];
+      for (int j = k + 1; j <= lane; j++) a[lane * kFS + j] -= lik * a[j * kFS + k];
     }
     __syncwarp();
   }
@@ -136,39 +145,40 @@ __global__ void __launch_bounds__(kMxWarps * 32) k_mx_schwarz_factor(Dev d, MixB
       for (int j = 0; j < 24; j++) {
         double v = 0;
         if (i == j && i < dw) {
-          const double dd = d.diag[d.domVerts[start + i / 3] * 3 + i % 3];
+          const double dd = d.diag[dvs[wib][i / 3] * 3 + i % 3];
           v = dd > 1e-12 ? 1 / dd : 0.0;
         }
         Li[i * 24 + j] = (float)v;
       }
     return;
   }
-  // column j of L^-1 by forward substitution (lane j), kept in registers
+  // column `lane` of L^-1: forward substitution with the right-hand side e_lane,
+  // eliminating column by column (rows past dw hold zeros)
   double col[24];
-  for (int i = 0; i < 24; i++) col[i] = 0;
-  if (lane < dw) {
-    for (int i = 0; i < dw; i++) {
-      double s = i == lane ? 1.0 : 0.0;
-      for (int k = 0; k < i; k++) s -= a[i * dw + k] * col[k];
-      col[i] = i < lane ? 0.0 : s / a[i * dw + i];
+#pragma unroll
+  for (int i = 0; i < 24; i++) col[i] = i == lane ? 1.0 : 0.0;
+#pragma unroll
+  for (int i = 0; i < 24; i++) {
+    if (i < dw) {
+      const double xi = col[i] / a[i * kFS + i];
+      col[i] = xi;
+#pragma unroll
+      for (int r = i + 1; r < 24; r++) col[r] -= a[r * kFS + i] * xi;
     }
   }
   __syncwarp();
-  // overwrite the upper triangle region with L^-1 columns: reuse a[] as Linv (row-major)
-  // (L is no longer needed after every lane finished its column)
-  for (int i = 0; i < dw; i++) {
-    const double v = lane < dw ? col[i] : 0.0;
-    __syncwarp();
-    if (lane < dw) a[i * dw + lane] = v;  // a = L^-1
-    __syncwarp();
-  }
-  // A^-1[i][j] = sum_k Linv[k][i] Linv[k][j]; lane i writes row i
+  // a = L^-1 (row-major), written once every lane has finished reading L
+#pragma unroll
+  for (int i = 0; i < 24; i++)
+    if (i < dw && lane < dw) a[i * kFS + lane] = col[i];
+  __syncwarp();
+  // A^-1[i][j] = sum_k L^-1[k][i] L^-1[k][j]; lane i writes row i
   if (lane < 24) {
     for (int j = 0; j < 24; j++) {
-      double s = 0;
+      double sv = 0;
       if (lane < dw && j < dw)
-        for (int k = 0; k < dw; k++) s += a[k * dw + lane] * a[k * dw + j];
-      Li[lane * 24 + j] = (float)s;
+        for (int k = 0; k < dw; k++) sv += a[k * kFS + lane] * a[k * kFS + j];
+      Li[lane * 24 + j] = (float)sv;
     }
   }
 }
