@@ -37,6 +37,10 @@ struct CView {  // kernel view of the contact host buffers
   // [0] trial distance, [1] trial TOI, [2] active-set distance.
   unsigned long long* omin;
   int* badList;                // indices of failing trial candidates (first kBadCap)
+  // A trial enqueued before its Newton iteration's gradient norm was read
+  // records nothing unless *gradGate >= gradTol (null: always records).
+  const double* gradGate;
+  double gradTol;
   const uint32_t* ccnt;        // [self pairs, static pairs] of the current query (device)
   uint32_t* cflag;
   uint32_t* fflag;
@@ -611,6 +615,10 @@ __global__ void k_trial_floor(CView v, const double* xt, double dMin) {
 __global__ void k_trial_final(CView v, double dMin) {
   const double minDist = dbl_of(v.omin[0]);
   const double minTOI = dbl_of(v.omin[1]);
+  if (v.gradGate && !(v.gradGate[0] >= v.gradTol)) {  // the iteration ends at its convergence test
+    v.cint[CI_VALID] = 0;
+    return;
+  }
   if (v.cint[CI_MOVED]) {  // the query is repeated on a rebuilt superset
     v.cint[CI_VALID] = -1;
     return;
@@ -781,6 +789,8 @@ static CView view(ContactHost& h, Solver& s) {
   v.fflag = h.fflag;
   v.omin = h.omin;
   v.badList = h.badList;
+  v.gradGate = nullptr;
+  v.gradTol = 0;
   v.active = h.active;
   v.dd = h.dd;
   v.cg = h.cg;
@@ -1139,11 +1149,13 @@ void ContactHost::merit_energy(Solver& s, const double* x) {
 // checkTrial (contact-assembly.ts:489-553) launched without a host read: the
 // candidate and floor kernels, then an asynchronous copy of the counters that
 // trial_result reads after the caller's next synchronization.
-void ContactHost::trial_launch(Solver& s, const double* xt) {
+void ContactHost::trial_launch(Solver& s, const double* xt, const double* gradGate, double gradTol) {
   cudaStream_t st = s.stream;
   int64_t& lc = launch_counter();
   launch_query(s, xt, p.dmin);
   CView v = view(*this, s);
+  v.gradGate = gradGate;
+  v.gradTol = gradTol;
   k_trial_reset<<<1, 1, 0, st>>>(v);
   k_trial_cand<<<cand_blocks(), kCT, 0, st>>>(v, xt, p.dmin);
   k_trial_bad_lo<<<4 * smCount, kCT, 0, st>>>(v);

@@ -119,7 +119,9 @@ class ContactHost {
   bool check_trial(Solver& s, const double* xt);
   // The same split around the caller's own synchronization: trial_launch
   // enqueues the check and the copy of its counters, trial_result reads them.
-  void trial_launch(Solver& s, const double* xt);
+  // gradGate: the device copy of the iteration's gradient norm when the trial
+  // is enqueued before the convergence test (see k_trial_final).
+  void trial_launch(Solver& s, const double* xt, const double* gradGate = nullptr, double gradTol = 0);
   int trial_result();
   bool trial_redo(Solver& s, const double* xt);
   void commit(Solver& s, const double* x);

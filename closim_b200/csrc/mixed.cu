@@ -476,6 +476,20 @@ __global__ void __launch_bounds__(kThreads) k_mx_sum_terms(const double* t, int 
   const double b = block_sum(s, sm);
   if (threadIdx.x == 0) part[blockIdx.x] = b;
 }
+// The three energy term arrays in one launch: blockIdx.y picks the array; each
+// is summed over the same block partition as a k_mx_sum_terms launch of gridDim.x.
+__global__ void __launch_bounds__(kThreads) k_mx_sum_terms3(const double* t0, int n0, const double* t1, int n1,
+                                                           const double* t2, int n2, double* p0, double* p1,
+                                                           double* p2) {
+  __shared__ double sm[32];
+  const double* t = blockIdx.y == 0 ? t0 : blockIdx.y == 1 ? t1 : t2;
+  const int n = blockIdx.y == 0 ? n0 : blockIdx.y == 1 ? n1 : n2;
+  double* part = blockIdx.y == 0 ? p0 : blockIdx.y == 1 ? p1 : p2;
+  double s = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) s += t[i];
+  const double b = block_sum(s, sm);
+  if (threadIdx.x == 0) part[blockIdx.x] = b;
+}
 __global__ void k_mx_grad_final(Dev d, int nbT, int nbG) {
   if (threadIdx.x >= 32) return;
   const double ms = warp_max_partials(d.part + 0 * d.partStride, nbT);
@@ -536,11 +550,11 @@ void mx_grad_final(const Dev& d, cudaStream_t s, int64_t* lc) {
 void mx_energy_final(const Dev& d, cudaStream_t s, int64_t* lc) {
   const int nb = std::min(mblk(std::max(std::max(d.n * 3, d.m + d.hg), d.hasContact ? d.c.nActive : 0)),
                           d.partStride);
-  k_mx_sum_terms<<<nb, kThreads, 0, s>>>(d.T0, d.n * 3, d.part + 2 * d.partStride);
-  k_mx_sum_terms<<<nb, kThreads, 0, s>>>(d.T1, d.m + (d.kb > 0 ? d.hg : 0), d.part + 3 * d.partStride);
-  k_mx_sum_terms<<<nb, kThreads, 0, s>>>(d.Tc, d.hasContact ? d.c.nActive : 0, d.part + 4 * d.partStride);
+  k_mx_sum_terms3<<<dim3(nb, 3), kThreads, 0, s>>>(d.T0, d.n * 3, d.T1, d.m + (d.kb > 0 ? d.hg : 0), d.Tc,
+                                                   d.hasContact ? d.c.nActive : 0, d.part + 2 * d.partStride,
+                                                   d.part + 3 * d.partStride, d.part + 4 * d.partStride);
   k_mx_energy_final<<<1, 32, 0, s>>>(d, nb);
-  *lc += 4;
+  *lc += 2;
 }
 
 }  // namespace cs

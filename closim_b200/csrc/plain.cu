@@ -10,6 +10,7 @@
 // bit for bit.
 #include <cstdio>
 
+#include "adjoint_math.cuh"
 #include "contact.cuh"
 #include "plain.cuh"
 
@@ -126,6 +127,21 @@ __global__ void __launch_bounds__(kThreads) k_hinge_grad(Dev d) {
   load3(d.x, hv.x, q); load3(d.x, hv.y, q + 3); load3(d.x, hv.z, q + 6); load3(d.x, hv.w, q + 9);
   double out[12];
   hinge_fd_grad(q, d.hmeta[hh * 3], d.hmeta[hh * 3 + 1], d.hmeta[hh * 3 + 2], d.kb, out);
+#pragma unroll
+  for (int k = 0; k < 12; k++) d.helem[(size_t)hh * 12 + k] = out[k];
+}
+
+// Mixed path: the analytic gradient of the same hinge energy (bend_grad, the
+// derivative of bending.ts:7-16) in place of the reference's central
+// differences, which cost 24 energy evaluations per hinge.
+__global__ void __launch_bounds__(kThreads) k_hinge_grad_analytic(Dev d) {
+  const int hh = blockIdx.x * blockDim.x + threadIdx.x;
+  if (hh >= d.hg) return;
+  const int4 hv = d.hinge[hh];
+  double q[12];
+  load3(d.x, hv.x, q); load3(d.x, hv.y, q + 3); load3(d.x, hv.z, q + 6); load3(d.x, hv.w, q + 9);
+  double out[12];
+  bend_grad<double>(q, d.hmeta[hh * 3], d.hmeta[hh * 3 + 1], d.hmeta[hh * 3 + 2], d.kb, out);
 #pragma unroll
   for (int k = 0; k < 12; k++) d.helem[(size_t)hh * 12 + k] = out[k];
 }
@@ -727,9 +743,12 @@ void launch_predict(const Dev& d, cudaStream_t s) {
 void launch_pins(const Dev& d, double* x, cudaStream_t s) {
   if (d.npins > 0) k_pins<<<nblk(d.npins), kThreads, 0, s>>>(d, x);
 }
-void launch_grad_terms(const Dev& d, cudaStream_t s) {
+void launch_grad_terms(const Dev& d, cudaStream_t s, bool analyticBend) {
   k_tri_grad<<<nblk(d.m), kThreads, 0, s>>>(d);
-  if (d.kb > 0 && d.hg > 0) k_hinge_grad<<<nblk(d.hg), kThreads, 0, s>>>(d);
+  if (d.kb > 0 && d.hg > 0) {
+    if (analyticBend) k_hinge_grad_analytic<<<nblk(d.hg), kThreads, 0, s>>>(d);
+    else k_hinge_grad<<<nblk(d.hg), kThreads, 0, s>>>(d);
+  }
   k_gather_grad<<<nblk(d.n), kThreads, 0, s>>>(d);
 }
 void launch_grad(const Dev& d, cudaStream_t s) {

@@ -91,7 +91,9 @@ constexpr int NPART = 8;
 void launch_predict(const Dev& d, cudaStream_t s);
 void launch_pins(const Dev& d, double* x, cudaStream_t s);
 void launch_grad(const Dev& d, cudaStream_t s);           // g, gradNorm, maxStrain
-void launch_grad_terms(const Dev& d, cudaStream_t s);     // g and its squared terms, strain partials
+// g and its squared terms, strain partials; analyticBend (mixed path) takes the
+// analytic hinge gradient instead of the reference's central differences.
+void launch_grad_terms(const Dev& d, cudaStream_t s, bool analyticBend = false);
 void launch_energy_terms(const Dev& d, const double* x, cudaStream_t s);
 void launch_energy(const Dev& d, const double* x, cudaStream_t s);  // S_ENERGY_TRIAL
 void launch_diag_init(const Dev& d, double beta, cudaStream_t s);

@@ -369,18 +369,29 @@ class Solver {
       if (contact) contact->gradient_terms(*this);  // active set, barrier+friction grad, diag estimate
       phase(PH_GRADIENT);
       if (mixed()) {
-        launch_grad_terms(d, stream);
+        launch_grad_terms(d, stream, true);
         lc += 2 + (d.kb > 0 && d.hg > 0);
         mx_grad_final(d, stream, &lc);
       } else {
         launch_grad(d, stream);
         lc += 3 + (d.kb > 0 && d.hg > 0);
       }
-      read_scalars();
-      gradNorm = hscal[S_GRADNORM];
-      maxStrain = hscal[S_MAXSTRAIN];
-      if (!std::isfinite(gradNorm)) throw NonFinite();
-      if (gradNorm < opts.grad_tol) { converged = true; break; }
+      // The convergence test needs the gradient norm on the host. With a line
+      // search ahead, the solve and the first trial are enqueued before it is
+      // read and the norm comes back with the trial's synchronization: when
+      // the gradient turns out converged (or non-finite) that work is dropped,
+      // and the trial's contact check leaves no record (it reads the norm on
+      // the device). Without one, the norm is read here.
+      const bool speculate = newtonMode == 0 && opts.ls_iters > 0;
+      bool gradRead = false, stop = false;
+      if (!speculate) {
+        read_scalars();
+        gradNorm = hscal[S_GRADNORM];
+        maxStrain = hscal[S_MAXSTRAIN];
+        if (!std::isfinite(gradNorm)) throw NonFinite();
+        if (gradNorm < opts.grad_tol) { converged = true; break; }
+        gradRead = true;
+      }
       phase(PH_PRECOND);
       if (newtonMode == 1) {
         if (d.precond == 1) { launch_schwarz_factor(d, stream); lc += 1; }
@@ -417,11 +428,24 @@ class Solver {
         // The trial's validity check and its energy are enqueued together and
         // read with one synchronization; the energy has no side effects and is
         // used only when the trial is valid, as in the reference.
-        if (contact) contact->trial_launch(*this, d.xt);
+        if (contact) contact->trial_launch(*this, d.xt, gradRead ? nullptr : scal.p + S_GRADNORM, opts.grad_tol);
         phase(PH_ENERGY);
         if (contact) contact->merit_energy(*this, d.xt);
         energy_of(d.xt);
         read_scalars();
+        if (!gradRead) {
+          gradRead = true;
+          gradNorm = hscal[S_GRADNORM];
+          maxStrain = hscal[S_MAXSTRAIN];
+          if (!std::isfinite(gradNorm)) throw NonFinite();
+          if (gradNorm < opts.grad_tol) {
+            converged = true;
+            stop = true;
+            trials--;
+            profPending = false;
+            break;
+          }
+        }
         if (contact) {
           int r = contact->trial_result();
           if (r < 0) r = contact->trial_redo(*this, d.xt) ? 1 : 0;
@@ -458,6 +482,7 @@ class Solver {
         if (contact) contact->rejections++;
         alpha *= 0.5;
       }
+      if (stop) break;
       if (!haveSlope) {
         read_scalars();
         pcgTotal += (int)hscal[S_PCG_ITERS];
