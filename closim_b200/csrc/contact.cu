@@ -419,17 +419,32 @@ __global__ void k_contact_chains(CView v, int na) {
   if (threadIdx.x == 32) v.diag->frictionWork = v.diag->frictionWork + seq_sum(v.tf, na);
 }
 
+// The contact gradient in two passes: one thread per (contact, slot) record
+// computes the record's barrier and friction shares (a vertex may sit in many
+// contacts); each vertex then adds its records' shares in record order, the
+// order and the operations of a per-vertex walk (contact-assembly.ts:298-341).
+__global__ void k_contact_grad_rec(CView v, int nrec) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= nrec || q >= (int)v.c.cOff[v.n]) return;
+  const uint32_t rec = v.c.cRec[q];
+  const int ci = rec >> 2, slot = rec & 3;
+  double a[3] = {0, 0, 0}, b[3] = {0, 0, 0};
+  if (v.dd[ci] != 0) {
+    const Frozen f = v.active[ci];
+    dist_grad_slot(f, slot, v.cg[ci * 4], a);
+    friction_slot(f, slot, v.cg + ci * 4 + 1, b);
+  }
+  double* o = v.c.recScratch + (size_t)q * 6;
+  o[0] = a[0]; o[1] = a[1]; o[2] = a[2]; o[3] = b[0]; o[4] = b[1]; o[5] = b[2];
+}
 __global__ void k_contact_grad_gather(CView v, double* cgrad) {
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= v.n) return;
   double o[3] = {0, 0, 0};
   for (uint32_t k = v.c.cOff[q]; k < v.c.cOff[q + 1]; k++) {
-    const uint32_t rec = v.c.cRec[k];
-    const int ci = rec >> 2, slot = rec & 3;
-    if (v.dd[ci] == 0) continue;
-    const Frozen f = v.active[ci];
-    dist_grad_slot(f, slot, v.cg[ci * 4], o);
-    friction_slot(f, slot, v.cg + ci * 4 + 1, o);
+    const double* r = v.c.recScratch + (size_t)k * 6;
+    o[0] += r[0]; o[1] += r[1]; o[2] += r[2];
+    o[0] += r[3]; o[1] += r[4]; o[2] += r[5];
   }
   cgrad[q * 3] = o[0]; cgrad[q * 3 + 1] = o[1]; cgrad[q * 3 + 2] = o[2];
 }
@@ -442,25 +457,40 @@ __global__ void k_contact_curv(CView v, const double* x, int na) {
   v.dd[i] = d >= v.c.dHat ? 0.0 : barrier_curvature(d, v.c.dHat, v.c.kappa);
 }
 
+// The diagonal estimate in the same two passes (addDiagEstimate,
+// contact-assembly.ts:436-471).
+__global__ void k_contact_diag_rec(CView v, int nrec) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= nrec || q >= (int)v.c.cOff[v.n]) return;
+  const uint32_t rec = v.c.cRec[q];
+  const int ci = rec >> 2, slot = rec & 3;
+  double c[3] = {0, 0, 0};
+  const double kk = v.dd[ci];
+  if (kk != 0) {
+    const Frozen f = v.active[ci];
+    if (f.kind == 2) {
+      c[1] = kk;
+    } else {
+      const double n2[3] = {f.nx * f.nx, f.ny * f.ny, f.nz * f.nz};
+      if (f.kind == 0 && slot == 0) {
+        for (int a = 0; a < 3; a++) c[a] = kk * n2[a];
+      } else {
+        const double w = f.kind == 0 ? (slot == 1 ? f.w0 : slot == 2 ? f.w1 : f.w2)
+                                     : (slot == 0 ? f.w0 : slot == 1 ? f.w1 : slot == 2 ? f.w2 : f.w3);
+        for (int a = 0; a < 3; a++) c[a] = kk * w * w * n2[a];
+      }
+    }
+  }
+  double* o = v.c.recScratch + (size_t)q * 6;
+  o[0] = c[0]; o[1] = c[1]; o[2] = c[2];
+}
 __global__ void k_contact_diag_gather(CView v, double* diag) {
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= v.n) return;
   double o[3] = {diag[q * 3], diag[q * 3 + 1], diag[q * 3 + 2]};
   for (uint32_t k = v.c.cOff[q]; k < v.c.cOff[q + 1]; k++) {
-    const uint32_t rec = v.c.cRec[k];
-    const int ci = rec >> 2, slot = rec & 3;
-    const double kk = v.dd[ci];
-    if (kk == 0) continue;
-    const Frozen f = v.active[ci];
-    if (f.kind == 2) { o[1] += kk; continue; }
-    const double n2[3] = {f.nx * f.nx, f.ny * f.ny, f.nz * f.nz};
-    if (f.kind == 0 && slot == 0) {
-      for (int a = 0; a < 3; a++) o[a] += kk * n2[a];
-      continue;
-    }
-    const double w = f.kind == 0 ? (slot == 1 ? f.w0 : slot == 2 ? f.w1 : f.w2)
-                                 : (slot == 0 ? f.w0 : slot == 1 ? f.w1 : slot == 2 ? f.w2 : f.w3);
-    for (int a = 0; a < 3; a++) o[a] += kk * w * w * n2[a];
+    const double* r = v.c.recScratch + (size_t)k * 6;
+    o[0] += r[0]; o[1] += r[1]; o[2] += r[2];
   }
   diag[q * 3] = o[0]; diag[q * 3 + 1] = o[1]; diag[q * 3 + 2] = o[2];
 }
@@ -929,7 +959,7 @@ void ContactHost::ensure_active(Solver& s, size_t na) {
   dalloc(rp1, 4 * c);
   dalloc(rhist, 256 * ((4 * c + kSortTile - 1) / kSortTile) + 1);
   dalloc(kpred, 4 * c);
-  dalloc(recScratch, 12 * c);
+  dalloc(recScratch, 24 * c);
   (void)s;
 }
 void ContactHost::ensure_lag(size_t nl) {
@@ -1129,12 +1159,17 @@ void ContactHost::gradient_terms(Solver& s) {
     k_contact_chains<<<1, 64, 0, st>>>(v, 0);
     lc++;
   }
+  if (na > 0) {
+    k_contact_grad_rec<<<cnb(4l * na), kCT, 0, st>>>(v, 4 * na);
+    lc++;
+  }
   k_contact_grad_gather<<<cnb(n), kCT, 0, st>>>(v, s.d.cgrad);
   lc++;
   if (na > 0) {
     k_contact_curv<<<cnb(na), kCT, 0, st>>>(v, s.d.x, na);
+    k_contact_diag_rec<<<cnb(4l * na), kCT, 0, st>>>(v, 4 * na);
     k_contact_diag_gather<<<cnb(n), kCT, 0, st>>>(v, s.d.diag);
-    lc += 2;
+    lc += 3;
   }
 }
 

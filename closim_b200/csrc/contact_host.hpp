@@ -85,7 +85,7 @@ class ContactHost {
   uint32_t* rp0 = nullptr; uint32_t* rp1 = nullptr; uint32_t* rhist = nullptr;
   uint32_t* cOff = nullptr;    // n + 1
   int* kpred = nullptr;        // 4 per contact: predecessor on each vertex (restitution pass)
-  double* recScratch = nullptr;  // 3 per record (4 per contact): the PCG's contact HVP shares
+  double* recScratch = nullptr;  // 6 per record (4 per contact): per-record contact shares before their ordered sums
   // lagged normals / multipliers
   double* lagFloor = nullptr;  // n
   uint8_t* lagFloorOk = nullptr;

@@ -34,7 +34,7 @@ struct Contact {
   double* cg;              // 4 per contact: barrier dE/dd, friction force args (-f)
   const uint32_t* cOff;    // n+1: vertex -> records (contact << 2 | slot), contact order
   const uint32_t* cRec;
-  double* recScratch;      // 3 per record: one record's HVP share, written and read within a PCG iteration
+  double* recScratch;      // 6 per record: per-record contact shares, summed per vertex in record order
 };
 
 // Everything a kernel of the FP64 path needs, passed by value.

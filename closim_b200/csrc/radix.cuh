@@ -142,16 +142,42 @@ __global__ void __launch_bounds__(kBlockSortThreads) k_block_radix(Key<KW>* k0, 
                                                                    uint32_t* p1, int n, int passes) {
   __shared__ uint32_t cnt[kBlockSortThreads / 32][256];
   __shared__ uint32_t tot[256];
+  __shared__ uint32_t orw[KW], andw[KW];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   constexpr int kWarps = kBlockSortThreads / 32;
   const int chunk = ((n + kWarps - 1) / kWarps + 31) & ~31;
   const int lo = min(n, warp * chunk), hi = min(n, lo + chunk);
   const uint32_t lt = (1u << lane) - 1u;
+  // Bits that differ between keys: a pass whose digit is the same for every
+  // key would leave the (stable) order as it is, so it is skipped.
+  if (threadIdx.x < KW) { orw[threadIdx.x] = 0u; andw[threadIdx.x] = ~0u; }
+  __syncthreads();
+  {
+    uint32_t o[KW], a[KW];
+#pragma unroll
+    for (int w = 0; w < KW; w++) { o[w] = 0u; a[w] = ~0u; }
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      const Key<KW> k = k0[i];
+#pragma unroll
+      for (int w = 0; w < KW; w++) { o[w] |= k.w[w]; a[w] &= k.w[w]; }
+    }
+#pragma unroll
+    for (int w = 0; w < KW; w++) {
+      o[w] = __reduce_or_sync(0xffffffffu, o[w]);
+      a[w] = __reduce_and_sync(0xffffffffu, a[w]);
+      if (lane == 0) { atomicOr(&orw[w], o[w]); atomicAnd(&andw[w], a[w]); }
+    }
+  }
+  __syncthreads();
+  int flip = 0;  // executed passes, mod 2: the records are in (k1, p1) when set
   for (int pass = 0; pass < passes; pass++) {
-    const Key<KW>* ki = (pass & 1) ? k1 : k0;
-    const uint32_t* pi = (pass & 1) ? p1 : p0;
-    Key<KW>* ko = (pass & 1) ? k0 : k1;
-    uint32_t* po = (pass & 1) ? p0 : p1;
+    const int dw = KW - 1 - pass / 4, sh = (pass % 4) * 8;
+    if ((((orw[dw] ^ andw[dw]) >> sh) & 0xffu) == 0u) continue;
+    const Key<KW>* ki = flip ? k1 : k0;
+    const uint32_t* pi = flip ? p1 : p0;
+    Key<KW>* ko = flip ? k0 : k1;
+    uint32_t* po = flip ? p0 : p1;
+    flip ^= 1;
     for (int w = 0; w < kWarps; w++)
       if (threadIdx.x < 256) cnt[w][threadIdx.x] = 0;
     __syncthreads();
@@ -212,6 +238,14 @@ __global__ void __launch_bounds__(kBlockSortThreads) k_block_radix(Key<KW>* k0, 
       __syncwarp();
     }
     __syncthreads();
+  }
+  // The caller expects the records where `passes` executed passes would leave them.
+  if (flip != (passes & 1)) {
+    const Key<KW>* ks = flip ? k1 : k0;
+    const uint32_t* ps = flip ? p1 : p0;
+    Key<KW>* kd = flip ? k0 : k1;
+    uint32_t* pd = flip ? p0 : p1;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) { kd[i] = ks[i]; pd[i] = ps[i]; }
   }
 }
 
