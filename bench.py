@@ -79,6 +79,12 @@ class ClockSampler:
             return
         self.thread = threading.Thread(target=self._read, daemon=True)
         self.thread.start()
+        # nvidia-smi's start-up (NVML initialization) can stall the GPU's
+        # clients for tens of ms: wait for its first sample, so the start-up
+        # falls before the warm-up steps that follow, not inside timed steps.
+        t0 = time.time()
+        while not self.lines and time.time() - t0 < 10 and self.proc.poll() is None:
+            time.sleep(0.01)
 
     def _read(self):
         for line in self.proc.stdout:
@@ -197,6 +203,13 @@ def pcg_kernel_name(precision, prof):
     return "k_mx_pcg_cluster" if info.get("pcgClusterCtas") else "k_mx_pcg"
 
 
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of
+# the headline PCG kernel on the 64x64 floor drape, from one ncu --set full
+# capture; the command and the other counters are in
+# profiles/k_mx_pcg_cluster_floor_drape_64x64.md.
+PCG_DRAM_BYTES = {"k_mx_pcg_cluster": 3.418e6}
+
+
 def run_precision(cfg, precision, local, args, ext_stream_cb, flush, sampler=None, prof_out=None):
     """Warm-up W steps, then K device-resident steps, each bracketed by CUDA
     events on the solver's stream after an L2 flush. Returns (ms_total, solver,
@@ -215,13 +228,13 @@ def run_precision(cfg, precision, local, args, ext_stream_cb, flush, sampler=Non
         sc.pinned.update(configs.pins_at(cfg, k[0] % cfg["steps"]))
         k[0] += 1
 
+    if sampler:
+        sampler.start()  # before the warm-up steps (see ClockSampler.start)
     for _ in range(args.warmup + args.skip):
         set_pins()
         solver.advance(cfg["h"], 1)
     torch.cuda.synchronize()
     ext_stream_cb()
-    if sampler:
-        sampler.start()
     launches0 = solver.kernelLaunches()
     if args.profiler_range:
         torch.cuda.profiler.start()  # ncu --profile-from-start off captures the timed steps only
@@ -277,12 +290,12 @@ def run_batch(args, world, rank, local):
     threads = bs.autotune(h)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{local}")
     ext = torch.cuda.ExternalStream(bs.stream(), device=local)
+    sampler = ClockSampler(local)
+    sampler.start()  # before the warm-up steps (see ClockSampler.start)
     bs.step(h, args.warmup)
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
-    sampler = ClockSampler(local)
-    sampler.start()
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     total = 0.0
@@ -494,7 +507,10 @@ def main():
                        "parallelism": f"replicas x{world}", "l2": "flushed between timed steps (256 MiB write)"},
             "roofline": {"bound": "hbm", "kernel": pcg_kernel_name(headline, prof),
                          "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None, "launches": prof.get("launches"),
+                         "frac": achieved / peak, "traffic": PCG_DRAM_BYTES.get(pcg_kernel_name(headline, prof))
+                         if cfg["name"] == "floor_drape" and not args.small else None,
+                         "traffic_source": "profiles/k_mx_pcg_cluster_floor_drape_64x64.md (one ncu capture)",
+                         "launches": prof.get("launches"),
                          "ms_per_launch": prof.get("ms_per_launch"), "pcg_iters": prof.get("iters"),
                          "alg_bytes_per_launch": prof["bytes"] / max(1, prof["launches"]) if prof else None,
                          "share_of_step": prof["ms"] / total_ms if total_ms and prof else None},
