@@ -911,23 +911,32 @@ void ContactHost::init(Solver& s, const cs_contact_params* prm, int floor_on, do
   dalloc(cint, CI_N);
   CK(cudaMallocHost(&hint, CI_N * sizeof(int)));
   CK(cudaMallocHost(&hdiag, sizeof(DevDiag)));
-  ensure_pairs(1024, 64);
-  ensure_cands(1024);
-  ensure_flags(1024);
+  // Capacities sized from the mesh up front: a buffer that grows mid-run costs
+  // a cudaFree (a device-wide synchronization) and a cudaMalloc inside a step,
+  // measured at 10-70 ms per event. Sixteen pairs per triangle covers the
+  // drapes here with room for folds; growth past it still works (doubling).
+  const size_t pairs0 = std::max<size_t>(1024, 16 * (size_t)m);
+  ensure_pairs(pairs0, ms > 0 ? pairs0 : 64);
+  supCap = pairCap;
+  supSCap = spairCap;
+  dalloc(supPairs, supCap);
+  dalloc(supSPairs, supSCap);
+  ensure_cands(std::max<size_t>(1024, (size_t)m));
+  ensure_flags(15 * pairs0 + (ms > 0 ? 12 * pairs0 : 0));
   {
     int dev = 0;
     CK(cudaGetDevice(&dev));
     CK(cudaDeviceGetAttribute(&smCount, cudaDevAttrMultiProcessorCount, dev));
   }
-  ensure_active(s, std::max(1024, n + 64));
-  ensure_lag(1024);
+  ensure_active(s, std::max<size_t>(1024, (size_t)n + 2 * (size_t)m));
+  ensure_lag(std::max<size_t>(1024, 4 * ((size_t)n + (size_t)m)));
   bvh.flags = cint + CI_OVERFLOW;
   bind(s);
 }
 
 void ContactHost::ensure_pairs(size_t np, size_t nsp) {
-  if (np > pairCap) { pairCap = np + np / 2 + 64; dalloc(bvh.pairs, pairCap); }
-  if (nsp > spairCap) { spairCap = nsp + nsp / 2 + 64; dalloc(spairs, spairCap); }
+  if (np > pairCap) { pairCap = 2 * np + 64; dalloc(bvh.pairs, pairCap); }
+  if (nsp > spairCap) { spairCap = 2 * nsp + 64; dalloc(spairs, spairCap); }
 }
 void ContactHost::ensure_cands(size_t nc) {
   if ((int)nc <= cand.cap) return;
@@ -946,7 +955,7 @@ void ContactHost::ensure_flags(size_t nc) {
 }
 void ContactHost::ensure_active(Solver& s, size_t na) {
   if (na <= actCap) return;
-  const size_t c = na + na / 2 + 256;
+  const size_t c = 2 * na + 256;
   actCap = c;
   dalloc(active, c);
   dalloc(dd, c);
@@ -964,7 +973,7 @@ void ContactHost::ensure_active(Solver& s, size_t na) {
 }
 void ContactHost::ensure_lag(size_t nl) {
   if (nl <= lagCap) return;
-  const size_t c = nl + nl / 2 + 256;
+  const size_t c = 2 * nl + 256;
   // keep existing sorted entries
   Key<6>* ok = nullptr;
   double4* ov = nullptr;
@@ -1036,8 +1045,8 @@ void ContactHost::build_superset(Solver& s, const double* x, double padSup) {
     nSupS = (int)S;
     if (P <= supCap && S <= supSCap) break;
     if (attempt == 1) throw CapacityError("broadphase superset changed between identical traversals");
-    if (P > supCap) { supCap = P + P / 2 + 64; dalloc(supPairs, supCap); }
-    if (S > supSCap) { supSCap = S + S / 2 + 64; dalloc(supSPairs, supSCap); }
+    if (P > supCap) { supCap = 2 * P + 64; dalloc(supPairs, supCap); }
+    if (S > supSCap) { supSCap = 2 * S + 64; dalloc(supSPairs, supSCap); }
   }
   ensure_pairs((size_t)nSup, (size_t)nSupS);
   const size_t bound = 15 * (size_t)nSup + 12 * (size_t)nSupS;
