@@ -194,6 +194,35 @@ def test_bending_gradient_and_hvp(hc):
     assert worst_h < 1e-6, worst_h
 
 
+def test_bending_gradient_large_angles(hc):
+    """The mixed path takes the analytic hinge gradient in place of the
+    reference's central differences (bending.ts:19-44), so it must hold away
+    from flat too: hinges folded by 0.3 to 3.1 rad about the shared edge, flat
+    rest angle, against central differences of the reference's hinge energy."""
+    p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+    hc.hc_bend_grad.restype = C.c_double
+    hc.hc_bend_grad.argtypes = [p, p, C.c_double, p]
+    rng = np.random.default_rng(3)
+    meta = np.array([np.pi, 0.7, 0.9])
+    k = 2e-4
+    for ang in (0.3, 1.0, 1.5, 2.0, 2.5, 2.9, 3.1):
+        worst = 0.0
+        for _ in range(10):
+            # edge along x; wing 2 in +z, wing 3 turned by `ang` about x from -z
+            q = np.array([0, 0, 0, 1, 0, 0, 0.4, 0, 1, 0.6, np.sin(ang), -np.cos(ang)], np.float64)
+            q = q + rng.uniform(-0.02, 0.02, 12)
+            g = np.zeros(12)
+            hc.hc_bend_grad(q, meta, k, g)
+            fd = np.zeros(12)
+            for a in range(12):
+                qp, qm = q.copy(), q.copy()
+                qp[a] += 1e-6
+                qm[a] -= 1e-6
+                fd[a] = (O.hinge_energy(qp, meta, k) - O.hinge_energy(qm, meta, k)) / 2e-6
+            worst = max(worst, np.max(np.abs(fd - g)) / max(np.max(np.abs(fd)), 1e-30))
+        assert worst < 1e-6, (ang, worst)
+
+
 def test_membrane_block9_matches_oracle(hc):
     """The mixed path's closed-form 9x9 membrane block against the oracle's
     restatement of membrane-blocks.ts:21-98 (same Hessian, different algebra)."""
