@@ -43,13 +43,13 @@ def strip_pull(seed: int = 1, nx: int = 40, ny: int = 8, w: float = 1.0, hgt: fl
 
 
 def floor_drape(seed: int = 2, nx: int = 63, ny: int = 63, w: float = 0.8, hgt: float = 0.8, steps: int = 240,
-                precond: str = "schwarz"):
-    """0.8 x 0.8 m sheet, 64 x 64 vertices (7938 triangles), 0.3 m above a y = 0
-    floor; dHat = 1e-3 m, mu = 0.3; C00 = 5e3, C11 = 3e3, G = 1e3; h = 1/120 s;
-    Schwarz-block PCG. Seeded U(+-1e-3) vertical noise."""
+                precond: str = "schwarz", height: float = 0.3):
+    """0.8 x 0.8 m sheet, 64 x 64 vertices (7938 triangles), 0.3 m (`height`)
+    above a y = 0 floor; dHat = 1e-3 m, mu = 0.3; C00 = 5e3, C11 = 3e3, G = 1e3;
+    h = 1/120 s; Schwarz-block PCG. Seeded U(+-1e-3) vertical noise."""
     pos, uv, idx = buildGrid(nx, ny, w, hgt)
     pos = pos.copy()
-    pos[1::3] = (pos[1::3].astype(np.float64) + 0.3).astype(np.float32)
+    pos[1::3] = (pos[1::3].astype(np.float64) + height).astype(np.float32)
     n = len(pos) // 3
     rng = np.random.default_rng(seed)
     x = pos.astype(np.float64)

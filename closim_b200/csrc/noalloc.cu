@@ -34,6 +34,9 @@ double* g_scratch_ptr[64] = {};  // device address of g_hvp_scratch, per device
 }  // namespace
 
 // Resolves the array's device address on the current device (once per device).
+// The address is cached by device index for the life of the process; a
+// cudaDeviceReset unloads the library's device image and leaves the cache
+// stale, so the entry point is not for processes that reset a device.
 static int scratch_on_current_device(double** out) {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return CS_E_CUDA;

@@ -208,12 +208,15 @@ int cs_adjoint_stats(cs_solver* s, double* out5);
  * cudaStream_t (NULL = the legacy default stream), and the kernels' scratch
  * (18 doubles per triangle plus 3 per vertex, about 11 MB) is a fixed array
  * inside this library that every GPU loading the library holds until exit.
- * inc_offsets (n+1) and inc_records (3m, value = triangle * 4 + corner, in
- * ascending triangle order per vertex) are the membrane incidence of
- * src/mesh/incidence.ts:41-55. Limits: n <= CS_STATIC_HVP_MAX_VERTICES and
+ * inc_offsets (n+1) and inc_records (3m) are the membrane incidence as a CSR
+ * over vertices: the records of vertex v are inc_records[inc_offsets[v] ..
+ * inc_offsets[v+1]), each the value triangle * 4 + corner, listed in ascending
+ * triangle order. Limits: n <= CS_STATIC_HVP_MAX_VERTICES and
  * m <= CS_STATIC_HVP_MAX_TRIANGLES, else CS_E_CAPACITY. The first call on a
  * device resolves the array's address (cudaGetSymbolAddress): make that call
- * before any stream capture. All calls share the array: calls that overlap on
+ * before any stream capture. The address is cached per device index for the
+ * life of the process: after cudaDeviceReset the cache is stale, so do not call
+ * this entry point again in that process. All calls share the array: calls that overlap on
  * the GPU race, so serialize them. Returns CS_OK, CS_E_ARG, CS_E_CAPACITY or
  * CS_E_CUDA. */
 #define CS_STATIC_HVP_MAX_VERTICES 65536

@@ -3,14 +3,16 @@
 Reads the reference's published PCG iteration table
 (G5_PRECONDITIONER_REPORT.md:65-76, produced by
 tests/preconditioner-compare.test.ts) and writes g5_pcg_iters.json.
-Run from the repo root: python tests/golden/make_golden.py [reference_dir]
+Run from the repo root: python tests/golden/make_golden.py <reference_dir>
 """
 import json
 import os
 import re
 import sys
 
-ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) != 2:
+    sys.exit("usage: python tests/golden/make_golden.py <reference checkout>")
+ref = sys.argv[1]
 text = open(os.path.join(ref, "G5_PRECONDITIONER_REPORT.md")).read().splitlines()
 rows = {}
 start = None

@@ -50,3 +50,28 @@ def test_session_flags_nonfinite_positions_and_keeps_snapshot():
         sess.stepOnce(1)
     assert sess.restoreStable()
     assert np.array_equal(sc.positions, good)
+
+
+def test_session_published_positions_match_oracle_through_contact():
+    """Every position the session publishes (cs_session_step's device hand-off)
+    equals the oracle's state after the same step, through the landing of a
+    sheet on the floor (barrier, friction and restitution active)."""
+    from tests.helpers import oracle_scene, oracle_step_kwargs
+    cfg = configs.floor_drape(nx=11, ny=11, w=0.15, hgt=0.15, steps=14, height=0.012)
+    sc = configs.make_scene(cfg)
+    published = []
+    sess = SimulationSession(cb.CudaSolver("fp64", **cfg["options"]), lambda x: published.append(x.copy()))
+    sess.attach(sc, cfg["h"])
+    osc = oracle_scene(cfg)
+    kw = oracle_step_kwargs(cfg)
+    floor_contacts = 0
+    for s in range(cfg["steps"]):
+        sess.stepOnce(1)
+        ost = osc.step(cfg["h"], **kw)
+        xo = osc.positions
+        err = np.max(np.abs(published[-1] - xo)) / np.max(np.abs(xo))
+        assert err <= 1e-9, (s, err)
+        assert sess.lastStats.contact["floorPairs"] == ost["floorPairs"], s
+        floor_contacts = max(floor_contacts, ost["floorPairs"])
+    assert floor_contacts > 0, "the sheet never reached the floor"
+    assert sess.stableStep == cfg["steps"] and len(published) == cfg["steps"] + 1
