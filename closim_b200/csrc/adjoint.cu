@@ -16,7 +16,8 @@
 // dg/dtheta: the membrane gradient is linear in (C00, C11, C01, G), so its
 // derivative along C00 is the gradient evaluated with C00 = 1 and the others 0
 // (likewise C11, G); the bending gradient is linear in k, so its derivative is
-// the forward's own finite-difference hinge gradient (bending.ts:19-42) at k = 1.
+// the analytic hinge gradient at k = 1, the gradient the exact-Newton forward
+// takes (the derivative of bending.ts:7-16).
 #include <cooperative_groups.h>
 
 #include "adjoint.cuh"
@@ -130,26 +131,7 @@ __device__ __forceinline__ void mem_hvp64(const double* x0, const double* x1, co
   double S00 = m.C00 * E00 + m.C01 * E11;
   double S11 = m.C11 * E11 + m.C01 * E00;
   double S01 = 2 * m.G * E01;
-  if (psd) {
-    const double hm = 0.5 * (S00 + S11), hd = 0.5 * (S00 - S11);
-    const double rad = sqrt(hd * hd + S01 * S01);
-    const double l1 = hm + rad, l2 = hm - rad;
-    if (l2 < 0) {
-      if (l1 <= 0) {
-        S00 = S11 = S01 = 0;
-      } else {
-        // S+ = l1 u u^T, u the unit eigenvector of l1
-        double ux = S01, uy = l1 - S00;
-        if (ux * ux + uy * uy < 1e-300) { ux = l1 - S11; uy = S01; }
-        const double nn = ux * ux + uy * uy;
-        if (nn < 1e-300) { ux = S00 >= S11 ? 1 : 0; uy = 1 - ux; }
-        else { const double q = 1 / sqrt(nn); ux *= q; uy *= q; }
-        S00 = l1 * ux * ux;
-        S11 = l1 * uy * uy;
-        S01 = l1 * ux * uy;
-      }
-    }
-  }
+  if (psd) psd_stress(S00, S11, S01);
   const double dS00 = m.C00 * dE00 + m.C01 * dE11;
   const double dS11 = m.C11 * dE11 + m.C01 * dE00;
   const double dS01 = 2 * m.G * dE01;
@@ -311,7 +293,7 @@ __global__ void __launch_bounds__(kThreads) k_adj_theta_terms(Dev d, const doubl
     const int ids[4] = {hv.x, hv.y, hv.z, hv.w};
     double q[12], g[12];
     for (int c = 0; c < 4; c++) load3(d.x, ids[c], q + c * 3);
-    hinge_fd_grad(q, d.hmeta[hh * 3], d.hmeta[hh * 3 + 1], d.hmeta[hh * 3 + 2], 1.0, g);
+    bend_grad<double>(q, d.hmeta[hh * 3], d.hmeta[hh * 3 + 1], d.hmeta[hh * 3 + 2], 1.0, g);
     double s = 0;
     for (int c = 0; c < 4; c++) {
       if (d.pinned[ids[c]]) continue;

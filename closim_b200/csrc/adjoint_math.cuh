@@ -117,6 +117,43 @@ CSHD void bend_hvp(const double* q, const double* v, double restAngle, double ed
   for (int a = 0; a < 12; a++) out[a] = g[a].d;
 }
 
+// Gauss-Newton factor of one hinge: g = sqrt(k w) d phi / dx (12 values), so
+// that g g^T is the positive semi-definite part k w (d phi)(d phi)^T of the
+// bending Hessian (the term k w dev d^2 phi, small near the rest angle, is
+// dropped). The exact-Newton mode of the mixed path applies it as g (g . v).
+CSHD void bend_gn(const double* q, double edgeLen, double areaSum, double k, double* g) {
+  double dphi[12];
+  bend_angle_grad<double>(q, dphi);
+  const double w = edgeLen * edgeLen / (areaSum > 1e-12 ? areaSum : 1e-12);
+  const double r = sqrt(k * w);
+  for (int a = 0; a < 12; a++) g[a] = r * dphi[a];
+}
+
+// Positive part of the symmetric 2x2 second Piola stress (S00, S11, S01):
+// negative principal stresses are set to zero. Used in the geometric term of
+// the membrane Hessian (dF S) it makes every element block positive
+// semi-definite: a Newton matrix for the forward solve that leaves its
+// converged solution unchanged.
+CSHD void psd_stress(double& S00, double& S11, double& S01) {
+  const double hm = 0.5 * (S00 + S11), hd = 0.5 * (S00 - S11);
+  const double rad = sqrt(hd * hd + S01 * S01);
+  const double l1 = hm + rad, l2 = hm - rad;
+  if (l2 >= 0) return;
+  if (l1 <= 0) {
+    S00 = S11 = S01 = 0;
+    return;
+  }
+  // S+ = l1 u u^T, u the unit eigenvector of l1
+  double ux = S01, uy = l1 - S00;
+  if (ux * ux + uy * uy < 1e-300) { ux = l1 - S11; uy = S01; }
+  const double nn = ux * ux + uy * uy;
+  if (nn < 1e-300) { ux = S00 >= S11 ? 1 : 0; uy = 1 - ux; }
+  else { const double q = 1 / sqrt(nn); ux *= q; uy *= q; }
+  S00 = l1 * ux * ux;
+  S11 = l1 * uy * uy;
+  S01 = l1 * ux * uy;
+}
+
 // Closed-form 9x9 membrane Hessian block of one triangle (the derivative of
 // membrane.ts:17-80's gradient), for the mixed path's Schwarz assembly:
 //   H_ab = s [ (K_a . S K_b) I3 + sum_{k,m} alpha_km F_k F_m^T ],
@@ -125,9 +162,11 @@ CSHD void bend_hvp(const double* q, const double* v, double restAngle, double ed
 // with F_k the columns of F, K_0 = -(a + c, b + d), K_1 = (a, b), K_2 = (c, d)
 // (the rows of the shape-function gradient) and s = thickness * area. Row-major
 // h[(3a + i) * 9 + 3b + p], stored as O (double, or float for the FP32 path).
+// psd: S replaced by its positive part (psd_stress).
 template <class O>
 CSHD void membrane_block9(const double* x0, const double* x1, const double* x2, double a, double b, double c,
-                          double d, double s, double C00, double C11, double C01, double G, O* h) {
+                          double d, double s, double C00, double C11, double C01, double G, O* h,
+                          bool psd = false) {
   const double K[3][2] = {{-(a + c), -(b + d)}, {a, b}, {c, d}};
   double F0[3], F1[3];
   for (int i = 0; i < 3; i++) {
@@ -138,7 +177,8 @@ CSHD void membrane_block9(const double* x0, const double* x1, const double* x2, 
   const double E00 = 0.5 * (F0[0] * F0[0] + F0[1] * F0[1] + F0[2] * F0[2] - 1);
   const double E11 = 0.5 * (F1[0] * F1[0] + F1[1] * F1[1] + F1[2] * F1[2] - 1);
   const double E01 = 0.5 * (F0[0] * F1[0] + F0[1] * F1[1] + F0[2] * F1[2]);
-  const double S00 = C00 * E00 + C01 * E11, S11 = C11 * E11 + C01 * E00, S01 = 2 * G * E01;
+  double S00 = C00 * E00 + C01 * E11, S11 = C11 * E11 + C01 * E00, S01 = 2 * G * E01;
+  if (psd) psd_stress(S00, S11, S01);  // geometric term only (the material term has no S)
   for (int A = 0; A < 3; A++)
     for (int B = 0; B < 3; B++) {
       const double ka0 = K[A][0], ka1 = K[A][1], kb0 = K[B][0], kb1 = K[B][1];

@@ -41,9 +41,11 @@ __global__ void __launch_bounds__(kThreads) k_mx_tristate(Dev d, MixBufs mb) {
   const Mat<double>& m = d.mat;
   float* o = mb.tris + (size_t)t * 16;
   for (int i = 0; i < 3; i++) { o[i] = (float)F0[i]; o[3 + i] = (float)F1[i]; }
-  o[6] = (float)(m.C00 * E00 + m.C01 * E11);
-  o[7] = (float)(m.C11 * E11 + m.C01 * E00);
-  o[8] = (float)(2 * m.G * E01);
+  double S00 = m.C00 * E00 + m.C01 * E11, S11 = m.C11 * E11 + m.C01 * E00, S01 = 2 * m.G * E01;
+  if (mb.psd) psd_stress(S00, S11, S01);
+  o[6] = (float)S00;
+  o[7] = (float)S11;
+  o[8] = (float)S01;
   o[9] = iv.x; o[10] = iv.y; o[11] = iv.z; o[12] = iv.w;
   o[13] = (float)(m.thickness * (double)d.area[t]);
   o[14] = 0.f; o[15] = 0.f;
@@ -67,7 +69,23 @@ __global__ void __launch_bounds__(kThreads) k_mx_h9(Dev d, MixBufs mb) {
   ld3(d.x, d.idx[t * 3], x0); ld3(d.x, d.idx[t * 3 + 1], x1); ld3(d.x, d.idx[t * 3 + 2], x2);
   const float4 iv = d.inv[t];
   membrane_block9<float>(x0, x1, x2, iv.x, iv.y, iv.z, iv.w, d.mat.thickness * (double)d.area[t], d.mat.C00,
-                         d.mat.C11, d.mat.C01, d.mat.G, mb.h9 + (size_t)t * 81);
+                         d.mat.C11, d.mat.C01, d.mat.G, mb.h9 + (size_t)t * 81, mb.psd != 0);
+}
+
+// Exact-Newton mode: per hinge its vertex ids and the Gauss-Newton factor
+// g = sqrt(k w) d phi / dx (bend_gn) in FP32, for the HVP term g (g . p).
+__global__ void __launch_bounds__(kThreads) k_mx_hinge_gn(Dev d, MixBufs mb) {
+  const int hh = blockIdx.x * blockDim.x + threadIdx.x;
+  if (hh >= d.hg) return;
+  const int4 hv = d.hinge[hh];
+  double q[12], g[12];
+  ld3(d.x, hv.x, q); ld3(d.x, hv.y, q + 3); ld3(d.x, hv.z, q + 6); ld3(d.x, hv.w, q + 9);
+  bend_gn(q, d.hmeta[hh * 3 + 1], d.hmeta[hh * 3 + 2], d.kb, g);
+  float4* o = mb.hrec + (size_t)hh * 4;
+  o[0] = make_float4(__int_as_float(hv.x), __int_as_float(hv.y), __int_as_float(hv.z), __int_as_float(hv.w));
+  o[1] = make_float4((float)g[0], (float)g[1], (float)g[2], (float)g[3]);
+  o[2] = make_float4((float)g[4], (float)g[5], (float)g[6], (float)g[7]);
+  o[3] = make_float4((float)g[8], (float)g[9], (float)g[10], (float)g[11]);
 }
 
 // Schwarz factor: assemble (FP64 sums of the stored blocks + Jacobi diagonal),
@@ -518,6 +536,10 @@ __global__ void k_mx_energy_final(Dev d, int nb) {
 void mx_prepare(const Dev& d, const MixBufs& mb, bool schwarz, cudaStream_t s, int64_t* lc) {
   k_mx_tristate<<<mblk(d.m), kThreads, 0, s>>>(d, mb);
   *lc += 1;
+  if (mb.hrec && d.hg > 0) {
+    k_mx_hinge_gn<<<mblk(d.hg), kThreads, 0, s>>>(d, mb);
+    *lc += 1;
+  }
   if (schwarz) {
     k_mx_h9<<<mblk(d.m), kThreads, 0, s>>>(d, mb);
     k_mx_schwarz_factor<<<(d.D + kMxWarps - 1) / kMxWarps, kMxWarps * 32, 0, s>>>(d, mb);

@@ -17,6 +17,12 @@ struct MixBufs {
   float4* vrec;                // 5 x 3m (null when unused)
   const uint32_t* triSlot;     // 3m: incidence record of (triangle, corner)
   float C00, C11, C01, G;
+  // Exact-Newton mode: psd = 1 stores the positive part of S (psd_stress) in
+  // the triangle records and the Schwarz blocks; hrec (4 float4 per hinge: the
+  // 4 vertex ids, then the 12-value Gauss-Newton factor of bend_gn) adds the
+  // bending term g (g . p) to the HVP. Both off in the reference mode.
+  int psd;
+  float4* hrec;
 };
 
 void mx_prepare(const Dev& d, const MixBufs& mb, bool schwarz, cudaStream_t s, int64_t* lc);

@@ -345,6 +345,29 @@ __global__ void __launch_bounds__(kClT, 1) k_mx_pcg_cluster(ClArgs A) {
           }
         }
       }
+      if (valid && mb.hrec) {
+        // exact-Newton mode: Gauss-Newton bending g (g . p) of the incident
+        // hinges (record = hinge << 2 | corner), split over the T lanes
+        const uint32_t h1 = d.hinOff[v + 1];
+        for (uint32_t q = d.hinOff[v] + lane; q < h1; q += T) {
+          const uint32_t rec = d.hinRec[q];
+          const float4* hr = mb.hrec + (size_t)(rec >> 2) * 4;
+          const float4 hid = __ldg(hr), g0 = __ldg(hr + 1), g1 = __ldg(hr + 2), g2 = __ldg(hr + 3);
+          const float3 P0 = ld_p(mb.z, pc, beta, first, __float_as_int(hid.x));
+          const float3 P1 = ld_p(mb.z, pc, beta, first, __float_as_int(hid.y));
+          const float3 P2 = ld_p(mb.z, pc, beta, first, __float_as_int(hid.z));
+          const float3 P3 = ld_p(mb.z, pc, beta, first, __float_as_int(hid.w));
+          const float gs = g0.x * P0.x + g0.y * P0.y + g0.z * P0.z + g0.w * P1.x + g1.x * P1.y + g1.y * P1.z +
+                           g1.z * P2.x + g1.w * P2.y + g2.x * P2.z + g2.y * P3.x + g2.z * P3.y + g2.w * P3.z;
+          const int c = (int)(rec & 3);  // this vertex's 3 values of g, selected without local memory
+          const float ga = c == 0 ? g0.x : c == 1 ? g0.w : c == 2 ? g1.z : g2.y;
+          const float gb = c == 0 ? g0.y : c == 1 ? g1.x : c == 2 ? g1.w : g2.z;
+          const float gc = c == 0 ? g0.z : c == 1 ? g1.y : c == 2 ? g2.x : g2.w;
+          sp[0] += gs * ga;
+          sp[1] += gs * gb;
+          sp[2] += gs * gc;
+        }
+      }
 #pragma unroll
       for (int o = 1; o < T; o <<= 1) {
         sp[0] += __shfl_xor_sync(0xffffffffu, sp[0], o);

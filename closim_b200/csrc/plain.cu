@@ -700,6 +700,106 @@ void launch_membrane_hvp(const uint32_t* idx, const float4* inv, const float* ar
   k_hvp_gather<<<nblk(n), kThreads, 0, s>>>(memOff, memRec, n, elem, h, out);
 }
 
+// ---- material-model evaluation (material-model.ts:278-288) -------------------------
+// internalEnergyOnly (fem.ts:56-75) terms: triangle energies, then hinge
+// energies when kb > 0, into T1 in the order the reference adds them.
+__global__ void __launch_bounds__(kThreads) k_internal_energy_terms(Dev d, const double* x) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < d.m) {
+    double p0[3], p1[3], p2[3];
+    load3(x, d.idx[i * 3], p0); load3(x, d.idx[i * 3 + 1], p1); load3(x, d.idx[i * 3 + 2], p2);
+    const float4 iv = d.inv[i];
+    d.T1[i] = tri_energy<double>(p0, p1, p2, iv.x, iv.y, iv.z, iv.w, d.area[i], d.mat);
+  }
+  if (i < d.hg && d.kb > 0) {
+    const int4 hv = d.hinge[i];
+    double q[12];
+    load3(x, hv.x, q); load3(x, hv.y, q + 3); load3(x, hv.z, q + 6); load3(x, hv.w, q + 9);
+    d.T1[d.m + i] = hinge_energy4(q, d.hmeta[i * 3], d.hmeta[i * 3 + 1], d.hmeta[i * 3 + 2], d.kb);
+  }
+}
+// evalInternal's gradient (fem.ts:15-54): per vertex, its triangle terms in
+// ascending triangle order, then its hinge terms in hinge order (the
+// reference's scatter order); no inertia, pins or contact.
+__global__ void __launch_bounds__(kThreads) k_gather_internal(Dev d, double* grad) {
+  const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= d.n) return;
+  double s[3] = {0, 0, 0};
+  for (uint32_t k = d.memOff[v]; k < d.memOff[v + 1]; k++) {
+    const uint32_t rec = d.memRec[k];
+    const double* e = d.elem + (size_t)(rec >> 2) * 9 + (rec & 3) * 3;
+    s[0] += e[0]; s[1] += e[1]; s[2] += e[2];
+  }
+  if (d.kb > 0)
+    for (uint32_t k = d.hinOff[v]; k < d.hinOff[v + 1]; k++) {
+      const uint32_t rec = d.hinRec[k];
+      const double* e = d.helem + (size_t)(rec >> 2) * 12 + (rec & 3) * 3;
+      s[0] += e[0]; s[1] += e[1]; s[2] += e[2];
+    }
+  grad[v * 3] = s[0];
+  grad[v * 3 + 1] = s[1];
+  grad[v * 3 + 2] = s[2];
+}
+// out[0] = the internal energy chain, out[1] = max strain over the triangle
+// partials (nbT of them; 0 when none were computed).
+__global__ void __launch_bounds__(kThreads) k_internal_final(Dev d, int nbT, double* out) {
+  __shared__ double cbuf[2 * kChunk];
+  const double e = block_chain(d.T1, d.m + (d.kb > 0 ? d.hg : 0), cbuf);
+  if (threadIdx.x >= 32) return;
+  const double ms = nbT > 0 ? warp_max_partials(d.part + 0 * d.partStride, nbT) : 0.0;
+  if (threadIdx.x == 0) {
+    out[0] = e;
+    out[1] = ms;
+  }
+}
+// evalMembraneHvp (membrane-hvp.ts:80-108): the analytic per-triangle HVP
+// (triangleHvp, membrane-hvp.ts:18-75) and the same vertex gather order.
+__global__ void __launch_bounds__(kThreads) k_tri_hvp_elem(Dev d, const double* x, const double* p) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= d.m) return;
+  const uint32_t i0 = d.idx[t * 3], i1 = d.idx[t * 3 + 1], i2 = d.idx[t * 3 + 2];
+  double p0[3], p1[3], p2[3], v0[3], v1[3], v2[3];
+  load3(x, i0, p0); load3(x, i1, p1); load3(x, i2, p2);
+  load3(p, i0, v0); load3(p, i1, v1); load3(p, i2, v2);
+  const float4 iv = d.inv[t];
+  double o[9];
+  tri_hvp<double>(p0, p1, p2, v0, v1, v2, iv.x, iv.y, iv.z, iv.w, d.area[t], d.mat, o);
+#pragma unroll
+  for (int k = 0; k < 9; k++) d.elem[(size_t)t * 9 + k] = o[k];
+}
+__global__ void __launch_bounds__(kThreads) k_gather_elem9(Dev d, double* out) {
+  const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= d.n) return;
+  double s[3] = {0, 0, 0};
+  for (uint32_t k = d.memOff[v]; k < d.memOff[v + 1]; k++) {
+    const uint32_t rec = d.memRec[k];
+    const double* e = d.elem + (size_t)(rec >> 2) * 9 + (rec & 3) * 3;
+    s[0] += e[0]; s[1] += e[1]; s[2] += e[2];
+  }
+  out[v * 3] = s[0];
+  out[v * 3 + 1] = s[1];
+  out[v * 3 + 2] = s[2];
+}
+
+void launch_internal_eval(const Dev& d0, const double* x, double* grad, double* out2, cudaStream_t s) {
+  Dev d = d0;
+  d.x = const_cast<double*>(x);
+  int nbT = 0;
+  if (grad) {
+    k_tri_grad<<<nblk(d.m), kThreads, 0, s>>>(d);
+    nbT = nblk(d.m);
+    if (d.kb > 0 && d.hg > 0) k_hinge_grad<<<nblk(d.hg), kThreads, 0, s>>>(d);
+    k_gather_internal<<<nblk(d.n), kThreads, 0, s>>>(d, grad);
+  }
+  k_internal_energy_terms<<<nblk(std::max(d.m, d.hg)), kThreads, 0, s>>>(d, x);
+  k_internal_final<<<1, kThreads, 0, s>>>(d, nbT, out2);
+}
+
+void launch_membrane_hvp_analytic(const Dev& d, const double* x, const double* p, double* out, cudaStream_t s) {
+  k_tri_hvp_elem<<<nblk(d.m), kThreads, 0, s>>>(d, x, p);
+  k_gather_elem9<<<nblk(d.n), kThreads, 0, s>>>(d, out);
+}
+
 // ---- Armijo trial + velocity ----------------------------------------------------
 __global__ void k_trial(Dev d, double alpha) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -751,8 +851,8 @@ void launch_grad_terms(const Dev& d, cudaStream_t s, bool analyticBend) {
   }
   k_gather_grad<<<nblk(d.n), kThreads, 0, s>>>(d);
 }
-void launch_grad(const Dev& d, cudaStream_t s) {
-  launch_grad_terms(d, s);
+void launch_grad(const Dev& d, cudaStream_t s, bool analyticBend) {
+  launch_grad_terms(d, s, analyticBend);
   k_grad_final<<<1, kThreads, 0, s>>>(d, nblk(d.m));
 }
 void launch_energy_terms(const Dev& d, const double* x, cudaStream_t s) {

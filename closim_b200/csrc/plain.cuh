@@ -90,7 +90,9 @@ constexpr int NPART = 8;
 // Launchers (plain.cu).
 void launch_predict(const Dev& d, cudaStream_t s);
 void launch_pins(const Dev& d, double* x, cudaStream_t s);
-void launch_grad(const Dev& d, cudaStream_t s);           // g, gradNorm, maxStrain
+// g, gradNorm, maxStrain; analyticBend: the analytic hinge gradient instead of
+// the reference's central differences (see launch_grad_terms).
+void launch_grad(const Dev& d, cudaStream_t s, bool analyticBend = false);
 // g and its squared terms, strain partials; analyticBend (mixed path) takes the
 // analytic hinge gradient instead of the reference's central differences.
 void launch_grad_terms(const Dev& d, cudaStream_t s, bool analyticBend = false);
@@ -104,6 +106,12 @@ void launch_velocity(const Dev& d, double damp, cudaStream_t s);
 // SimulationSession.doStep hand-off (sim-session.ts:132-150) on the device:
 // flag = any non-finite coordinate; stable <- x when finite.
 void launch_session_check(const double* x, double* stable, int n3, int* flag, cudaStream_t s);
+// Material-model evaluation over the mesh at x (no inertia, pins or contact):
+// out2[0] = internalEnergyOnly, out2[1] = max strain (when grad is given);
+// grad (3n, may be null) = evalInternal's gradient.
+void launch_internal_eval(const Dev& d, const double* x, double* grad, double* out2, cudaStream_t s);
+// evalMembraneHvp: analytic membrane Hessian-vector product at x along p.
+void launch_membrane_hvp_analytic(const Dev& d, const double* x, const double* p, double* out, cudaStream_t s);
 int pcg_grid_blocks(const Dev& d);
 // FD membrane HVP over device arrays (T: 3n terms, h: 1 double, elem: 18m scratch).
 void launch_membrane_hvp(const uint32_t* idx, const float4* inv, const float* area, const Mat<double>& mat, int n,

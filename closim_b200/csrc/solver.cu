@@ -124,6 +124,24 @@ int cs_membrane_hvp(cs_solver* h, const double* x, const double* p, double* out)
     h->s.membrane_hvp(x, p, out);
   });
 }
+int cs_internal_energy(cs_solver* h, const double* x, double* energy) {
+  return guarded(h, [&] {
+    if (!x || !energy) throw std::invalid_argument("null argument");
+    h->s.internal_eval(x, energy, nullptr, nullptr);
+  });
+}
+int cs_internal_gradient(cs_solver* h, const double* x, double* energy, double* grad, double* max_strain) {
+  return guarded(h, [&] {
+    if (!x || !grad) throw std::invalid_argument("null argument");
+    h->s.internal_eval(x, energy, grad, max_strain);
+  });
+}
+int cs_membrane_hvp_analytic(cs_solver* h, const double* x, const double* p, double* out) {
+  return guarded(h, [&] {
+    if (!x || !p || !out) throw std::invalid_argument("null argument");
+    h->s.membrane_hvp_analytic(x, p, out);
+  });
+}
 int cs_last_stats(cs_solver* h, cs_step_stats* out) {
   return guarded(h, [&] {
     if (!h->s.haveStats) throw std::logic_error("CpuSolver not initialized: no step taken");

@@ -373,7 +373,11 @@ class Solver {
         lc += 2 + (d.kb > 0 && d.hg > 0);
         mx_grad_final(d, stream, &lc);
       } else {
-        launch_grad(d, stream);
+        // Exact-Newton mode takes the analytic hinge gradient: the reference's
+        // central differences of an acos-based angle carry rounding noise near
+        // flat hinges (about 1e-3 in |g| on a flat sheet), a floor no tight
+        // tolerance can get under.
+        launch_grad(d, stream, newtonMode == 1);
         lc += 3 + (d.kb > 0 && d.hg > 0);
       }
       // The convergence test needs the gradient norm on the host. With a line
@@ -393,7 +397,14 @@ class Solver {
         gradRead = true;
       }
       phase(PH_PRECOND);
-      if (newtonMode == 1) {
+      // Exact-Newton mode on the mixed path (one-cluster sheets): the FP32 PCG
+      // solves the positive semi-definite Newton matrix (clamped membrane
+      // stress, Gauss-Newton bending, frozen barrier) to a tolerance FP32 can
+      // reach; larger sheets take the FP64 exact solve.
+      const bool exactMixed = newtonMode == 1 && mixed() && mxCluster > 0;
+      mb.psd = exactMixed ? 1 : 0;
+      mb.hrec = exactMixed && d.kb > 0 && d.hg > 0 ? ensure_hrec() : nullptr;
+      if (newtonMode == 1 && !exactMixed) {
         if (d.precond == 1) { launch_schwarz_factor(d, stream); lc += 1; }
       } else if (mixed()) {
         mx_prepare(d, mb, d.precond == 1, stream, &lc);
@@ -403,7 +414,7 @@ class Solver {
       }
       phase(PH_PCG);
       if (prof) CK(cudaEventRecord(pev0, stream));
-      if (newtonMode == 1) {
+      if (newtonMode == 1 && !exactMixed) {
         ensure_adj_buffers();
         AdjArgs a{d, adjRhs.p, d.dx, adjR.p, adjZ.p, adjP.p, adjAp.p, adjTri.p, adjHin.p, d.kb, 1,
                   opts.pcg_max_iters, newtonTol, adjOut.p};
@@ -411,7 +422,8 @@ class Solver {
         lc += 3;
       } else if (mixed() && mxCluster > 0)
         CK((cudaError_t)mx_launch_pcg_cluster(d, mb, fp.p, fp2.p, d.hasContact ? d.c.dd : nullptr,
-                                              opts.pcg_max_iters, 1e-3, mxCluster, stream));
+                                              opts.pcg_max_iters, exactMixed ? std::max(newtonTol, kMixedTolFloor) : 1e-3,
+                                              mxCluster, stream));
       else if (mixed()) CK((cudaError_t)mx_launch_pcg(d, mb, opts.pcg_max_iters, 1e-3, mxBlocks, stream));
       else CK((cudaError_t)launch_pcg(d, opts.pcg_max_iters, 1e-3, pcgBlocks, stream));
       if (prof) { CK(cudaEventRecord(pev1, stream)); profPending = true; }
@@ -532,6 +544,32 @@ class Solver {
     CK(cudaStreamSynchronize(stream));
   }
 
+  // ---- material model (material-model.ts:232-296) on the current material ----------
+  // energy: internalEnergyOnly (fem.ts:56-75); grad (3n, may be null):
+  // evalInternal's gradient (fem.ts:15-54) with its max strain. Host arrays.
+  void internal_eval(const double* x, double* energy, double* grad, double* maxStrain) {
+    if (!ready) throw std::logic_error("CpuSolver not initialized");
+    const size_t b = 3 * (size_t)mesh.n * 8;
+    CK(cudaMemcpyAsync(vr.p, x, b, cudaMemcpyHostToDevice, stream));
+    launch_internal_eval(d, vr.p, grad ? vAp.p : nullptr, scal.p + S_CH0, stream);
+    launch_counter() += grad ? 4 + (d.kb > 0 && d.hg > 0) : 2;
+    if (grad) CK(cudaMemcpyAsync(grad, vAp.p, b, cudaMemcpyDeviceToHost, stream));
+    read_scalars();
+    if (energy) *energy = hscal[S_CH0];
+    if (maxStrain) *maxStrain = grad ? hscal[S_CH1] : 0.0;
+  }
+  // evalMembraneHvp (membrane-hvp.ts:80-108): analytic membrane HVP at x along p.
+  void membrane_hvp_analytic(const double* x, const double* p, double* out) {
+    if (!ready) throw std::logic_error("CpuSolver not initialized");
+    const size_t b = 3 * (size_t)mesh.n * 8;
+    CK(cudaMemcpyAsync(vr.p, x, b, cudaMemcpyHostToDevice, stream));
+    CK(cudaMemcpyAsync(vz.p, p, b, cudaMemcpyHostToDevice, stream));
+    launch_membrane_hvp_analytic(d, vr.p, vz.p, vAp.p, stream);
+    launch_counter() += 2;
+    CK(cudaMemcpyAsync(out, vAp.p, b, cudaMemcpyDeviceToHost, stream));
+    CK(cudaStreamSynchronize(stream));
+  }
+
   // ---- differentiable rollout (no reference counterpart) -------------------------
   // forward(): `steps` steps of size h from the current state with the pins
   // fixed, keeping (x, v) at every K-th step start; backward(): the reverse
@@ -554,6 +592,15 @@ class Solver {
   // contact) solved to newtonTol, for rollouts that must converge tightly.
   int newtonMode = 0;
   double newtonTol = 1e-8;
+
+  // Relative PCG tolerance the FP32 solve of the exact-Newton mode is held to
+  // at the tightest (single precision cannot resolve residuals much below it).
+  static constexpr double kMixedTolFloor = 1e-5;
+  DBuf<float4> hrecBuf;
+  float4* ensure_hrec() {
+    if (hrecBuf.n < 4 * (size_t)mesh.hg) hrecBuf.alloc(4 * (size_t)mesh.hg);
+    return hrecBuf.p;
+  }
 
   void ensure_adj_buffers() {
     const size_t n3 = 3 * (size_t)mesh.n;

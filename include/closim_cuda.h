@@ -127,6 +127,19 @@ int cs_last_stats(cs_solver* s, cs_step_stats* out);
  * on the initialized mesh and current material. Host arrays of 3n doubles. */
 int cs_membrane_hvp(cs_solver* s, const double* x, const double* p, double* out);
 
+/* ---- material model (src/physics/material-model.ts:232-296) ----
+ * ClothMaterialModel.energy / gradient / hessianVector of the orthotropic StVK
+ * model on the GPU, for the handle's mesh and current material (cs_set_material),
+ * at positions x (host, 3n doubles): no inertia, pins or contact.
+ * cs_internal_energy: internalEnergyOnly (src/physics/fem.ts:56-75).
+ * cs_internal_gradient: evalInternal (fem.ts:15-54): energy, gradient (3n),
+ *   max |Green strain|; energy and max_strain may be NULL.
+ * cs_membrane_hvp_analytic: evalMembraneHvp (src/physics/membrane-hvp.ts:80-108),
+ *   the analytic membrane Hessian-vector product along p (bending excluded). */
+int cs_internal_energy(cs_solver* s, const double* x, double* energy);
+int cs_internal_gradient(cs_solver* s, const double* x, double* energy, double* grad, double* max_strain);
+int cs_membrane_hvp_analytic(cs_solver* s, const double* x, const double* p, double* out);
+
 /* ---- device-resident helpers (no reference counterpart needed by a drop-in) ---- */
 /* Runs `nsteps` steps back to back without copying state to the host. */
 int cs_step_n(cs_solver* s, double dt, int32_t nsteps);
