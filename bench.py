@@ -2,8 +2,18 @@
 
 python bench.py --gpus N --steps K --warmup W [--impl cuda|reference]
                 [--workload floor_drape|strip_pull|sphere_drape|batch_sheets|material_fit]
-                [--precision fp64|mixed|both]
-                [--skip S]   # S extra untimed steps before timing (e.g. to reach contact)
+                [--skip S]   # untimed steps after the warm-up (default 17: the window spans the landing)
+                [--budget converged|reference]
+
+Default (floor drape, 64 x 64): the mixed-precision path and
+the FP64 path run the same steps under a stepper budget where both converge
+(exact-Newton mode: 40 Newton iterations, 3000 PCG iterations, gradTol 1e-8);
+the timed window is steps W+S .. W+S+K (steps 20..119 by default: free fall,
+the landing near step 28 and resting contact). `value` is the mixed path's
+steps/s when its positions stay within 1e-5 (relative) of the FP64 path's on
+every timed step with no admitted intersection, else the FP64 path's (the line
+then says which gate failed). The reference's own budget (10 Newton, 60 PCG
+iterations, PCG tolerance 1e-3) is reported beside it.
 
 One process per GPU (torchrun for N > 1); every rank steps its own replica of
 the workload (a single sheet does not shard: "replicas only", weak scaling).
@@ -149,22 +159,40 @@ def cpu_baseline(cfg, budget_s: float, max_steps: int):
 
 
 def run_reference(args, rank):
+    """The reference's CPU path (the oracle, a C++ restatement of CpuSolver;
+    the TypeScript itself has no runtime here) on the same workload, built
+    with the oracle's own grid builder, stepped from step 0 at the reference's
+    budget; timed over the CUDA arm's window start (steps W+S ..), as many
+    steps as fit a bounded sample."""
     if rank != 0:
         return 0
-    cfg = workload(args.workload, args.steps)
     from oracle import oracle as O
+    from closim_b200 import configs
+    configs.set_grid_builder(O.build_grid)
+    cfg = workload(args.workload, args.steps)
+    from tests.helpers import oracle_scene, oracle_step_kwargs
     O.lib()
-    per = []
-    for i in range(args.warmup + args.steps):
-        b = cpu_baseline(cfg, budget_s=max(5.0, 60.0 / max(1, args.warmup + args.steps)), max_steps=cfg["steps"])
-        if i >= args.warmup:
-            per.append(b["value"])
-    v = statistics.mean(per)
-    line = {"metric": "sim steps/s", "value": v, "unit": "steps/s", "n_gpus": args.gpus, "steps": args.steps,
+    sc = oracle_scene(cfg)
+    kw = oracle_step_kwargs(cfg)
+    start = args.warmup + args.skip
+    for k in range(start):
+        sc.set_pins(configs.pins_at(cfg, k))
+        sc.step(cfg["h"], **kw)
+    t0 = time.perf_counter()
+    k = 0
+    while k < args.steps and (k == 0 or time.perf_counter() - t0 < 60.0):
+        sc.set_pins(configs.pins_at(cfg, start + k))
+        sc.step(cfg["h"], **kw)
+        k += 1
+    dt = time.perf_counter() - t0
+    v = k / dt
+    sample = f"steps {start}..{start + k - 1} of {cfg['name']} ({dt:.1f} s, 1 thread, after {start} untimed steps)"
+    line = {"metric": "sim steps/s", "value": v, "unit": "steps/s", "n_gpus": args.gpus, "steps": k,
             "warmup": args.warmup, "higher_is_better": True, "impl": "reference", "scaling": "weak",
             "dtype": "f64", "data": "synthetic (seeded)",
-            "config": {"workload": cfg["name"], "n": len(cfg["x"]) // 3, "h": cfg["h"]},
-            "cpu_baseline": {"value": v, "unit": "steps/s", "cores": 1, "kind": "port", "sample": b["sample"]},
+            "config": {"workload": cfg["name"], "n": len(cfg["x"]) // 3, "h": cfg["h"],
+                       "budget": "reference (10 Newton, 60 PCG iterations, PCG tolerance 1e-3)"},
+            "cpu_baseline": {"value": v, "unit": "steps/s", "cores": 1, "kind": "port", "sample": sample},
             "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "vs_baseline": None}
     print(json.dumps(line), flush=True)
@@ -204,77 +232,103 @@ def pcg_kernel_name(precision, prof):
 
 
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of
-# the headline PCG kernel on the 64x64 floor drape, from one ncu --set full
-# capture; the command and the other counters are in
-# profiles/k_mx_pcg_cluster_floor_drape_64x64.md.
+# the PCG kernel on the 64 x 64 floor drape, from one ncu capture of that kernel
+# on that workload (not measured by this run; reported as traffic_from_profile).
 PCG_DRAM_BYTES = {"k_mx_pcg_cluster": 3.418e6}
 
 
-def run_precision(cfg, precision, local, args, ext_stream_cb, flush, sampler=None, prof_out=None):
-    """Warm-up W steps, then K device-resident steps, each bracketed by CUDA
-    events on the solver's stream after an L2 flush. Returns (ms_total, solver,
-    scene, final positions, kernel launches)."""
+CONVERGED = dict(newtonIters=40, pcgMaxIters=3000, gradTol=1e-8)
+EXACT_TOL = 1e-6   # relative PCG tolerance of the exact-Newton solves (FP32 floor 1e-5 on the mixed path)
+GATE_REL_ERR = 1e-5
+
+
+def budget_options(cfg, budget):
+    o = dict(cfg["options"])
+    if budget == "converged":
+        o.update(CONVERGED)
+    return o
+
+
+def run_path(cfg, precision, local, args, flush, budget, mode="device", sampler=None, record=False,
+             profile=False):
+    """Steps 0 .. W+S+K of `cfg` on one solver; the last K are timed, each
+    bracketed by CUDA events on the solver's stream after an L2 flush.
+
+    mode "device": device-resident steps (cs_step_n); "e2e": CudaSolver.step
+    with the scene's pinned host arrays uploaded before and read back after
+    every step (the ClothSolver call a user makes). profile: the PCG kernel's
+    launches timed with events (this runs the host-driven step). Returns a dict
+    with the timed milliseconds, per-step positions and contact minima of the
+    timed window (record), launches, and the solver."""
     import torch
     import closim_b200 as cb
     from closim_b200 import configs
     sc = configs.make_scene(cfg)
-    solver = cb.CudaSolver(precision, device=local, **cfg["options"])
+    solver = cb.CudaSolver(precision, device=local, **budget_options(cfg, budget))
     solver.initialize(sc)
+    if budget == "converged":
+        solver.setNewtonMode("exact", EXACT_TOL)
     ext = torch.cuda.ExternalStream(solver.stream(), device=local)
+    n = len(cfg["x"]) // 3
+    if mode == "e2e":
+        px = torch.empty(n * 3, dtype=torch.float64).pin_memory()
+        pv = torch.empty(n * 3, dtype=torch.float64).pin_memory()
+        px.numpy()[:] = sc.positions
+        pv.numpy()[:] = sc.velocities
+        sc.positions = px.numpy()
+        sc.velocities = pv.numpy()
+        solver.syncFromScene = True
     k = [0]
 
-    def set_pins():
+    def one():
         sc.pinned.clear()
         sc.pinned.update(configs.pins_at(cfg, k[0] % cfg["steps"]))
         k[0] += 1
+        if mode == "e2e":
+            solver.step(cfg["h"])
+        else:
+            solver.advance(cfg["h"], 1)
 
     if sampler:
         sampler.start()  # before the warm-up steps (see ClockSampler.start)
     for _ in range(args.warmup + args.skip):
-        set_pins()
-        solver.advance(cfg["h"], 1)
+        one()
     torch.cuda.synchronize()
-    ext_stream_cb()
     launches0 = solver.kernelLaunches()
-    if args.profiler_range:
-        torch.cuda.profiler.start()  # ncu --profile-from-start off captures the timed steps only
-    solver.profile(True)
+    graph0 = solver.graphInfo()
+    if profile:
+        solver.profile(True)
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     total = 0.0
+    pos, mind, stats = [], [], []
     step_bytes = 0.0
-    mesh = configs.make_scene(cfg).mesh
+    mesh = sc.mesh
     for _ in range(args.steps):
-        set_pins()
         with torch.cuda.stream(ext):
             flush.fill_(1.0)
         ev0.record(ext)
-        solver.advance(cfg["h"], 1)
+        one()
         ev1.record(ext)
         ev1.synchronize()
         total += ev0.elapsed_time(ev1)
-        step_bytes += step_algorithmic_bytes(solver.lastStats, mesh, precision, cfg)
+        st = solver.lastStats
+        stats.append(st)
+        step_bytes += step_algorithmic_bytes(st, mesh, precision, cfg)
+        if st.contact:
+            mind.append(st.contact["minDistance"])
+        if record:
+            if mode != "e2e":
+                solver.pull()
+            pos.append(sc.positions.copy())
     torch.cuda.synchronize()
-    if args.profiler_range:
-        torch.cuda.profiler.stop()
-    if prof_out is not None:
-        prof_out.update(solver.profileRead())
-    solver.profile(False)
-    launches = solver.kernelLaunches() - launches0
-    if prof_out is not None:
-        prof_out["launch_info"] = solver.launchInfo()
-        prof_out["step_bytes"] = step_bytes
-    if prof_out is not None and args.phase_steps > 0:
-        # wall-time breakdown over a few extra (untimed) steps
-        solver.profile(True, phases=True)
-        for _ in range(args.phase_steps):
-            set_pins()
-            solver.advance(cfg["h"], 1)
-        torch.cuda.synchronize()
-        prof_out["phases_ms_per_step"] = {k: v / args.phase_steps for k, v in solver.profilePhases().items()}
+    out = dict(ms=total, launches=solver.kernelLaunches() - launches0, solver=solver, scene=sc, pos=pos, mind=mind,
+               stats=stats, step_bytes=step_bytes, graph=solver.graphInfo(), graph0=graph0)
+    if profile:
+        out["prof"] = solver.profileRead()
+        out["prof"]["launch_info"] = solver.launchInfo()
         solver.profile(False)
-    solver.pull()
-    return total, solver, sc, sc.positions.copy(), launches, ext, set_pins
+    return out
 
 
 def run_batch(args, world, rank, local):
@@ -407,20 +461,19 @@ def run_material_fit(args, world, rank, local):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
     ap.add_argument("--workload", default="floor_drape",
                     choices=["floor_drape", "strip_pull", "sphere_drape", "batch_sheets", "material_fit"])
     ap.add_argument("--rollout-steps", type=int, default=40, help="material_fit: steps of the timed rollout")
     ap.add_argument("--sheets", type=int, default=512, help="batch_sheets: number of sheets (512 in the workload)")
-    ap.add_argument("--skip", type=int, default=0, help="extra untimed steps before the timed region")
-    ap.add_argument("--phase-steps", type=int, default=3, help="extra steps for the per-phase wall-time breakdown")
+    ap.add_argument("--skip", type=int, default=17, help="extra untimed steps before the timed region")
+    ap.add_argument("--budget", default="converged", choices=["converged", "reference"],
+                    help="stepper budget of the timed paths (converged: exact-Newton, both paths converge)")
+    ap.add_argument("--no-reference-budget", action="store_true", help="skip the reference-budget figure")
     ap.add_argument("--small", action="store_true", help="32x32 floor drape (for profiler captures)")
-    ap.add_argument("--precision", default="both", choices=["both", "fp64", "mixed"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--profiler-range", action="store_true",
-                    help="mark the timed steps for ncu --profile-from-start off")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -447,92 +500,86 @@ def main():
     else:
         cfg = workload(args.workload, args.steps)
     n = len(cfg["x"]) // 3
-    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{local}")  # 256 MiB > 126 MB L2
+    dev = f"cuda:{local}"
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MiB > 126 MB L2
 
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    headline = "mixed" if args.precision in ("both", "mixed") else "fp64"
-    res = {}
-    if args.precision in ("both", "fp64"):
-        t, _, _, pos, la, _, _ = run_precision(cfg, "fp64", local, args, barrier, flush)
-        res["fp64"] = dict(ms=t, pos=pos, launches=la)
+    # the FP64 path and the mixed path over the same steps and budget
+    fp64 = run_path(cfg, "fp64", local, args, flush, args.budget, record=True)
     sampler = ClockSampler(local)
-    prof = {}
-    t, solver, sc, pos, la, ext, set_pins = run_precision(cfg, headline, local, args, barrier, flush, sampler, prof)
+    mixed = run_path(cfg, "mixed", local, args, flush, args.budget, sampler=sampler, record=True)
     clocks = sampler.stop()
-    res[headline] = dict(ms=t, pos=pos, launches=la)
+    e2e = run_path(cfg, "mixed", local, args, flush, args.budget, mode="e2e")
+    prof = run_path(cfg, "mixed", local, args, flush, args.budget, profile=True)["prof"]
+    ref_budget = None
+    if args.budget == "converged" and not args.no_reference_budget:
+        ref_budget = run_path(cfg, "mixed", local, args, flush, "reference")
+    errs = [float(np.max(np.abs(b - a)) / np.max(np.abs(a))) for a, b in zip(fp64["pos"], mixed["pos"])]
+    dmin = cfg["contact"]["dMinM"] if cfg["contact"] else None
+    min_dist = min(mixed["mind"]) if mixed["mind"] else None
+    gate_err = max(errs) <= GATE_REL_ERR
+    gate_contact = min_dist is None or min_dist >= dmin * (1 - 1e-9)
+    conv = sum(1 for st in mixed["stats"] if st.converged), sum(1 for st in fp64["stats"] if st.converged)
 
-    # ---- end to end through the public API: host state in, host state out ----
-    px = torch.empty(n * 3, dtype=torch.float64).pin_memory()
-    pv = torch.empty(n * 3, dtype=torch.float64).pin_memory()
-    px.numpy()[:] = sc.positions
-    pv.numpy()[:] = sc.velocities
-    sc.positions = px.numpy()
-    sc.velocities = pv.numpy()
-    solver.syncFromScene = True
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
-    e2e_ms = 0.0
-    e_steps = max(3, args.steps // 2)
-    for _ in range(e_steps):
-        set_pins()
-        ev0.record(ext)
-        solver.step(cfg["h"])
-        ev1.record(ext)
-        ev1.synchronize()
-        e2e_ms += ev0.elapsed_time(ev1)
-    h2d = 2 * n * 3 * 8 + len(sc.pinned) * (4 + 24)
-    d2h = 2 * n * 3 * 8
-
-    times = [res[headline]["ms"], e2e_ms, res.get("fp64", {}).get("ms", 0.0)]
-    total_ms, e2e_ms, fp64_ms = max_over_ranks(times, f"cuda:{local}", world)
+    times = [mixed["ms"], e2e["ms"], fp64["ms"]] + ([ref_budget["ms"]] if ref_budget else [])
+    times = max_over_ranks(times, dev, world)
+    mixed_ms, e2e_ms, fp64_ms = times[:3]
     if world > 1:
         dist.barrier()
-    value = replica_throughput(world, args.steps, total_ms)
-    e2e_value = replica_throughput(world, e_steps, e2e_ms)
+    mixed_value = replica_throughput(world, args.steps, mixed_ms)
+    fp64_value = replica_throughput(world, args.steps, fp64_ms)
+    gate_pass = gate_err and gate_contact
+    head = "mixed" if gate_pass else "fp64"
+    value = mixed_value if gate_pass else fp64_value
+    head_ms = mixed_ms if gate_pass else fp64_ms
 
     if rank == 0:
         peak, peak_kind = measured_peak()
-        achieved = (prof["bytes"] / prof["launches"] / (prof["ms_per_launch"] / 1000.0) / 1e9
-                    if prof.get("launches") else 0.0)
+        achieved = prof["bytes"] / prof["launches"] / (prof["ms_per_launch"] / 1000.0) / 1e9 if prof.get("launches") \
+            else 0.0
+        kname = pcg_kernel_name("mixed", prof)
+        n_h2d = 2 * n * 3 * 8
         line = {
             "metric": "sim steps/s", "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if headline == "mixed" else "f64",
+            "warmup": args.warmup, "ms_per_step": head_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if head == "mixed" else "f64",
             "data": "synthetic (seeded)", "impl": "cuda",
             "config": {"workload": cfg["name"] + ("_32x32" if args.small else ""), "n": n, "m": len(cfg["idx"]) // 3,
-                       "h": cfg["h"], "precision": headline, "precond": cfg["options"]["precond"],
-                       "parallelism": f"replicas x{world}", "l2": "flushed between timed steps (256 MiB write)"},
-            "roofline": {"bound": "hbm", "kernel": pcg_kernel_name(headline, prof),
-                         "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": PCG_DRAM_BYTES.get(pcg_kernel_name(headline, prof))
-                         if cfg["name"] == "floor_drape" and not args.small else None,
-                         "traffic_source": "profiles/k_mx_pcg_cluster_floor_drape_64x64.md (one ncu capture)",
-                         "launches": prof.get("launches"),
-                         "ms_per_launch": prof.get("ms_per_launch"), "pcg_iters": prof.get("iters"),
-                         "alg_bytes_per_launch": prof["bytes"] / max(1, prof["launches"]) if prof else None,
-                         "share_of_step": prof["ms"] / total_ms if total_ms and prof else None},
-            "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-            "gpu_launches": res[headline]["launches"],
+                       "h": cfg["h"], "headline_path": head, "precond": cfg["options"]["precond"],
+                       "budget": args.budget + (" (exact-Newton: 40 Newton, 3000 PCG iterations, gradTol 1e-8, "
+                                                "PCG rel. tol 1e-6 FP64 / 1e-5 FP32)" if args.budget == "converged"
+                                                else " (10 Newton, 60 PCG, PCG tol 1e-3)"),
+                       "timed_steps": [args.warmup + args.skip, args.warmup + args.skip + args.steps - 1],
+                       "parallelism": f"replicas x{world}", "l2": "flushed between timed steps (256 MiB write)",
+                       "graph_steps": mixed["graph"]["graphSteps"] - mixed["graph0"]["graphSteps"]},
+            "gate": {"mixed_vs_fp64_rel_pos_err_max": max(errs), "mixed_vs_fp64_rel_pos_err_last": errs[-1],
+                     "limit": GATE_REL_ERR, "steps_compared": len(errs), "min_distance": min_dist, "dmin": dmin,
+                     "intersection_free": gate_contact, "pass": gate_pass,
+                     "converged_steps": {"mixed": conv[0], "fp64": conv[1], "of": args.steps}},
+            "mixed_path": {"value": mixed_value, "ms_per_step": mixed_ms / args.steps,
+                           "gpu_launches": mixed["launches"]},
+            "fp64_path": {"value": fp64_value, "ms_per_step": fp64_ms / args.steps, "gpu_launches": fp64["launches"]},
+            "mixed_over_fp64": mixed_value / fp64_value,
+            "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak,
+                         "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                         "traffic_from_profile": PCG_DRAM_BYTES.get(kname) if cfg["name"] == "floor_drape" else None,
+                         "launches": prof.get("launches"), "ms_per_launch": prof.get("ms_per_launch"),
+                         "pcg_iters": prof.get("iters"),
+                         "alg_bytes_per_launch": prof["bytes"] / max(1, prof["launches"]),
+                         "timing": "CUDA events around each launch, host-driven replay of the same steps"},
+            "e2e": {"value": replica_throughput(world, args.steps, e2e_ms), "unit": "steps/s",
+                    "h2d_bytes_per_step": n_h2d, "d2h_bytes_per_step": n_h2d,
+                    "path": "mixed, CudaSolver.step with pinned host arrays, same steps as value"},
+            "gpu_launches": mixed["launches"] if head == "mixed" else fp64["launches"],
             "clocks": clocks,
-            "phases_ms_per_step": prof.get("phases_ms_per_step"),
-            "step_roofline": {"bound": "hbm", "alg_bytes_per_step": prof.get("step_bytes", 0.0) / args.steps,
-                              "achieved": prof.get("step_bytes", 0.0) / (total_ms / 1000.0) / 1e9,
-                              "peak": measured_peak()[0], "unit": "GB/s",
-                              "frac": prof.get("step_bytes", 0.0) / (total_ms / 1000.0) / 1e9 / measured_peak()[0]},
-            "launch_info": prof.get("launch_info"),
+            "step_roofline": {"bound": "hbm", "alg_bytes_per_step": mixed["step_bytes"] / args.steps,
+                              "achieved": mixed["step_bytes"] / (mixed_ms / 1000.0) / 1e9, "peak": peak,
+                              "unit": "GB/s", "frac": mixed["step_bytes"] / (mixed_ms / 1000.0) / 1e9 / peak},
         }
-        if args.skip:
-            line["config"]["untimed_steps_before"] = args.warmup + args.skip
-        if "fp64" in res and headline == "mixed":
-            a, b = res["fp64"]["pos"], res["mixed"]["pos"]
-            line["fp64_path"] = {"value": world * args.steps / (fp64_ms / 1000.0), "unit": "steps/s",
-                                 "ms_per_step": fp64_ms / args.steps,
-                                 "gpu_launches": res["fp64"]["launches"]}
-            line["mixed_vs_fp64_rel_pos_err"] = float(np.max(np.abs(b - a)) / np.max(np.abs(a)))
-            line["mixed_vs_fp64_steps"] = args.warmup + args.skip + args.steps
+        if ref_budget:
+            rv = replica_throughput(world, args.steps, times[3])
+            line["reference_budget"] = {"value": rv, "unit": "steps/s", "ms_per_step": times[3] / args.steps,
+                                        "path": "mixed, the reference's stepper budget (10 Newton, 60 PCG, "
+                                                "PCG tol 1e-3): steps do not converge, so no 1e-5 comparison"}
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(cfg, budget_s=20.0, max_steps=cfg["steps"])
         print(json.dumps(line), flush=True)

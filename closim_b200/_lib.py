@@ -60,7 +60,7 @@ EXPORTS = ["cs_create", "cs_destroy", "cs_last_error", "cs_initialize", "cs_set_
            "cs_batch_step", "cs_batch_get_positions", "cs_batch_get_velocities", "cs_batch_stats",
            "cs_batch_autotune", "cs_batch_set_threads", "cs_batch_stream", "cs_batch_launch_shape", "cs_session_step", "cs_session_reset",
            "cs_session_restore_stable", "cs_build_grid",
-           "cs_preprocess", "cs_internal_energy", "cs_internal_gradient", "cs_membrane_hvp_analytic",
+           "cs_preprocess", "cs_contact_active", "cs_update_static_positions", "cs_set_graph_mode", "cs_graph_info", "cs_internal_energy", "cs_internal_gradient", "cs_membrane_hvp_analytic",
            "cs_broadphase_create", "cs_broadphase_destroy", "cs_broadphase_last_error",
            "cs_broadphase_build", "cs_broadphase_diagnostics", "cs_broadphase_pairs", "cs_broadphase_state"]
 
@@ -95,6 +95,10 @@ def load():
         "cs_last_stats": (C.c_int, [vp, C.POINTER(cs_step_stats)]),
         "cs_membrane_hvp": (C.c_int, [vp, vp, vp, vp]),
         "cs_internal_energy": (C.c_int, [vp, vp, vp]),
+        "cs_contact_active": (C.c_int, [vp, C.c_int32, vp, vp, vp]),
+        "cs_set_graph_mode": (C.c_int, [vp, C.c_int32]),
+        "cs_update_static_positions": (C.c_int, [vp, vp, C.c_int32]),
+        "cs_graph_info": (C.c_int, [vp, vp]),
         "cs_internal_gradient": (C.c_int, [vp, vp, vp, vp, vp]),
         "cs_membrane_hvp_analytic": (C.c_int, [vp, vp, vp, vp]),
         "cs_sync": (C.c_int, [vp]),

@@ -17,6 +17,22 @@ import numpy as np
 from .solver import (ClothMaterial, ClothScene, ContactParams, ContactSystem, buildGrid, createScene,
                      preprocess)
 
+# Grid builder of the workloads: buildGrid (src/mesh/mesh.ts:17-48) through the
+# CUDA library's cs_build_grid by default. A caller that must not load the
+# library (a CPU-only timing of the same workload) installs another
+# implementation of the same function with set_grid_builder.
+_GRID_BUILDER = None
+
+
+def set_grid_builder(fn) -> None:
+    """fn(nx, ny, w, h) -> (pos f32[3n], uv f32[2n], idx u32[6 nx ny]); None restores buildGrid."""
+    global _GRID_BUILDER
+    _GRID_BUILDER = fn
+
+
+def _grid(nx, ny, w, h):
+    return (_GRID_BUILDER or buildGrid)(nx, ny, w, h)
+
 
 def _material(**kw):
     m = dict(arealDensityKgM2=0.2, thickness=1.0, stretchWarp=5e3, stretchWeft=5e3, stretchCoupling=0.0,
@@ -29,7 +45,7 @@ def strip_pull(seed: int = 1, nx: int = 40, ny: int = 8, w: float = 1.0, hgt: fl
     """1.0 x 0.2 m strip, 41 x 9 vertices (640 triangles); C00 = C11 = 5e3 N/m,
     G = 1e3, k_bend = 1e-4, 0.2 kg/m^2; h = 0.01 s; Newton tol 1e-6; Jacobi PCG.
     Seeded U(+-1e-4) jitter on the vertical coordinate of the initial state."""
-    pos, uv, idx = buildGrid(nx, ny, w, hgt)
+    pos, uv, idx = _grid(nx, ny, w, hgt)
     n = len(pos) // 3
     rng = np.random.default_rng(seed)
     x = pos.astype(np.float64)
@@ -47,7 +63,7 @@ def floor_drape(seed: int = 2, nx: int = 63, ny: int = 63, w: float = 0.8, hgt: 
     """0.8 x 0.8 m sheet, 64 x 64 vertices (7938 triangles), 0.3 m (`height`)
     above a y = 0 floor; dHat = 1e-3 m, mu = 0.3; C00 = 5e3, C11 = 3e3, G = 1e3;
     h = 1/120 s; Schwarz-block PCG. Seeded U(+-1e-3) vertical noise."""
-    pos, uv, idx = buildGrid(nx, ny, w, hgt)
+    pos, uv, idx = _grid(nx, ny, w, hgt)
     pos = pos.copy()
     pos[1::3] = (pos[1::3].astype(np.float64) + height).astype(np.float32)
     n = len(pos) // 3
@@ -100,7 +116,7 @@ def sphere_drape(seed: int = 3, nx: int = 255, ny: int = 255, w: float = 1.0, hg
     32 segments x 16 rings = 960 triangles) and folding onto itself: LBVH
     broadphase, VT + EE CCD, IPC barrier dHat = 5e-4 m, mu = 0.2, h = 1/200 s.
     Seeded U(+-5e-4) in-plane (x, z) jitter of the initial state."""
-    pos, uv, idx = buildGrid(nx, ny, w, hgt)
+    pos, uv, idx = _grid(nx, ny, w, hgt)
     n = len(pos) // 3
     rng = np.random.default_rng(seed)
     x = pos.astype(np.float64)
@@ -128,7 +144,7 @@ def material_fit(seed: int = 4, nx: int = 95, ny: int = 95, w: float = 0.6, hgt:
     seeded U(1 - perturb, 1 + perturb). Loss = mean over vertices of
     |x_N - x_N*|^2. The stepper budget lets every step converge (gradTol 1e-9),
     which the implicit-function-theorem gradient assumes."""
-    pos, uv, idx = buildGrid(nx, ny, w, hgt)
+    pos, uv, idx = _grid(nx, ny, w, hgt)
     n = len(pos) // 3
     rng = np.random.default_rng(seed)
     theta_gt = np.array([6e3, 3e3, 8e2, 2e-4])
@@ -157,7 +173,7 @@ def batch_sheets(seed: int = 5, count: int = 512, side_min: int = 16, side_max: 
     sheets = []
     for i in range(count):
         sd = int(rng.integers(side_min, side_max + 1))
-        pos, uv, idx = buildGrid(sd - 1, sd - 1, sheet_size, sheet_size)
+        pos, uv, idx = _grid(sd - 1, sd - 1, sheet_size, sheet_size)
         n = len(pos) // 3
         x = pos.astype(np.float64)
         x[0::3] += i * spacing

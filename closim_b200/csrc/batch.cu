@@ -420,7 +420,7 @@ __device__ void step_sheet(const BatchDev& b, int s, double* sm) {
 }
 
 template <int T>
-__global__ void __launch_bounds__(T) k_batch_step(BatchDev b) {
+__global__ void __launch_bounds__(T, 1) k_batch_step(BatchDev b) {
   __shared__ double sm[32];
   __shared__ int sheetSh;
   for (int guard = 0; guard <= b.S; guard++) {
@@ -443,18 +443,18 @@ int batch_max_ctas(int threads) {
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   cudaError_t e = cudaSuccess;
-  if (threads == 256) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_batch_step<256>, 256, 0);
-  else if (threads == 512) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_batch_step<512>, 512, 0);
-  else e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_batch_step<1024>, 1024, 0);
+  if (threads == 128) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_batch_step<128>, 128, 0);
+  else if (threads == 256) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_batch_step<256>, 256, 0);
+  else e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_batch_step<512>, 512, 0);
   if (e != cudaSuccess || per < 1) per = 1;
   return per * sms;
 }
 
 int batch_launch_step(const BatchDev& b, int threads, int ctas, cudaStream_t s) {
   cudaMemsetAsync(b.work, 0, sizeof(unsigned int), s);
-  if (threads == 256) k_batch_step<256><<<ctas, 256, 0, s>>>(b);
-  else if (threads == 512) k_batch_step<512><<<ctas, 512, 0, s>>>(b);
-  else k_batch_step<1024><<<ctas, 1024, 0, s>>>(b);
+  if (threads == 128) k_batch_step<128><<<ctas, 128, 0, s>>>(b);
+  else if (threads == 256) k_batch_step<256><<<ctas, 256, 0, s>>>(b);
+  else k_batch_step<512><<<ctas, 512, 0, s>>>(b);
   return (int)cudaGetLastError();
 }
 

@@ -267,9 +267,11 @@ struct Batch {
     cudaEvent_t e0, e1;
     BK(cudaEventCreate(&e0));
     BK(cudaEventCreate(&e1));
-    // Candidates: block size x number of resident blocks. Fewer blocks keep
-    // fewer sheets in flight, so their working sets can stay in L2.
-    const int cands[3] = {256, 512, 1024};
+    // Candidates: block size (vertices per thread of a sheet) x number of
+    // resident blocks (sheets in flight per SM). Fewer blocks keep fewer sheets
+    // in flight, so their working sets can stay in L2. Every candidate compiles
+    // without register spills (1024 threads would cap a thread at 64 registers).
+    const int cands[3] = {128, 256, 512};
     const int fracs[3] = {1, 2, 3};
     float best = 1e30f;
     int bestT = threads, bestC = ctas;
@@ -422,7 +424,7 @@ int cs_batch_autotune(cs_batch* h, double dt, int32_t* threads) {
 int cs_batch_set_threads(cs_batch* h, int32_t threads) {
   cs::Batch* b = B(h);
   return bguard(b, [&] {
-    if (threads != 256 && threads != 512 && threads != 1024) throw cs::BErr(CS_E_ARG, "threads: 256, 512 or 1024");
+    if (threads != 128 && threads != 256 && threads != 512) throw cs::BErr(CS_E_ARG, "threads: 128, 256 or 512");
     b->threads = threads;
     b->ctas = b->ready ? cs::batch_max_ctas(threads) : 0;
     b->drop_graph();

@@ -444,8 +444,9 @@ __device__ __forceinline__ void append_pair(bool keep, int2 pr, int2* out, uint3
 }
 
 __global__ void __launch_bounds__(256) k_filter_self(BvhBufs b, const int2* sup, int nsup, int2* out, uint32_t cap,
-                                                     uint32_t* cnt) {
+                                                     uint32_t* cnt, const int* dn = nullptr) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (dn) nsup = min(nsup, *dn);
   bool keep = false;
   int2 pr = make_int2(0, 0);
   if (i < nsup) {
@@ -456,8 +457,9 @@ __global__ void __launch_bounds__(256) k_filter_self(BvhBufs b, const int2* sup,
 }
 
 __global__ void __launch_bounds__(256) k_filter_static(BvhBufs b, const int2* sup, int nsup, double pad, int2* out,
-                                                       uint32_t cap, uint32_t* cnt) {
+                                                       uint32_t cap, uint32_t* cnt, const int* dn = nullptr) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (dn) nsup = min(nsup, *dn);
   bool keep = false;
   int2 pr = make_int2(0, 0);
   if (i < nsup) {
@@ -478,6 +480,21 @@ void filter_pairs(const BvhBufs& b, const int2* sup, int nsup, int2* out, uint32
   }
   if (nssup > 0) {
     k_filter_static<<<(nssup + 255) / 256, 256, 0, s>>>(b, ssup, nssup, pad, sout, scap, scnt);
+    *launches += 1;
+  }
+}
+
+// The same filter with the superset sizes read on the device (dn[0] self,
+// dn[1] static pairs), launched for the capacities nsup / nssup.
+void filter_pairs_dev(const BvhBufs& b, const int2* sup, int nsup, int2* out, uint32_t cap, uint32_t* cnt,
+                      const int2* ssup, int nssup, double pad, int2* sout, uint32_t scap, uint32_t* scnt,
+                      const int* dn, cudaStream_t s, int64_t* launches) {
+  if (nsup > 0) {
+    k_filter_self<<<(nsup + 255) / 256, 256, 0, s>>>(b, sup, nsup, out, cap, cnt, dn);
+    *launches += 1;
+  }
+  if (nssup > 0) {
+    k_filter_static<<<(nssup + 255) / 256, 256, 0, s>>>(b, ssup, nssup, pad, sout, scap, scnt, dn + 1);
     *launches += 1;
   }
 }

@@ -73,6 +73,9 @@ void bvh_boxes(BvhBufs& b, const double* x0, const double* x1, double pad, cudaS
 void filter_pairs(const BvhBufs& b, const int2* sup, int nsup, int2* out, uint32_t cap, uint32_t* cnt,
                   const int2* ssup, int nssup, double pad, int2* sout, uint32_t scap, uint32_t* scnt, cudaStream_t s,
                   int64_t* launches);
+void filter_pairs_dev(const BvhBufs& b, const int2* sup, int nsup, int2* out, uint32_t cap, uint32_t* cnt,
+                      const int2* ssup, int nssup, double pad, int2* sout, uint32_t scap, uint32_t* scnt,
+                      const int* dn, cudaStream_t s, int64_t* launches);
 
 // Sort buffers for the order keys of candidates (15 per self pair, 12 per
 // static pair; the records are decoded from the pairs where they are used).

@@ -14,6 +14,7 @@
 #include "broadphase.cuh"
 #include "contact.cuh"
 #include "contact_host.hpp"
+#include "graph_ctx.hpp"
 #include "solver.hpp"
 
 namespace cs {
@@ -56,7 +57,16 @@ struct CView {  // kernel view of the contact host buffers
   int lagCount;
   int* cint;
   DevDiag* diag;
+  // Graph-captured steps: the frozen-set and lag-table counts on the device
+  // (ACnt); every count below is then read from here, and launches are sized
+  // for capacities. Null on the host-driven path.
+  int* acnt;
 };
+
+__device__ __forceinline__ int v_ncand(const CView& v) { return v.acnt ? v.acnt[AC_NCAND] : v.nCand; }
+__device__ __forceinline__ int v_lag(const CView& v) { return v.acnt ? v.acnt[AC_LAG] : v.lagCount; }
+// A contact count passed by the host, or (negative) read from the device.
+__device__ __forceinline__ int v_na(const CView& v, int na) { return na >= 0 ? na : v.acnt[AC_NA]; }
 
 __device__ __forceinline__ double seq_sum(const double* t, int n) {
   double s = 0.0;
@@ -248,6 +258,7 @@ __global__ void k_floor_flags(CView v, const double* x) {
 // (updateActiveSet, contact-assembly.ts:164-220).
 __global__ void k_cand_active(CView v, const double* x, const uint32_t* order, int nAct) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (nAct < 0) nAct = v.acnt[AC_NCAND];
   if (j >= nAct) return;
   int r[6];
   cand_rec(v, (int)order[j], r);
@@ -275,7 +286,7 @@ __global__ void k_floor_compact(CView v, const double* x) {
   f.kind = 2; f.p = i; f.a = f.b = f.c = f.d = -1;
   f.w0 = f.w1 = f.w2 = f.w3 = 0;
   f.nx = 0; f.ny = 1; f.nz = 0;
-  v.active[v.nCand + v.fflag[i]] = f;
+  v.active[v_ncand(v) + v.fflag[i]] = f;
 }
 
 __global__ void k_active_reset(CView v) {
@@ -292,6 +303,7 @@ __global__ void k_active_min(CView v) {
 // CSR records: one per (contact, slot) whose vertex is a cloth vertex.
 __global__ void k_csr_records(CView v, Key<1>* k, uint32_t* p, int na) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  na = v_na(v, na);
   if (i >= na * 4) return;
   const int c = i >> 2, slot = i & 3;
   const Frozen f = v.active[c];
@@ -303,8 +315,9 @@ __global__ void k_csr_records(CView v, Key<1>* k, uint32_t* p, int na) {
   p[i] = (uint32_t)i;
 }
 
-__global__ void k_csr_offsets(const Key<1>* k, int nrec, uint32_t* off, int n) {
+__global__ void k_csr_offsets(const Key<1>* k, int nrec, uint32_t* off, int n, const int* dna = nullptr) {
   const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (dna) nrec = 4 * *dna;
   if (v > n) return;
   int lo = 0, hi = nrec;
   while (lo < hi) {
@@ -340,7 +353,7 @@ __device__ __forceinline__ void lag_key(const Frozen& f, int ns, Key<6>& k) {
 
 // Latest committed (n, lambdaN) for a VT/EE key; false when never committed.
 __device__ __forceinline__ bool lag_find(const CView& v, const Key<6>& k, double4& out) {
-  int lo = 0, hi = v.lagCount;  // first entry whose key words exceed k (seq ignored)
+  int lo = 0, hi = v_lag(v);  // first entry whose key words exceed k (seq ignored)
   while (lo < hi) {
     const int mid = (lo + hi) >> 1;
     const Key<6>& e = v.lagKeys[mid];
@@ -377,22 +390,13 @@ __device__ __forceinline__ void relative_slip(const CView& v, const double* x, c
   for (int i = 0; i < 3; i++) u[i] = f.w0 * da[i] + f.w1 * db[i] + f.w2 * dc[i] + f.w3 * dd[i];
 }
 
-// Per contact: active flag (dd), barrier dE/dd and friction args (cg), the
-// energy and friction-work chain terms (tc, tf).
-__global__ void k_contact_prep(CView v, const double* x, int na) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= na) return;
-  const Frozen f = v.active[i];
+// Lagged normal and normal force of a contact at distance d: the committed
+// (n, lambdaN) of its key, else the frozen normal and the barrier's normal force
+// at d (energyGrad, contact-assembly.ts:262-285).
+__device__ __forceinline__ void fric_lagged(const CView& v, const Frozen& f, double d, double& nx, double& ny,
+                                            double& nz, double& lam) {
   const Contact& c = v.c;
-  const double d = js_max(frozen_dist(c, x, f), 1e-12);
-  if (d >= c.dHat) {
-    v.dd[i] = 0; v.tc[i] = 0; v.tf[i] = 0;
-    return;
-  }
-  v.dd[i] = 1;
-  v.tc[i] = c.kappa * barrier_value(d, c.dHat);
-  const double g = barrier_grad_scalar(d, c.dHat, c.kappa, 1);
-  double nx = f.nx, ny = f.ny, nz = f.nz, lam;
+  nx = f.nx; ny = f.ny; nz = f.nz;
   bool has = false;
   double4 lv;
   if (f.kind == 2) {
@@ -404,6 +408,25 @@ __global__ void k_contact_prep(CView v, const double* x, int na) {
   }
   if (has) { nx = lv.x; ny = lv.y; nz = lv.z; lam = lv.w; }
   else lam = barrier_normal_force(d, c.dHat, c.kappa, 1);
+}
+
+// Per contact: active flag (dd), barrier dE/dd and friction args (cg), the
+// energy and friction-work chain terms (tc, tf).
+__global__ void k_contact_prep(CView v, const double* x, int na) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= v_na(v, na)) return;
+  const Frozen f = v.active[i];
+  const Contact& c = v.c;
+  const double d = js_max(frozen_dist(c, x, f), 1e-12);
+  if (d >= c.dHat) {
+    v.dd[i] = 0; v.tc[i] = 0; v.tf[i] = 0;
+    return;
+  }
+  v.dd[i] = 1;
+  v.tc[i] = c.kappa * barrier_value(d, c.dHat);
+  const double g = barrier_grad_scalar(d, c.dHat, c.kappa, 1);
+  double nx, ny, nz, lam;
+  fric_lagged(v, f, d, nx, ny, nz, lam);
   double u[3], fr[3];
   relative_slip(v, x, f, u);
   coulomb_force(u, nx, ny, nz, lam, c.mu, c.eps, fr);
@@ -415,6 +438,7 @@ __global__ void k_contact_prep(CView v, const double* x, int na) {
 }
 
 __global__ void k_contact_chains(CView v, int na) {
+  if (na < 0) na = v.acnt ? v.acnt[AC_NA] : 0;
   if (threadIdx.x == 0) v.diag->barrierEnergy = seq_sum(v.tc, na);
   if (threadIdx.x == 32) v.diag->frictionWork = v.diag->frictionWork + seq_sum(v.tf, na);
 }
@@ -452,7 +476,7 @@ __global__ void k_contact_grad_gather(CView v, double* cgrad) {
 // addDiagEstimate (contact-assembly.ts:436-471): dd = kappa max(b'', 0).
 __global__ void k_contact_curv(CView v, const double* x, int na) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= na) return;
+  if (i >= v_na(v, na)) return;
   const double d = js_max(frozen_dist(v.c, x, v.active[i]), 1e-12);
   v.dd[i] = d >= v.c.dHat ? 0.0 : barrier_curvature(d, v.c.dHat, v.c.kappa);
 }
@@ -495,12 +519,55 @@ __global__ void k_contact_diag_gather(CView v, double* diag) {
   diag[q * 3] = o[0]; diag[q * 3 + 1] = o[1]; diag[q * 3 + 2] = o[2];
 }
 
-// meritEnergy terms (contact-assembly.ts:419-428).
+// Exact-Newton mode: the friction potential's data at x for this Newton
+// iteration (fh, see Contact): mu lambda and the lagged normal of every contact
+// inside dHat (as its gradient term in k_contact_prep), s = mu lambda / m and
+// t = P u / m with m = sqrt(|P u|^2 + eps^2), the gradient's own magnitude.
+__global__ void k_contact_fric(CView v, const double* x, int na, double* fh) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= v_na(v, na)) return;
+  double* o = fh + (size_t)i * 8;
+  const Frozen f = v.active[i];
+  const Contact& c = v.c;
+  const double d = js_max(frozen_dist(c, x, f), 1e-12);
+  if (d >= c.dHat) {
+    for (int k = 0; k < 8; k++) o[k] = 0;
+    return;
+  }
+  double nx, ny, nz, lam;
+  fric_lagged(v, f, d, nx, ny, nz, lam);
+  double u[3];
+  relative_slip(v, x, f, u);
+  const double un = u[0] * nx + u[1] * ny + u[2] * nz;
+  const double t[3] = {u[0] - un * nx, u[1] - un * ny, u[2] - un * nz};
+  const double mag = sqrt(t[0] * t[0] + t[1] * t[1] + t[2] * t[2] + c.eps * c.eps);
+  const double ml = c.mu * fmax(0.0, lam);
+  o[0] = ml;
+  o[1] = ml / mag;
+  o[2] = t[0] / mag; o[3] = t[1] / mag; o[4] = t[2] / mag;
+  o[5] = nx; o[6] = ny; o[7] = nz;
+}
+
+// meritEnergy terms (contact-assembly.ts:419-428); in exact-Newton mode plus
+// the friction potential mu lambda sqrt(|P u|^2 + eps^2) with this iteration's
+// frozen mu lambda and normal.
 __global__ void k_contact_merit(CView v, const double* x, int na) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= na) return;
-  const double d = js_max(frozen_dist(v.c, x, v.active[i]), 1e-12);
-  v.tc[i] = d >= v.c.dHat ? 0.0 : v.c.kappa * barrier_value(d, v.c.dHat);
+  if (i >= v_na(v, na)) return;
+  const Frozen f = v.active[i];
+  const double d = js_max(frozen_dist(v.c, x, f), 1e-12);
+  double e = d >= v.c.dHat ? 0.0 : v.c.kappa * barrier_value(d, v.c.dHat);
+  if (v.c.fric) {
+    const double* fh = v.c.fh + (size_t)i * 8;
+    if (fh[0] != 0) {
+      double u[3];
+      relative_slip(v, x, f, u);
+      const double un = u[0] * fh[5] + u[1] * fh[6] + u[2] * fh[7];
+      const double t[3] = {u[0] - un * fh[5], u[1] - un * fh[6], u[2] - un * fh[7]};
+      e += fh[0] * sqrt(t[0] * t[0] + t[1] * t[1] + t[2] * t[2] + v.c.eps * v.c.eps);
+    }
+  }
+  v.tc[i] = e;
 }
 
 // commit (contact-assembly.ts:475-485): floor multipliers in a per-vertex
@@ -508,6 +575,11 @@ __global__ void k_contact_merit(CView v, const double* x, int na) {
 __global__ void k_contact_commit(CView v, const double* x, int na, Key<6>* lk, uint32_t* lp, double4* lval,
                                  int base, int commitNo) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v.acnt) {
+    na = v.acnt[AC_NA];
+    base = v.acnt[AC_LAG];
+    commitNo = v.acnt[AC_COMMIT];
+  }
   if (i >= na) return;
   const Frozen f = v.active[i];
   const double d = js_max(frozen_dist(v.c, x, f), 1e-12);
@@ -517,7 +589,7 @@ __global__ void k_contact_commit(CView v, const double* x, int na, Key<6>* lk, u
     if (ok) { v.lagFloor[f.p] = lam; v.lagFloorOk[f.p] = 1; }
     return;
   }
-  if (i >= v.nCand) return;
+  if (i >= v_ncand(v)) return;
   const int e = base + i;
   Key<6> k;
   if (ok) {
@@ -531,13 +603,17 @@ __global__ void k_contact_commit(CView v, const double* x, int na, Key<6>* lk, u
   lval[e] = make_double4(f.nx, f.ny, f.nz, lam);
 }
 
-__global__ void k_iota(uint32_t* p, int n) {
+__global__ void k_iota(uint32_t* p, int n, const int* dn = nullptr) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (dn) n = min(n, *dn);
   if (i < n) p[i] = (uint32_t)i;
 }
 
-__global__ void k_gather_vals(const double4* src, const uint32_t* order, int n, double4* dst) {
+// dn (optional): n read on the device.
+__global__ void k_gather_vals(const double4* src, const uint32_t* order, int n, double4* dst,
+                              const int* dn = nullptr) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (dn) n = min(n, *dn);
   if (i < n) dst[i] = src[order[i]];
 }
 
@@ -726,9 +802,15 @@ __device__ __forceinline__ void kill_one(const Frozen& c, double* vel) {
   }
 }
 
+constexpr int kKillRoundsMax = 48 * 1024 * 8;  // contacts whose done bits fit 48 KB of shared memory
+
 // VT/EE impulses in list order by one thread (each sees the earlier updates).
 __global__ void k_kill_vtee(CView v, double* vel, int nve) {
   if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  if (v.acnt) {
+    nve = v.acnt[AC_NCAND];
+    if (nve <= kKillRoundsMax) return;  // the rounds kernel handled it
+  }
   for (int i = 0; i < nve; i++) kill_one(v.active[i], vel);
 }
 
@@ -738,6 +820,10 @@ __global__ void k_kill_vtee(CView v, double* vel, int nve) {
 __global__ void k_kill_pred(CView v, const Key<1>* rk, const uint32_t* rp, const uint32_t* off, int nrec, int nve,
                             int* pred) {
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v.acnt) {
+    nrec = 4 * v.acnt[AC_NA];
+    nve = v.acnt[AC_NCAND];
+  }
   if (q >= nrec) return;
   const uint32_t vert = rk[q].w[0];
   const uint32_t pay = rp[q];
@@ -756,6 +842,12 @@ constexpr int kKillThreads = 1024;
 __global__ void __launch_bounds__(kKillThreads) k_kill_vtee_rounds(CView v, double* vel, int nve,
                                                                    const int* pred) {
   extern __shared__ uint32_t doneBits[];
+  if (v.acnt) {
+    // graph-captured step: launched with the largest bitset; longer lists take
+    // the one-thread pass (k_kill_vtee) instead
+    nve = v.acnt[AC_NCAND];
+    if (nve > kKillRoundsMax) return;
+  }
   const int words = (nve + 31) >> 5;
   for (int w = threadIdx.x; w < words; w += blockDim.x) doneBits[w] = 0;
   __syncthreads();
@@ -782,6 +874,10 @@ __global__ void __launch_bounds__(kKillThreads) k_kill_vtee_rounds(CView v, doub
 
 __global__ void k_kill_floor(CView v, double* vel, int base, int nf) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v.acnt) {
+    base = v.acnt[AC_NCAND];
+    nf = v.acnt[AC_NFLOOR];
+  }
   if (i >= nf) return;
   const int p = v.active[base + i].p;
   if (vel[p * 3 + 1] < 0) vel[p * 3 + 1] = 0;
@@ -833,6 +929,16 @@ static CView view(ContactHost& h, Solver& s) {
   v.lagCount = h.lagCount;
   v.cint = h.cint;
   v.diag = h.diag;
+  v.acnt = nullptr;
+  return v;
+}
+// The view of a graph-captured step: device counts, capacity-sized launches.
+static CView cview(ContactHost& h, Solver& s) {
+  CView v = view(h, s);
+  v.acnt = h.acnt;
+  v.nCand = 0;
+  v.nFloor = 0;
+  v.lagCount = 0;
   return v;
 }
 
@@ -845,9 +951,9 @@ ContactHost::~ContactHost() {
                    (void**)&cand.k0, (void**)&cand.k1, (void**)&cand.p0, (void**)&cand.p1, (void**)&cand.hist,
                    (void**)&cflag, (void**)&fflag, (void**)&omin, (void**)&badList, (void**)&active, (void**)&dd,
                    (void**)&cg, (void**)&tc, (void**)&tf, (void**)&rk0, (void**)&rk1, (void**)&rp0, (void**)&rp1,
-                   (void**)&rhist, (void**)&kpred, (void**)&recScratch, (void**)&cOff, (void**)&lagFloor, (void**)&lagFloorOk, (void**)&lk0,
+                   (void**)&rhist, (void**)&kpred, (void**)&recScratch, (void**)&fh, (void**)&fdd, (void**)&cOff, (void**)&lagFloor, (void**)&lagFloorOk, (void**)&lk0,
                    (void**)&lk1, (void**)&lp0, (void**)&lp1, (void**)&lhist, (void**)&lval, (void**)&lsorted,
-                   (void**)&probe, (void**)&diag, (void**)&cint, (void**)&supPairs,
+                   (void**)&probe, (void**)&diag, (void**)&cint, (void**)&acnt, (void**)&supPairs,
                    (void**)&supSPairs, (void**)&supBase})
     if (*q) cudaFree(*q);
   if (hint) cudaFreeHost(hint);
@@ -909,6 +1015,8 @@ void ContactHost::init(Solver& s, const cs_contact_params* prm, int floor_on, do
   dalloc(probe, 3 * (size_t)n);
   dalloc(diag, 1);
   dalloc(cint, CI_N);
+  dalloc(acnt, AC_N);
+  CK(cudaMemset(acnt, 0, AC_N * sizeof(int)));
   CK(cudaMallocHost(&hint, CI_N * sizeof(int)));
   CK(cudaMallocHost(&hdiag, sizeof(DevDiag)));
   // Capacities sized from the mesh up front: a buffer that grows mid-run costs
@@ -969,6 +1077,8 @@ void ContactHost::ensure_active(Solver& s, size_t na) {
   dalloc(rhist, 256 * ((4 * c + kSortTile - 1) / kSortTile) + 1);
   dalloc(kpred, 4 * c);
   dalloc(recScratch, 24 * c);
+  dalloc(fh, 8 * c);
+  dalloc(fdd, 3 * c);
   (void)s;
 }
 void ContactHost::ensure_lag(size_t nl) {
@@ -1007,12 +1117,16 @@ void ContactHost::bind(Solver& s) {
   c.ns = ns;
   c.spos = spos;
   c.nActive = nCand + nFloor;
+  c.nActiveD = nullptr;
   c.active = active;
   c.dd = dd;
   c.cg = cg;
   c.cOff = cOff;
   c.cRec = rp0;
   c.recScratch = recScratch;
+  c.fric = fricOn ? 1 : 0;
+  c.fh = fh;
+  c.fdd = fdd;
   s.d.Tc = tc;
   s.d.hasContact = 1;
 }
@@ -1182,6 +1296,16 @@ void ContactHost::gradient_terms(Solver& s) {
   }
 }
 
+void ContactHost::friction_terms(Solver& s) {
+  const int na = nCand + nFloor;
+  fricOn = true;
+  bind(s);
+  if (na <= 0) return;
+  CView v = view(*this, s);
+  k_contact_fric<<<cnb(na), kCT, 0, s.stream>>>(v, s.d.x, na, fh);
+  launch_counter()++;
+}
+
 void ContactHost::merit_energy(Solver& s, const double* x) {
   const int na = nCand + nFloor;
   if (na <= 0) return;
@@ -1297,6 +1421,7 @@ void ContactHost::begin_step_and_bisect(Solver& s) {
   lagCount = 0;
   commitNo = 0;
   rejections = 0;
+  fricOn = false;
   topoValid = false;
   supValid = false;
   candidatePairs = activePairs = vtPairs = eePairs = floorPairs = 0;
@@ -1337,11 +1462,295 @@ void ContactHost::fill_stats(Solver& s, cs_step_stats& out) {
   out.ccd_failures = hdiag->ccdFailures;
 }
 
+void ContactHost::update_static_positions(Solver& s, const float* sp, int nsv) {
+  if (ms <= 0 || nsv != ns) throw std::invalid_argument("static positions must match the static mesh's vertex count");
+  for (int i = 0; i < 3 * nsv; i++)
+    if (!std::isfinite(sp[i])) throw std::invalid_argument("static positions must be finite");
+  CK(cudaMemcpyAsync(spos, sp, 12 * (size_t)ns, cudaMemcpyHostToDevice, s.stream));
+  CK(cudaStreamSynchronize(s.stream));  // sp is the caller's
+  supValid = false;
+  topoValid = false;
+}
+
+int ContactHost::read_active(Solver& s, int cap, int32_t* ids6, double* w7) {
+  const int na = nCand + nFloor;
+  if (na > 0 && ids6 && w7 && cap >= na) {
+    std::vector<Frozen> h((size_t)na);
+    CK(cudaMemcpyAsync(h.data(), active, (size_t)na * sizeof(Frozen), cudaMemcpyDeviceToHost, s.stream));
+    CK(cudaStreamSynchronize(s.stream));
+    for (int i = 0; i < na; i++) {
+      const Frozen& f = h[i];
+      int32_t* o = ids6 + (size_t)i * 6;
+      o[0] = f.kind; o[1] = f.p; o[2] = f.a; o[3] = f.b; o[4] = f.c; o[5] = f.d;
+      double* w = w7 + (size_t)i * 7;
+      w[0] = f.w0; w[1] = f.w1; w[2] = f.w2; w[3] = f.w3; w[4] = f.nx; w[5] = f.ny; w[6] = f.nz;
+    }
+  }
+  return na;
+}
+
+// ---- graph-captured step ------------------------------------------------------------
+// The host-driven methods above read counts back to size launches and sorts and
+// to grow buffers. Their captured counterparts below read every count on the
+// device (acnt), size launches for capacities and report overflow in
+// acnt[AC_ERR]; the solver then repeats the step on the host-driven path with
+// grown buffers. Kernels and their arithmetic are the same, so a captured step
+// computes what the host-driven one does.
+
+__global__ void k_cap_begin(DevDiag* diag, int* acnt) {
+  DevDiag z{};
+  z.minDistance = INFINITY;
+  z.minTOI = INFINITY;
+  *diag = z;
+  for (int k = 0; k < AC_N; k++) acnt[k] = 0;
+}
+// Superset sizes of a traversal into acnt, with the checks build_superset makes.
+__global__ void k_cap_sup_counts(const int* cint, int* acnt, long supCap, long supSCap, long pairCap,
+                                 long spairCap, long flagCap, int hasStatic) {
+  const long P = (uint32_t)cint[CI_SELF], S = hasStatic ? (uint32_t)cint[CI_STATIC] : 0;
+  acnt[AC_NSUP] = (int)min(P, supCap);
+  acnt[AC_NSUPS] = (int)min(S, supSCap);
+  if (cint[CI_OVERFLOW] || P > supCap || S > supSCap || P > pairCap || S > spairCap || 15 * P + 12 * S > flagCap)
+    acnt[AC_ERR] |= ACE_CAPACITY;
+}
+__global__ void k_cap_cond_moved(const int* cint, cudaGraphConditionalHandle h) {
+  cudaGraphSetConditional(h, cint[CI_MOVED] ? 1u : 0u);
+}
+// A query repeated on a superset rebuilt around it must be covered.
+__global__ void k_cap_err_moved(const int* cint, int* acnt) {
+  if (cint[CI_MOVED]) acnt[AC_ERR] |= ACE_SUPERSET;
+}
+// Frozen-set layout of the query just made (update_active_set's host reads).
+__global__ void k_cap_active_counts(const int* cint, int* acnt, int candCap, int actCap) {
+  const int nc = cint[CI_NCAND], nf = cint[CI_NFLOOR];
+  if (nc > candCap || (long)nc + nf > actCap) acnt[AC_ERR] |= ACE_CAPACITY;
+  const int c = min(nc, candCap), na = min(c + nf, actCap);
+  acnt[AC_NCAND] = c;
+  acnt[AC_NFLOOR] = na - c;
+  acnt[AC_NVT] = cint[CI_NVT];
+  acnt[AC_NA] = na;
+  acnt[AC_NREC] = 4 * na;
+}
+// commit's host bookkeeping: the lag table grows by the candidates when there
+// are any, the commit sequence advances when there is any contact.
+__global__ void k_cap_lag_total(int* acnt) { acnt[AC_NTOT] = acnt[AC_LAG] + acnt[AC_NCAND]; }
+__global__ void k_cap_lag_advance(int* acnt, int lagCap) {
+  if (acnt[AC_NCAND] > 0) {
+    if (acnt[AC_NTOT] > lagCap) acnt[AC_ERR] |= ACE_CAPACITY;
+    else acnt[AC_LAG] = acnt[AC_NTOT];
+  }
+  if (acnt[AC_NA] > 0) acnt[AC_COMMIT] += 1;
+}
+__global__ void k_cap_copy_vals(double4* dst, const double4* src, int cap, const int* dn) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < min(cap, *dn)) dst[i] = src[i];
+}
+
+void ContactHost::cap_bind(Solver& s) {
+  bind(s);
+  Contact& c = s.d.c;
+  c.nActive = (int)actCap;      // launch sizes
+  c.nActiveD = acnt + AC_NA;    // the count kernels use
+}
+
+int ContactHost::cand_blocks_cap() const {
+  const long bound = 15l * (long)supCap + 12l * (long)(ms > 0 ? supSCap : 0);
+  return (int)std::max(1l, std::min((bound + kCT - 1) / kCT, 8l * smCount));
+}
+
+void ContactHost::cap_begin_step(Solver& s, GraphCtx& g) {
+  cudaStream_t st = g.cur();
+  k_cap_begin<<<1, 1, 0, st>>>(diag, acnt);
+  CK(cudaMemsetAsync(lagFloorOk, 0, (size_t)n, st));
+  launch_counter()++;
+  fricOn = false;
+  cap_bind(s);
+}
+
+void ContactHost::cap_superset(Solver& s, GraphCtx& g, const double* x) {
+  cudaStream_t st = g.cur();
+  int64_t& lc = launch_counter();
+  const double padSup = sup_pad();
+  CK(cudaMemcpyAsync(supBase, x, 3 * (size_t)n * 8, cudaMemcpyDeviceToDevice, st));
+  bvh_build(bvh, s.d.x0, x, padSup, false, st, &lc);
+  CK(cudaMemsetAsync(cint, 0, CI_N * sizeof(int), st));
+  BvhBufs sb = bvh;
+  sb.cnt = (uint32_t*)(cint + CI_SELF);
+  sb.pairs = supPairs;
+  sb.pairCap = (uint32_t)supCap;
+  bvh_append_self(sb, st, &lc);
+  if (ms > 0) bvh_append_static(bvh, padSup, supSPairs, (uint32_t)supSCap, (uint32_t*)(cint + CI_STATIC), st, &lc);
+  k_cap_sup_counts<<<1, 1, 0, st>>>(cint, acnt, (long)supCap, (long)supSCap, (long)pairCap, (long)spairCap,
+                                    (long)flagCap, ms > 0 ? 1 : 0);
+  lc++;
+}
+
+// launch_query, then (conditional node) the superset rebuilt around x and the
+// query repeated when x left the superset's 4 mm travel.
+void ContactHost::cap_query(Solver& s, GraphCtx& g, const double* x, double pad) {
+  int64_t& lc = launch_counter();
+  auto query = [&](cudaStream_t st) {
+    CK(cudaMemsetAsync(cint, 0, CI_N * sizeof(int), st));
+    const int n3 = 3 * n;
+    k_moved<<<std::min(1184, (n3 + 255) / 256), 256, 0, st>>>(x, supBase, n3, kSupTravel, cint);
+    bvh_boxes(bvh, s.d.x0, x, pad, st, &lc);
+    filter_pairs_dev(bvh, supPairs, (int)supCap, bvh.pairs, (uint32_t)pairCap, (uint32_t*)(cint + CI_SELF), supSPairs,
+                     ms > 0 ? (int)supSCap : 0, pad, spairs, (uint32_t)spairCap, (uint32_t*)(cint + CI_STATIC),
+                     acnt + AC_NSUP, st, &lc);
+    lc++;
+  };
+  query(g.cur());
+  const cudaGraphConditionalHandle h = g.handle(0);
+  k_cap_cond_moved<<<1, 1, 0, g.cur()>>>(cint, h);
+  lc++;
+  g.push(h, cudaGraphCondTypeIf);
+  cap_superset(s, g, x);
+  query(g.cur());
+  k_cap_err_moved<<<1, 1, 0, g.cur()>>>(cint, acnt);
+  lc++;
+  g.pop();
+}
+
+void ContactHost::cap_update_active_set(Solver& s, GraphCtx& g, const double* x) {
+  cap_query(s, g, x, p.dhat);
+  cudaStream_t st = g.cur();
+  int64_t& lc = launch_counter();
+  CView v = cview(*this, s);
+  k_active_reset<<<1, 1, 0, st>>>(v);
+  k_cand_flags<<<cand_blocks_cap(), kCT, 0, st>>>(v, x, cand.cap, cand.k0, cand.p0);
+  k_floor_flags<<<cnb(n), kCT, 0, st>>>(v, x);
+  k_active_min<<<1, 1, 0, st>>>(v);
+  lc += 4;
+  scan_counts(fflag, n, (uint32_t*)(cint + CI_NFLOOR), st, &lc);
+  k_cap_active_counts<<<1, 1, 0, st>>>(cint, acnt, cand.cap, (int)actCap);
+  lc++;
+  const bool flip = radix_sort_dev<4>(cand.k0, cand.p0, cand.k1, cand.p1, acnt + AC_NCAND, cand.cap,
+                                      cand_key_bits(idBits, 0), cand.hist, st, &lc);
+  k_cand_active<<<cnb(cand.cap), kCT, 0, st>>>(v, x, flip ? cand.p1 : cand.p0, -1);
+  k_floor_compact<<<cnb(n), kCT, 0, st>>>(v, x);
+  k_csr_records<<<cnb(4l * (long)actCap), kCT, 0, st>>>(v, rk0, rp0, -1);
+  lc += 3;
+  // 32-bit keys: an even number of passes leaves the result in (rk0, rp0)
+  radix_sort_dev<1>(rk0, rp0, rk1, rp1, acnt + AC_NREC, 4 * (int)actCap, 32, rhist, st, &lc);
+  k_csr_offsets<<<cnb(n + 1), kCT, 0, st>>>(rk0, 0, cOff, n, acnt + AC_NA);
+  lc++;
+  cap_bind(s);
+}
+
+void ContactHost::cap_gradient_terms(Solver& s, GraphCtx& g) {
+  cap_update_active_set(s, g, s.d.x);
+  cudaStream_t st = g.cur();
+  CView v = cview(*this, s);
+  const long cap = (long)actCap;
+  k_contact_prep<<<cnb(cap), kCT, 0, st>>>(v, s.d.x, -1);
+  k_contact_chains<<<1, 64, 0, st>>>(v, -1);
+  k_contact_grad_rec<<<cnb(4 * cap), kCT, 0, st>>>(v, (int)(4 * cap));
+  k_contact_grad_gather<<<cnb(n), kCT, 0, st>>>(v, s.d.cgrad);
+  k_contact_curv<<<cnb(cap), kCT, 0, st>>>(v, s.d.x, -1);
+  k_contact_diag_rec<<<cnb(4 * cap), kCT, 0, st>>>(v, (int)(4 * cap));
+  k_contact_diag_gather<<<cnb(n), kCT, 0, st>>>(v, s.d.diag);
+  launch_counter() += 7;
+}
+
+void ContactHost::cap_friction_terms(Solver& s, GraphCtx& g) {
+  fricOn = true;
+  cap_bind(s);
+  CView v = cview(*this, s);
+  k_contact_fric<<<cnb((long)actCap), kCT, 0, g.cur()>>>(v, s.d.x, -1, fh);
+  launch_counter()++;
+}
+
+void ContactHost::cap_merit_energy(Solver& s, GraphCtx& g, const double* x) {
+  CView v = cview(*this, s);
+  k_contact_merit<<<cnb((long)actCap), kCT, 0, g.cur()>>>(v, x, -1);
+  launch_counter()++;
+}
+
+void ContactHost::cap_trial(Solver& s, GraphCtx& g, const double* xt) {
+  cap_query(s, g, xt, p.dmin);
+  cudaStream_t st = g.cur();
+  CView v = cview(*this, s);
+  k_trial_reset<<<1, 1, 0, st>>>(v);
+  k_trial_cand<<<cand_blocks_cap(), kCT, 0, st>>>(v, xt, p.dmin);
+  k_trial_bad_lo<<<4 * smCount, kCT, 0, st>>>(v);
+  k_trial_floor<<<cnb(n), kCT, 0, st>>>(v, xt, p.dmin);
+  k_trial_final<<<1, 1, 0, st>>>(v, p.dmin);
+  launch_counter() += 5;
+}
+
+void ContactHost::cap_commit(Solver& s, GraphCtx& g, const double* x) {
+  cudaStream_t st = g.cur();
+  int64_t& lc = launch_counter();
+  const int lagSort = (int)std::min<size_t>(lagCap, kBlockSortMax);
+  CView v = cview(*this, s);
+  // the sorted prefix becomes entries 0..lagCount-1 with their values in place
+  k_cap_copy_vals<<<cnb(lagSort), kCT, 0, st>>>(lval, lsorted, lagSort, acnt + AC_LAG);
+  k_iota<<<cnb(lagSort), kCT, 0, st>>>(lp0, lagSort, acnt + AC_LAG);
+  k_contact_commit<<<cnb((long)actCap), kCT, 0, st>>>(v, x, -1, lk0, lp0, lval, 0, 0);
+  k_cap_lag_total<<<1, 1, 0, st>>>(acnt);
+  lc += 4;
+  // one-block sort (192-bit keys, an even number of passes: the result stays in
+  // (lk0, lp0)); a table past its capacity is reported, not sorted
+  radix_sort_dev<6>(lk0, lp0, lk1, lp1, acnt + AC_NTOT, lagSort, 192, lhist, st, &lc);
+  k_gather_vals<<<cnb(lagSort), kCT, 0, st>>>(lval, lp0, lagSort, lsorted, acnt + AC_NTOT);
+  k_cap_lag_advance<<<1, 1, 0, st>>>(acnt, lagSort);
+  lc += 2;
+}
+
+void ContactHost::cap_kill_approach_velocity(Solver& s, GraphCtx& g) {
+  cap_update_active_set(s, g, s.d.x);
+  cudaStream_t st = g.cur();
+  CView v = cview(*this, s);
+  const long cap = (long)actCap;
+  k_kill_pred<<<cnb(4 * cap), kCT, 0, st>>>(v, rk0, rp0, cOff, (int)(4 * cap), (int)cap, kpred);
+  k_kill_vtee_rounds<<<1, kKillThreads, 48 * 1024, st>>>(v, s.d.v, (int)cap, kpred);
+  k_kill_vtee<<<1, 1, 0, st>>>(v, s.d.v, (int)cap);
+  k_kill_floor<<<cnb(cap), kCT, 0, st>>>(v, s.d.v, 0, (int)cap);
+  launch_counter() += 4;
+}
+
+void ContactHost::cap_collect(const int* ha, const int* hc, double rejectionsDev) {
+  nCand = ha[AC_NCAND];
+  nFloor = ha[AC_NFLOOR];
+  nVT = ha[AC_NVT];
+  lagCount = ha[AC_LAG];
+  commitNo = ha[AC_COMMIT];
+  nSup = ha[AC_NSUP];
+  nSupS = ha[AC_NSUPS];
+  candidatePairs = 15.0 * (uint32_t)hc[CI_SELF] + 12.0 * (uint32_t)(ms > 0 ? hc[CI_STATIC] : 0);
+  activePairs = nCand + nFloor;
+  vtPairs = nVT;
+  eePairs = nCand - nVT;
+  floorPairs = nFloor;
+  rejections = rejectionsDev;
+  supValid = false;  // the next host-driven query rebuilds the superset
+}
+
+void ContactHost::cap_grow(Solver& s, const int* ha, const int* hc) {
+  (void)ha;
+  (void)hc;
+  // Counts past a capacity were clamped on the device, so grow by doubling;
+  // the host-driven repeat of the step grows further as it needs.
+  ensure_cands(2 * (size_t)cand.cap);
+  ensure_active(s, 2 * actCap);
+  ensure_lag(2 * lagCap);
+  ensure_pairs(2 * pairCap, 2 * spairCap);
+  ensure_flags(2 * flagCap);
+  supCap = 2 * supCap;
+  dalloc(supPairs, supCap);
+  if (ms > 0) {
+    supSCap = 2 * supSCap;
+    dalloc(supSPairs, supSCap);
+  }
+  supValid = false;
+}
+
 void set_contact(Solver& s, const cs_contact_params* p, int floor_on, double floor_y, const float* sp, int ns,
                  const uint32_t* si, int ms) {
   if (!p) {
     s.contact.reset();
     s.d.hasContact = 0;
+    s.initEpoch++;
     return;
   }
   if (!(p->dhat > 0) || !(p->dmin >= 0) || !(p->kappa >= 0) || !(p->eps > 0) || !(p->mu >= 0))
@@ -1350,6 +1759,7 @@ void set_contact(Solver& s, const cs_contact_params* p, int floor_on, double flo
   auto c = std::make_unique<ContactHost>();
   c->init(s, p, floor_on, floor_y, sp, ns, si, ms);
   s.contact = std::move(c);
+  s.initEpoch++;
 }
 
 }  // namespace cs

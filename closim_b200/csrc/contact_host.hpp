@@ -11,6 +11,7 @@
 
 #include "../../include/closim_cuda.h"
 #include "broadphase.cuh"
+#include "graph_ctx.hpp"
 #include "plain.cuh"
 
 namespace cs {
@@ -33,6 +34,15 @@ enum CInt { CI_SELF = 0, CI_STATIC, CI_OVERFLOW, CI_NCAND, CI_NFLOOR, CI_NVT, CI
             CI_FLOORBAD, CI_NBAD, CI_N = 16 };
 // Failing trial candidates listed by index for the second key pass.
 constexpr int kBadCap = 4096;
+// Device-side counts of a graph-captured step (ContactHost::acnt, int32): the
+// frozen set layout, the lag table, the superset sizes and an error word. In a
+// captured step every launch is sized for its buffer's capacity and the kernels
+// read these; the host reads them once, after the step.
+enum ACnt { AC_NCAND = 0, AC_NFLOOR, AC_NVT, AC_NA, AC_LAG, AC_COMMIT, AC_NSUP, AC_NSUPS, AC_ERR, AC_NREC, AC_NTOT,
+            AC_N = 16 };
+// AC_ERR bits: a buffer capacity was exceeded, or a query fell outside a
+// freshly rebuilt superset; the step is then repeated on the host-driven path.
+enum ACErr { ACE_CAPACITY = 1, ACE_SUPERSET = 2 };
 
 class ContactHost {
  public:
@@ -86,6 +96,10 @@ class ContactHost {
   uint32_t* cOff = nullptr;    // n + 1
   int* kpred = nullptr;        // 4 per contact: predecessor on each vertex (restitution pass)
   double* recScratch = nullptr;  // 6 per record (4 per contact): per-record contact shares before their ordered sums
+  // exact-Newton friction potential (see Contact::fric): 8 + 3 per contact
+  double* fh = nullptr;
+  double* fdd = nullptr;
+  bool fricOn = false;         // set by friction_terms for the rest of the step
   // lagged normals / multipliers
   double* lagFloor = nullptr;  // n
   uint8_t* lagFloorOk = nullptr;
@@ -114,6 +128,9 @@ class ContactHost {
   }
   void update_active_set(Solver& s, double* x);
   void merit_energy(Solver& s, const double* x);
+  // Exact-Newton mode: freeze the friction potential at the current iterate
+  // (fh) and include it in the merit and the Newton matrix from now on.
+  void friction_terms(Solver& s);
   void gradient_terms(Solver& s);
   // Trial validity with one host synchronization (bisection, commit).
   bool check_trial(Solver& s, const double* xt);
@@ -127,9 +144,37 @@ class ContactHost {
   void commit(Solver& s, const double* x);
   void kill_approach_velocity(Solver& s);
   void fill_stats(Solver& s, cs_step_stats& st);
+  // Replaces the static mesh's vertex positions (same triangles), for a
+  // collider that moves between steps (ContactSystem.setStaticMesh with the
+  // sampled pose, avatar-collider.ts:205-237).
+  void update_static_positions(Solver& s, const float* sp, int nsv);
+  // The frozen active set of the last update (kind, p, a, b, c, d and
+  // w0..w3, n), in active-list order; returns its size.
+  int read_active(Solver& s, int cap, int32_t* ids6, double* w7);
   // broadphase stage only: the pairs of a segment xStep -> x with pad, counted on the device
   void launch_query(Solver& s, const double* x, double pad);
   void bind(Solver& s);  // refresh the Contact view inside the solver's Dev
+
+  // ---- graph-captured step (graph_step.cu): the same work, launched into a
+  // capture with every count read on the device (acnt) and every launch sized
+  // for its buffer's capacity; overflows set acnt[AC_ERR] instead of growing.
+  int* acnt = nullptr;         // AC_N device ints
+  void cap_bind(Solver& s);
+  void cap_begin_step(Solver& s, GraphCtx& g);
+  void cap_superset(Solver& s, GraphCtx& g, const double* x);
+  void cap_query(Solver& s, GraphCtx& g, const double* x, double pad);
+  void cap_update_active_set(Solver& s, GraphCtx& g, const double* x);
+  void cap_gradient_terms(Solver& s, GraphCtx& g);
+  void cap_friction_terms(Solver& s, GraphCtx& g);
+  void cap_merit_energy(Solver& s, GraphCtx& g, const double* x);
+  void cap_trial(Solver& s, GraphCtx& g, const double* xt);
+  void cap_commit(Solver& s, GraphCtx& g, const double* x);
+  void cap_kill_approach_velocity(Solver& s, GraphCtx& g);
+  // After a replay (one host read): the stats the host path keeps on the host.
+  void cap_collect(const int* hacnt, const int* hcint, double rejectionsDev);
+  // After a replay that set AC_ERR: grow every capacity a captured step cannot.
+  void cap_grow(Solver& s, const int* hacnt, const int* hcint);
+  int cand_blocks_cap() const;
  private:
   void read_ints(Solver& s);
   void ensure_pairs(size_t np, size_t nsp);

@@ -335,7 +335,7 @@ __global__ void __launch_bounds__(kThreads) k_mx_pcg(MxArgs A) {
     if (d.hasContact) {
       // frozen-barrier coefficients in FP64 (contact-assembly.ts:371-387)
       const Contact& c = d.c;
-      for (int i = tid; i < c.nActive; i += nth) {
+      for (int i = tid, na = n_active(c); i < na; i += nth) {
         const Frozen f = c.active[i];
         const double dist = js_max(frozen_dist(c, d.x, f), 1e-12);
         double jv;
@@ -498,10 +498,10 @@ __global__ void __launch_bounds__(kThreads) k_mx_sum_terms(const double* t, int 
 // is summed over the same block partition as a k_mx_sum_terms launch of gridDim.x.
 __global__ void __launch_bounds__(kThreads) k_mx_sum_terms3(const double* t0, int n0, const double* t1, int n1,
                                                            const double* t2, int n2, double* p0, double* p1,
-                                                           double* p2) {
+                                                           double* p2, const int* dn2) {
   __shared__ double sm[32];
   const double* t = blockIdx.y == 0 ? t0 : blockIdx.y == 1 ? t1 : t2;
-  const int n = blockIdx.y == 0 ? n0 : blockIdx.y == 1 ? n1 : n2;
+  const int n = blockIdx.y == 0 ? n0 : blockIdx.y == 1 ? n1 : (dn2 ? min(n2, *dn2) : n2);
   double* part = blockIdx.y == 0 ? p0 : blockIdx.y == 1 ? p1 : p2;
   double s = 0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) s += t[i];
@@ -574,7 +574,8 @@ void mx_energy_final(const Dev& d, cudaStream_t s, int64_t* lc) {
                           d.partStride);
   k_mx_sum_terms3<<<dim3(nb, 3), kThreads, 0, s>>>(d.T0, d.n * 3, d.T1, d.m + (d.kb > 0 ? d.hg : 0), d.Tc,
                                                    d.hasContact ? d.c.nActive : 0, d.part + 2 * d.partStride,
-                                                   d.part + 3 * d.partStride, d.part + 4 * d.partStride);
+                                                   d.part + 3 * d.partStride, d.part + 4 * d.partStride,
+                                                   d.hasContact ? d.c.nActiveD : nullptr);
   k_mx_energy_final<<<1, 32, 0, s>>>(d, nb);
   *lc += 2;
 }

@@ -122,6 +122,21 @@ __device__ __forceinline__ double cl_jvp(const Frozen& f, const float* z, const 
   return f.w0 * nv[0] + f.w1 * nv[1] + f.w2 * nv[2] + f.w3 * nv[3];
 }
 
+// Relative-slip Jacobian along the current direction (slip_jvp with p formed
+// on the fly), for the exact-Newton friction term. FP64.
+__device__ __forceinline__ void cl_slip_jvp(const Frozen& f, const float* z, const float* pc, float beta, bool first,
+                                            double o[3]) {
+  o[0] = o[1] = o[2] = 0;
+  auto V = [&](int q, double s) {
+    if (q < 0) return;
+    const float3 pv = ld_p(z, pc, beta, first, q);
+    o[0] += s * (double)pv.x; o[1] += s * (double)pv.y; o[2] += s * (double)pv.z;
+  };
+  if (f.kind == 2) { V(f.p, 1.0); return; }
+  if (f.kind == 0) { V(f.p, 1.0); V(f.a, -f.w0); V(f.b, -f.w1); return; }
+  V(f.a, f.w0); V(f.b, f.w1); V(f.c, f.w2); V(f.d, f.w3);
+}
+
 // Phase B on K Schwarz domains dom0, dom0 + step, ... at once (one warp, lane =
 // local dof): the loads of all K are issued before any product, so their
 // latencies overlap. Adds the (r.r, r.z) shares.
@@ -258,7 +273,7 @@ __global__ void __launch_bounds__(kClT, 1) k_mx_pcg_cluster(ClArgs A) {
   }
   if (d.hasContact) {
     const Contact& c = d.c;
-    for (int i = tid; i < c.nActive; i += nth) {
+    for (int i = tid, na = n_active(c); i < na; i += nth) {
       const double dist = js_max(frozen_dist(c, d.x, c.active[i]), 1e-12);
       A.coef[i] = dist < c.dHat ? barrier_curvature(dist, c.dHat, c.kappa) : 0.0;
     }
@@ -307,6 +322,16 @@ __global__ void __launch_bounds__(kClT, 1) k_mx_pcg_cluster(ClArgs A) {
           if (g != 0) {
             const Frozen f = c.active[rec >> 2];
             dist_grad_slot(f, rec & 3, g * cl_jvp(f, mb.z, pc, beta, first), ch);
+          }
+          if (c.fric) {  // exact-Newton mode: friction potential Hessian
+            const double* fh = c.fh + (size_t)(rec >> 2) * 8;
+            if (fh[1] != 0) {
+              const Frozen f = c.active[rec >> 2];
+              double du[3], F[3];
+              cl_slip_jvp(f, mb.z, pc, beta, first, du);
+              fric_hess_apply(fh, du, F);
+              slip_jt_slot(f, rec & 3, F, ch);
+            }
           }
           double* o = c.recScratch + (size_t)q * 3;
           o[0] = ch[0]; o[1] = ch[1]; o[2] = ch[2];

@@ -12,8 +12,13 @@ namespace cs {
 enum ScalarSlot {
   S_GRADNORM = 0, S_MAXSTRAIN, S_ENERGY_TRIAL, S_GTDX, S_PCG_ITERS, S_PCG_RES, S_E_INERTIA,
   S_E_TRI, S_E_MERIT, S_E_HINGE, S_FALLBACK, S_MAXDX, S_VALID, S_MINDIST, S_MINTOI, S_CCDFAIL,
-  S_BARRIER_E, S_FWORK, S_CH0 = 24, S_CH1, S_CH2, S_CH3, S_NSCALARS = 32
+  S_BARRIER_E, S_FWORK, S_ENERGY_BASE, S_CH0 = 24, S_CH1, S_CH2, S_CH3, S_NSCALARS = 32
 };
+
+// Active contacts as seen by a kernel: the device count in a graph-captured
+// step, else the host's.
+struct Contact;
+__device__ __forceinline__ int n_active(const Contact& c);
 
 // One frozen contact (contact-assembly.ts:22-30): kind 0 VT, 1 EE, 2 floor.
 // Ids < 0 other than -1 are static vertices -(i + 2).
@@ -29,13 +34,26 @@ struct Contact {
   int ns;                  // static vertices
   const float* spos;       // 3 ns
   int nActive;             // active records (VT/EE first, then floor)
+  const int* nActiveD;     // graph-captured steps: the device's count (else null)
   const Frozen* active;
   double* dd;              // per-contact scalar (HVP coefficient, diag curvature, ...)
   double* cg;              // 4 per contact: barrier dE/dd, friction force args (-f)
   const uint32_t* cOff;    // n+1: vertex -> records (contact << 2 | slot), contact order
   const uint32_t* cRec;
   double* recScratch;      // 6 per record: per-record contact shares, summed per vertex in record order
+  // Exact-Newton mode only (fric = 1): lagged friction as the potential
+  // D = mu lambda sqrt(|P u|^2 + eps^2) of the relative slip u, with lambda and
+  // the normal frozen for the Newton iteration. fh (8 per contact: mu lambda,
+  // s = mu lambda / |.|, t = P u / |.|, n) feeds its Hessian s (P - t t^T) to the
+  // HVP and D to the merit; fdd (3 per contact) holds the HVP's per-contact
+  // friction share. The reference mode keeps friction out of both (as
+  // contact-assembly.ts:371-428 does).
+  int fric;
+  const double* fh;
+  double* fdd;
 };
+
+__device__ __forceinline__ int n_active(const Contact& c) { return c.nActiveD ? *c.nActiveD : c.nActive; }
 
 // Everything a kernel of the FP64 path needs, passed by value.
 struct Dev {

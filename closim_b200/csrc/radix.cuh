@@ -28,9 +28,12 @@ __device__ __forceinline__ uint32_t digit_of(const Key<KW>& k, int pass) {
   return (k.w[word] >> ((pass % 4) * 8)) & 0xffu;
 }
 
+// dn (optional): the element count, read on the device when the launch was
+// sized for a capacity n (graph-captured steps, where the host does not know it).
 template <int KW>
 __global__ void __launch_bounds__(kSortThreads) k_radix_hist(const Key<KW>* keys, int n, int pass, uint32_t* hist,
-                                                             int ntiles) {
+                                                             int ntiles, const int* dn = nullptr) {
+  if (dn) n = min(n, *dn);
   __shared__ uint32_t h[256];
   h[threadIdx.x] = 0;
   __syncthreads();
@@ -88,7 +91,8 @@ static __global__ void __launch_bounds__(1024) k_scan_exclusive(uint32_t* a, int
 template <int KW>
 __global__ void __launch_bounds__(kSortThreads) k_radix_scatter(const Key<KW>* kin, const uint32_t* pin, Key<KW>* kout,
                                                                 uint32_t* pout, int n, int pass, const uint32_t* offs,
-                                                                int ntiles) {
+                                                                int ntiles, const int* dn = nullptr) {
+  if (dn) n = min(n, *dn);
   __shared__ uint32_t running[256];
   __shared__ uint32_t wcount[kSortThreads / 32][256];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -139,7 +143,9 @@ constexpr int kBlockSortMax = 32768;
 
 template <int KW>
 __global__ void __launch_bounds__(kBlockSortThreads) k_block_radix(Key<KW>* k0, uint32_t* p0, Key<KW>* k1,
-                                                                   uint32_t* p1, int n, int passes) {
+                                                                   uint32_t* p1, int n, int passes,
+                                                                   const int* dn = nullptr) {
+  if (dn) n = max(0, min(n, *dn));
   __shared__ uint32_t cnt[kBlockSortThreads / 32][256];
   __shared__ uint32_t tot[256];
   __shared__ uint32_t orw[KW], andw[KW];
@@ -272,6 +278,35 @@ bool radix_sort(Key<KW>* k0, uint32_t* p0, Key<KW>* k1, uint32_t* p1, int n, int
     k_radix_hist<KW><<<ntiles, kSortThreads, 0, s>>>(ki, n, pass, hist, ntiles);
     k_scan_exclusive<<<1, 1024, 0, s>>>(hist, 256 * ntiles, nullptr);
     k_radix_scatter<KW><<<ntiles, kSortThreads, 0, s>>>(ki, pi, ko, po, n, pass, hist, ntiles);
+    if (launches) *launches += 3;
+    flip = !flip;
+  }
+  return flip;
+}
+
+// The same sort with the element count read on the device (*dn, at most cap):
+// every launch is sized for cap, so the sequence can be captured in a graph
+// before the count exists. The result lands where radix_sort would put it for
+// the same `bits` (the returned flag depends on cap and bits only).
+template <int KW>
+bool radix_sort_dev(Key<KW>* k0, uint32_t* p0, Key<KW>* k1, uint32_t* p1, const int* dn, int cap, int bits,
+                    uint32_t* hist, cudaStream_t s, int64_t* launches) {
+  const int passes = (bits + 7) / 8;
+  if (cap <= kBlockSortMax) {
+    k_block_radix<KW><<<1, kBlockSortThreads, 0, s>>>(k0, p0, k1, p1, cap, passes, dn);
+    if (launches) *launches += 1;
+    return (passes & 1) != 0;
+  }
+  const int ntiles = (cap + kSortTile - 1) / kSortTile;
+  bool flip = false;
+  for (int pass = 0; pass < passes; pass++) {
+    const Key<KW>* ki = flip ? k1 : k0;
+    const uint32_t* pi = flip ? p1 : p0;
+    Key<KW>* ko = flip ? k0 : k1;
+    uint32_t* po = flip ? p0 : p1;
+    k_radix_hist<KW><<<ntiles, kSortThreads, 0, s>>>(ki, cap, pass, hist, ntiles, dn);
+    k_scan_exclusive<<<1, 1024, 0, s>>>(hist, 256 * ntiles, nullptr);
+    k_radix_scatter<KW><<<ntiles, kSortThreads, 0, s>>>(ki, pi, ko, po, cap, pass, hist, ntiles, dn);
     if (launches) *launches += 3;
     flip = !flip;
   }

@@ -142,6 +142,37 @@ int cs_membrane_hvp_analytic(cs_solver* h, const double* x, const double* p, dou
     h->s.membrane_hvp_analytic(x, p, out);
   });
 }
+int cs_contact_active(cs_solver* h, int32_t cap, int32_t* count, int32_t* ids6, double* w7) {
+  int rc = CS_OK;
+  const int g = guarded(h, [&] {
+    if (!count) throw std::invalid_argument("null argument");
+    if (!h->s.ready) throw std::logic_error("CpuSolver not initialized");
+    *count = h->s.contact ? h->s.contact->read_active(h->s, cap, ids6, w7) : 0;
+    if (*count > cap && ids6) rc = CS_E_CAPACITY;
+  });
+  return g != CS_OK ? g : rc;
+}
+int cs_update_static_positions(cs_solver* h, const float* static_pos, int32_t ns) {
+  return guarded(h, [&] {
+    if (!static_pos) throw std::invalid_argument("null argument");
+    if (!h->s.ready) throw std::logic_error("CpuSolver not initialized");
+    if (!h->s.contact) throw std::invalid_argument("no contact system");
+    h->s.contact->update_static_positions(h->s, static_pos, ns);
+  });
+}
+int cs_set_graph_mode(cs_solver* h, int32_t enable) {
+  return guarded(h, [&] {
+    if (enable != 0 && enable != 1) throw std::invalid_argument("graph mode is 0 or 1");
+    h->s.graphMode = enable;
+  });
+}
+int cs_graph_info(cs_solver* h, int64_t* out2) {
+  return guarded(h, [&] {
+    if (!out2) throw std::invalid_argument("null argument");
+    out2[0] = h->s.graphSteps;
+    out2[1] = h->s.graphFallbacks;
+  });
+}
 int cs_last_stats(cs_solver* h, cs_step_stats* out) {
   return guarded(h, [&] {
     if (!h->s.haveStats) throw std::logic_error("CpuSolver not initialized: no step taken");

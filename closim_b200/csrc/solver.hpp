@@ -170,6 +170,7 @@ class Solver {
   }
 
   ~Solver() {
+    graph_release();
     if (pev0) cudaEventDestroy(pev0);
     if (pev1) cudaEventDestroy(pev1);
     if (hscal) cudaFreeHost(hscal);
@@ -307,7 +308,9 @@ class Solver {
     }
     upload_pins();
     contact.reset();
+    if (precision == CS_PRECISION_MIXED && mxCluster > 0) contact_free_valid();
     CK(cudaStreamSynchronize(stream));
+    initEpoch++;
     ready = true;
   }
 
@@ -339,9 +342,26 @@ class Solver {
     CK(cudaStreamSynchronize(stream));
   }
 
+  // ---- graph-captured step (graph_step.cu) ---------------------------------------
+  struct GraphStep;
+  GraphStep* gstep = nullptr;
+  int graphMode = 1;           // 1: the captured step where it applies (cs_set_graph_mode)
+  int64_t graphSteps = 0, graphFallbacks = 0;
+  int initEpoch = 0;           // bumped by initialize / set_contact: the captured graph is stale
+  DBuf<int> validOne;          // an always-valid trial flag for steps without contact
+  void graph_release();
+  std::vector<double> graph_key(double h) const;
+  void graph_capture(double h);
+  const int* contact_free_valid();
+  // One step as a captured graph replay with the decisions on the device;
+  // false when the configuration is not covered (or a buffer overflowed and
+  // the state was restored), and the caller runs the host-driven step.
+  bool step_graph(double h);
+
   // One implicit-Euler step (newton.ts:27-232).
   void step(double h) {
     if (!ready) throw std::logic_error("CpuSolver not initialized");
+    if (step_graph(h)) return;
     d.h = h;
     d.invH2 = 1 / (h * h);
     for (int k = 0; k < 3; k++) d.gravity[k] = gravity[k];
@@ -380,6 +400,16 @@ class Solver {
         launch_grad(d, stream, newtonMode == 1);
         lc += 3 + (d.kb > 0 && d.hg > 0);
       }
+      // Exact-Newton mode: the lagged friction becomes a potential frozen for
+      // this iteration (in the merit and the Newton matrix, so the Newton
+      // direction is a descent direction of the merit), and the Armijo base
+      // energy is re-evaluated with it at x.
+      const bool fricExact = newtonMode == 1 && contact && contact->p.mu > 0;
+      if (fricExact) {
+        contact->friction_terms(*this);
+        contact->merit_energy(*this, d.x);
+        energy_of(d.x);
+      }
       // The convergence test needs the gradient norm on the host. With a line
       // search ahead, the solve and the first trial are enqueued before it is
       // read and the norm comes back with the trial's synchronization: when
@@ -392,6 +422,7 @@ class Solver {
         read_scalars();
         gradNorm = hscal[S_GRADNORM];
         maxStrain = hscal[S_MAXSTRAIN];
+        if (fricExact) energy = hscal[S_ENERGY_TRIAL];
         if (!std::isfinite(gradNorm)) throw NonFinite();
         if (gradNorm < opts.grad_tol) { converged = true; break; }
         gradRead = true;
@@ -680,6 +711,7 @@ class Solver {
         d.invH2 = 1 / (ro.h * ro.h);
         if (contact) {
           contact->begin_segment(*this);
+          contact->fricOn = false;  // the adjoint holds friction constant
           contact->update_active_set(*this, x1);
         }
         launch_diag_init(d, beta, stream);

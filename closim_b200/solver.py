@@ -351,6 +351,43 @@ class CudaSolver:
         self._check(self._lib.cs_membrane_hvp(self._h, L.ptr(x), L.ptr(p), L.ptr(out)))
         return out
 
+    def activeContacts(self):
+        """ContactSystem.active after the last step: (ids [k, 6] int32: kind,
+        p, a, b, c, d; weights [k, 7]: w0..w3, nx, ny, nz), in list order."""
+        self._need()
+        k = C.c_int32(0)
+        self._check(self._lib.cs_contact_active(self._h, 0, C.byref(k), None, None))
+        ids = np.zeros(max(k.value, 1) * 6, np.int32)
+        w = np.zeros(max(k.value, 1) * 7)
+        self._check(self._lib.cs_contact_active(self._h, max(k.value, 1), C.byref(k), L.ptr(ids), L.ptr(w)))
+        return ids[:k.value * 6].reshape(-1, 6), w[:k.value * 7].reshape(-1, 7)
+
+    def setStaticPositions(self, positions) -> None:
+        """Moves the scene's static collider mesh (same triangles) before the
+        next step: ContactSystem.setStaticMesh with a collider's sampled pose
+        (src/collision/avatar-collider.ts:205-237). The scene's ContactSystem
+        keeps the new positions."""
+        self._need()
+        c = self.scene.contact
+        if c is None or c.staticPos is None:
+            raise ClothSolverError("the scene has no static mesh")
+        pos = np.ascontiguousarray(positions, np.float32).reshape(-1)
+        if pos.size != c.staticPos.size:
+            raise ValueError("static positions must keep the static mesh's vertex count")
+        self._check(self._lib.cs_update_static_positions(self._h, L.ptr(pos), pos.size // 3))
+        c.staticPos = pos.copy()
+
+    def setGraphMode(self, enable: bool) -> None:
+        """Graph-captured steps with device-side Newton/Armijo control (default
+        on; applies to the mixed path's one-cluster sheets); off forces the
+        host-driven step."""
+        self._check(self._lib.cs_set_graph_mode(self._h, 1 if enable else 0))
+
+    def graphInfo(self) -> dict:
+        out = np.zeros(2, np.int64)
+        self._check(self._lib.cs_graph_info(self._h, L.ptr(out)))
+        return dict(graphSteps=int(out[0]), hostRepeats=int(out[1]))
+
     def kernelLaunches(self) -> int:
         return int(self._lib.cs_kernel_launches(self._h))
 

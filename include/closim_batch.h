@@ -14,8 +14,9 @@
  * from a work list ordered largest first and runs that sheet's whole implicit
  * step with block barriers only. cs_batch_step with steps > 1 captures the
  * sequence once into a CUDA graph and replays it. cs_batch_autotune times the
- * candidate launch shapes (256, 512 or 1024 threads per block, all resident
- * blocks or a half or a third of them) on the batch's own state (restored
+ * candidate launch shapes (128, 256 or 512 threads per block, i.e. vertices
+ * per thread of a sheet; all resident blocks or a half or a third of them,
+ * i.e. sheets in flight per SM) on the batch's own state (restored
  * afterwards) and keeps the fastest: fewer blocks keep fewer sheets in flight,
  * whose working sets then stay in L2.
  */

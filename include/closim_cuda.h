@@ -127,6 +127,32 @@ int cs_last_stats(cs_solver* s, cs_step_stats* out);
  * on the initialized mesh and current material. Host arrays of 3n doubles. */
 int cs_membrane_hvp(cs_solver* s, const double* x, const double* p, double* out);
 
+/* A collider that moves between steps: replaces the static mesh's ns vertex
+ * positions (f32, the same triangles as cs_set_contact gave), as
+ * ContactSystem.setStaticMesh with a collider's sampled pose does
+ * (src/collision/avatar-collider.ts:205-237, attachCollisionObject). Within a
+ * step the static mesh stays where it was put, as in the reference. */
+int cs_update_static_positions(cs_solver* s, const float* static_pos, int32_t ns);
+
+/* ContactSystem.active (contact-assembly.ts:50): the frozen active set of the
+ * last update (after cs_step: the one its restitution pass used), in
+ * active-list order. *count receives its size; when ids6 (6 per record: kind
+ * 0 VT / 1 EE / 2 floor, p, a, b, c, d; static ids are -(i + 2)) and w7 (7 per
+ * record: w0..w3, nx, ny, nz) are given and cap >= *count they are filled,
+ * else CS_E_CAPACITY. */
+int cs_contact_active(cs_solver* s, int32_t cap, int32_t* count, int32_t* ids6, double* w7);
+
+/* Graph-captured steps (no counterpart in the reference): with enable = 1 (the
+ * default) a step of the mixed path whose PCG fits one thread-block cluster is
+ * a replay of a CUDA graph captured once per configuration, with the Newton,
+ * Armijo and trust-region decisions taken on the device (conditional graph
+ * nodes) and one host synchronization per step; its results equal the
+ * host-driven step's. A step whose buffers overflow is restored and repeated
+ * host-driven with grown buffers. enable = 0 forces the host-driven step.
+ * cs_graph_info: out2[0] steps taken as graph replays, out2[1] repeats. */
+int cs_set_graph_mode(cs_solver* s, int32_t enable);
+int cs_graph_info(cs_solver* s, int64_t* out2);
+
 /* ---- material model (src/physics/material-model.ts:232-296) ----
  * ClothMaterialModel.energy / gradient / hessianVector of the orthotropic StVK
  * model on the GPU, for the handle's mesh and current material (cs_set_material),

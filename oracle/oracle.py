@@ -407,7 +407,7 @@ STAT_KEYS = ["newtonIters", "pcgIters", "gradNorm", "energy", "maxStrain", "conv
              "barrierEnergy", "frictionWork", "rejectedLineSearchSteps", "ccdFailures",
              "newtonItersUsed", "armijoTrials"]
 
-PRECOND = {"jacobi": 0, "schwarz": 1, "block": 2}
+PRECOND = {"jacobi": 0, "schwarz": 1, "block": 2, "mas2": 3, "masX": 4}
 
 
 class Scene:

@@ -159,6 +159,24 @@ void build_schwarz_factors(const double* x, const Mesh& mesh, const Material& ma
                            const double* diag, const SchwarzDomains& dom, SchwarzFactors& f);
 void apply_schwarz(const SchwarzFactors& f, const double* r, double* out, int n);
 
+// Two-level additive Schwarz (mas.ts): coarse space = one constant per domain
+// and component.
+void restrict_coarse(const double* r, const SchwarzDomains& dom, double* rc);
+void prolongate_add(const double* c, const SchwarzDomains& dom, double* z);
+Vec build_coarse_diag(const double* x, const Mesh& mesh, const Material& mat, const double* diag,
+                      const SchwarzDomains& dom);
+void apply_mas2(const SchwarzFactors& sf, const Vec& dc, double omega, const double* r, double* out, int n);
+struct CoarseExact {
+  const SchwarzDomains* dom = nullptr;
+  int n = 0;     // 3 D
+  Vec chol;      // n x n: Cholesky L (lower) when flag, else the inverse diagonal
+  int flag = 0;
+};
+void build_coarse_exact(const double* x, const Mesh& mesh, const Material& mat, const double* diag,
+                        const SchwarzDomains& dom, CoarseExact& ce);
+void solve_coarse_exact(const CoarseExact& ce, const double* rhs, double* out);
+void apply_masx(const SchwarzFactors& sf, const CoarseExact& ce, const double* r, double* out, int n);
+
 struct BlockFactors { Vec inv; std::vector<uint8_t> flag; };
 void build_block_factors(const double* x, const Mesh& mesh, const Material& mat,
                          const double* diag, BlockFactors& f);

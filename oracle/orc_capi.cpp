@@ -230,6 +230,20 @@ int orc_pcg_solve(void* mh, const double* mat, const double* x, void* contact, d
     build_block_factors(X.data(), me, mt, dg.data(), bf);
     prec = [&](const Vec& r, Vec& z) { apply_block_factors(bf, r.data(), z.data(), n); };
   }
+  // two-level additive Schwarz: 3 = mas2 (damped-Jacobi coarse, omega 0.5), 4 = masX (exact coarse)
+  Vec coarseDiag;
+  CoarseExact ce;
+  if (precond == 3 || precond == 4) {
+    const SchwarzDomains& dom = *(SchwarzDomains*)domains;
+    build_schwarz_factors(X.data(), me, mt, dg.data(), dom, sf);
+    if (precond == 3) {
+      coarseDiag = build_coarse_diag(X.data(), me, mt, dg.data(), dom);
+      prec = [&](const Vec& r, Vec& z) { apply_mas2(sf, coarseDiag, 0.5, r.data(), z.data(), n); };
+    } else {
+      build_coarse_exact(X.data(), me, mt, dg.data(), dom, ce);
+      prec = [&](const Vec& r, Vec& z) { apply_masx(sf, ce, r.data(), z.data(), n); };
+    }
+  }
   Vec xo;
   auto nofilter = [](double*) {};
   PcgResult r = pcg(bb, hvp, dg, maxIters, tol, nofilter, false, prec ? &prec : nullptr, xo);

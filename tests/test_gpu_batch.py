@@ -95,7 +95,7 @@ def test_autotune_keeps_state():
     bs.step(0.01, 2)
     x0 = bs.allPositions()
     t = bs.autotune(0.01)
-    assert t in (256, 512, 1024)
+    assert t in (128, 256, 512)
     assert np.array_equal(bs.allPositions(), x0)
     bs.step(0.01)
     assert np.all(np.isfinite(bs.allPositions()))

@@ -149,13 +149,21 @@ def test_g5_pcg_iteration_counts_pin():
     (G5_PRECONDITIONER_REPORT.md:65-76): Jacobi, block-Jacobi and Schwarz-1 on
     the 6x6 tensile patch, free flight and floor contact, 5 stiffness scalings.
 
-    28 of 30 counts reproduce exactly. Two cells (schwarz1 1x/none, block
+    Jacobi, block-Jacobi and one-level Schwarz: 28 of 30 counts reproduce
+    exactly; two-level Schwarz (mas2, masX): all 10 floor cells exactly, the 10
+    free-flight cells within +-1. Two cells (schwarz1 1x/none, block
     5x/none) sit on a convergence boundary: a 1-ulp perturbation of the
     test's Math.sin-generated inputs flips them between the two values, so
     they are held to +-1 (V8's and glibc's sin may differ by an ulp).
     """
     gold = json.load(open(os.path.join(GOLD, "g5_pcg_iters.json")))
     boundary = {("1x/none", "schwarz1"), ("5x/none", "block"), ("10xbend/none", "schwarz1")}
+    # Two-level Schwarz (mas2, masX; src/solver/mas.ts): the free-flight cells
+    # take their vertical jitter from Math.sin, and a 1-ulp change of one sin
+    # value flips each of these counts between the published value and its
+    # neighbour (checked by perturbing the jitter), so they are held to +-1;
+    # the floor cells, whose state has no sin jitter, reproduce exactly.
+    boundary |= {(c, m) for c in gold["cells"] if c.endswith("/none") for m in ("mas2", "masX")}
     scale = {"1x": (1, 1), "2x": (2, 1), "5x": (5, 1), "10x": (10, 1), "10xbend": (1, 10)}
     base = O.DEFAULT_MATERIAL
     for cell, methods in gold["cells"].items():
@@ -185,8 +193,9 @@ def test_g5_pcg_iteration_counts_pin():
             cs.add_diag_estimate(diag, x)
         dom = O.SchwarzDomains(mesh, mesh.positions, 16, 8, 32)
         b = np.array([math.sin(i * 0.913) * 0.5 for i in range(3 * n)])
-        for name, pc in [("jacobi", 0), ("block", 2), ("schwarz1", 1)]:
-            it, res, _ = O.pcg_solve(mesh, mat, x, cs, 3600, diag, b, 200, 1e-6, pc, dom if pc == 1 else None)
+        for name, pc in [("jacobi", 0), ("block", 2), ("schwarz1", 1), ("mas2", 3), ("masX", 4)]:
+            it, res, _ = O.pcg_solve(mesh, mat, x, cs, 3600, diag, b, 200, 1e-6, pc,
+                                     dom if pc in (1, 3, 4) else None)
             want = methods[name]["iters"]
             if (cell, name) in boundary:
                 assert abs(it - want) <= 1, (cell, name, it, want)
