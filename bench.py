@@ -268,6 +268,8 @@ def run_path(cfg, precision, local, args, flush, budget, mode="device", sampler=
     solver.initialize(sc)
     if budget == "converged":
         solver.setNewtonMode("exact", EXACT_TOL)
+    if args.no_graph:
+        solver.setGraphMode(False)
     ext = torch.cuda.ExternalStream(solver.stream(), device=local)
     n = len(cfg["x"]) // 3
     if mode == "e2e":
@@ -298,6 +300,8 @@ def run_path(cfg, precision, local, args, flush, budget, mode="device", sampler=
     graph0 = solver.graphInfo()
     if profile:
         solver.profile(True)
+    if args.profiler_range and mode == "device" and not profile:
+        torch.cuda.profiler.start()  # ncu --profile-from-start off captures the timed steps only
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     total = 0.0
@@ -322,6 +326,8 @@ def run_path(cfg, precision, local, args, flush, budget, mode="device", sampler=
                 solver.pull()
             pos.append(sc.positions.copy())
     torch.cuda.synchronize()
+    if args.profiler_range and mode == "device" and not profile:
+        torch.cuda.profiler.stop()
     out = dict(ms=total, launches=solver.kernelLaunches() - launches0, solver=solver, scene=sc, pos=pos, mind=mind,
                stats=stats, step_bytes=step_bytes, graph=solver.graphInfo(), graph0=graph0)
     if profile:
@@ -474,6 +480,13 @@ def main():
     ap.add_argument("--no-reference-budget", action="store_true", help="skip the reference-budget figure")
     ap.add_argument("--small", action="store_true", help="32x32 floor drape (for profiler captures)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--paths", default="fp64,mixed,e2e,profile,refbudget",
+                    help="profiler captures: run only these device-resident paths (fp64 and/or mixed), no JSON line")
+    ap.add_argument("--no-graph", action="store_true",
+                    help="host-driven steps instead of the captured step graph (same kernels; profilers cannot "
+                         "capture kernel nodes of graphs with conditional nodes)")
+    ap.add_argument("--profiler-range", action="store_true",
+                    help="mark the timed steps for ncu --profile-from-start off")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -503,6 +516,31 @@ def main():
     dev = f"cuda:{local}"
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MiB > 126 MB L2
 
+    paths = set(args.paths.split(","))
+    if paths != {"fp64", "mixed", "e2e", "profile", "refbudget"}:
+        # some of the paths only (profiler captures, secondary workloads): one
+        # summary line per run, not the headline line
+        res = {}
+        for pth in ("fp64", "mixed"):
+            if pth in paths:
+                r = run_path(cfg, pth, local, args, flush, args.budget, record="fp64" in paths and "mixed" in paths)
+                res[pth] = r
+        if rank == 0 and not args.profiler_range:
+            line = {"metric": "sim steps/s", "unit": "steps/s", "impl": "cuda", "n_gpus": world,
+                    "config": {"workload": cfg["name"], "n": n, "budget": args.budget,
+                               "timed_steps": [args.warmup + args.skip, args.warmup + args.skip + args.steps - 1]}}
+            for pth, r in res.items():
+                line[pth] = {"value": args.steps / (r["ms"] / 1000.0), "ms_per_step": r["ms"] / args.steps,
+                             "converged_steps": sum(1 for st in r["stats"] if st.converged),
+                             "gpu_launches": r["launches"],
+                             "graph_steps": r["graph"]["graphSteps"] - r["graph0"]["graphSteps"],
+                             "min_distance": min(r["mind"]) if r["mind"] else None}
+            if len(res) == 2:
+                line["mixed_vs_fp64_rel_pos_err_max"] = max(
+                    float(np.max(np.abs(b - a)) / np.max(np.abs(a))) for a, b in zip(res["fp64"]["pos"],
+                                                                                    res["mixed"]["pos"]))
+            print(json.dumps(line), flush=True)
+        return 0
     # the FP64 path and the mixed path over the same steps and budget
     fp64 = run_path(cfg, "fp64", local, args, flush, args.budget, record=True)
     sampler = ClockSampler(local)

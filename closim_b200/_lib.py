@@ -11,7 +11,7 @@ LIB_PATH = os.path.join(_HERE, "libclosim_cuda.so")
 
 CS_OK, CS_E_UNINIT, CS_E_NONFINITE, CS_E_CAPACITY, CS_E_CUDA, CS_E_ARG = range(6)
 CS_PRECISION_FP64, CS_PRECISION_MIXED = 0, 1
-CS_PRECOND_JACOBI, CS_PRECOND_SCHWARZ = 0, 1
+CS_PRECOND_JACOBI, CS_PRECOND_SCHWARZ, CS_PRECOND_MAS2 = 0, 1, 2
 CS_BROADPHASE_MIRROR, CS_BROADPHASE_EXACT = 0, 1
 
 

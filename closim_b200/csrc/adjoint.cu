@@ -90,7 +90,7 @@ __device__ double adj_schwarz(const Dev& d, const double* r, double* z, int dom)
 
 __device__ __forceinline__ double adj_precond(const Dev& d, const AdjArgs& A, int tid, int nth) {
   double rz = 0;
-  if (d.precond == 1) {
+  if (d.precond >= 1) {  // one-level Schwarz factors (the two-level coarse term is not applied here)
     for (int dom = tid; dom < d.D; dom += nth) rz += adj_schwarz(d, A.r, A.z, dom);
   } else {
     for (int i = tid; i < d.n * 3; i += nth) {

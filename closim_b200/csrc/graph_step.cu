@@ -224,13 +224,14 @@ void Solver::graph_capture(double h) {
   d.h = h;
   d.invH2 = 1 / (h * h);
   for (int k = 0; k < 3; k++) d.gravity[k] = gravity[k];
-  d.precond = opts.precond == CS_PRECOND_SCHWARZ ? 1 : 0;
+  d.precond = precond_code();
   d.hasContact = contact ? 1 : 0;
   d.x = vx.p;
   d.xt = vxt.p;
   const bool exactMode = newtonMode == 1;
   mb.psd = exactMode ? 1 : 0;
   mb.hrec = exactMode && d.kb > 0 && d.hg > 0 ? ensure_hrec() : nullptr;
+  mb.dcoarse = d.precond == 2 ? fdc.p : nullptr;
   const bool fricExact = exactMode && contact && contact->p.mu > 0;
   const double beta = std::max(std::max(mat.stretch_warp, mat.stretch_weft), mat.shear) * mat.thickness * 0.1 + 1e-6;
   const double damp = 1 - std::min(std::max(mat.damping, 0.0), 0.1);
@@ -295,7 +296,7 @@ void Solver::graph_capture(double h) {
     const int64_t s0 = lc;
     g.push(hSolve, cudaGraphCondTypeIf);
     {
-      mx_prepare(d, mb, d.precond == 1, g.cur(), &lc);
+      mx_prepare(d, mb, d.precond >= 1, g.cur(), &lc);
       GCK((cudaError_t)mx_launch_pcg_cluster(d, mb, fp.p, fp2.p, contact ? contact->dd : nullptr, opts.pcg_max_iters,
                                              pcgTol, mxCluster, g.cur()));
       lc++;

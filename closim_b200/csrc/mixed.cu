@@ -131,6 +131,14 @@ __global__ void __launch_bounds__(kMxWarps * 32) k_mx_schwarz_factor(Dev d, MixB
     row[lane] += d.diag[v * 3 + aa];
   }
   __syncwarp();
+  // two-level: the coarse diagonal diag(R A P) of this domain, the sum of its
+  // component-c entries over member pairs divided by |d| (mas.ts:57-101)
+  if (mb.dcoarse && lane < 3) {
+    double c = 0;
+    for (int i = 0; i < dv; i++)
+      for (int j = 0; j < dv; j++) c += a[(i * 3 + lane) * kFS + j * 3 + lane];
+    reinterpret_cast<float*>(mb.dcoarse + dom)[lane] = (float)(c / dv);
+  }
   for (int i = lane; i < dw; i += 32)
     for (int j = i + 1; j < dw; j++) {
       const double sv = 0.5 * (a[i * kFS + j] + a[j * kFS + i]);
@@ -242,6 +250,7 @@ __device__ __forceinline__ double mx_schwarz(const Dev& d, const MixBufs& mb, in
       const float rj = __shfl_sync(0xffffffffu, rv, j);
       if (lane < dw) z = fmaf(Li[j], rj, z);
     }
+    if (mb.dcoarse) z += coarse_share(mb, dom, rv, dv);
     if (lane < dw) {
       if (d.pinned[gi / 3]) z = 0.f;
       mb.z[gi] = z;

@@ -23,7 +23,23 @@ struct MixBufs {
   // bending term g (g . p) to the HVP. Both off in the reference mode.
   int psd;
   float4* hrec;
+  // Two-level Schwarz (mas2): per domain the coarse diagonal (x, y, z) of
+  // R A P; null for the one-level preconditioner.
+  float4* dcoarse;
 };
+
+// Two-level Schwarz share of lane (member l, component c) of a domain warp:
+// omega Dc^-1 R r prolongated, = sc (omega / Dc[c]) sc sum_l' r[l', c] with
+// sc = 1 / sqrt(|d|) and omega = 0.5 (applyMasTwoLevel, mas.ts:120-139).
+__device__ __forceinline__ float coarse_share(const MixBufs& mb, int dom, float rv, int dv) {
+  const int lane = threadIdx.x & 31, c = lane % 3;
+  float rc = 0.f;
+#pragma unroll
+  for (int l = 0; l < 8; l++) rc += __shfl_sync(0xffffffffu, rv, l * 3 + c);
+  const float dc = reinterpret_cast<const float*>(mb.dcoarse + dom)[c];
+  const float sc2 = 1.f / (float)dv;  // sc * sc
+  return dc > 1e-12f ? 0.5f * rc * sc2 / dc : 0.f;
+}
 
 void mx_prepare(const Dev& d, const MixBufs& mb, bool schwarz, cudaStream_t s, int64_t* lc);
 int mx_pcg_grid_blocks(const Dev& d);

@@ -194,6 +194,10 @@ __device__ __forceinline__ void cl_domains(const Dev& d, const MixBufs& mb, cons
       z = fmaf(L[u][j4].z, __shfl_sync(0xffffffffu, rv[u], 4 * j4 + 2), z);
       z = fmaf(L[u][j4].w, __shfl_sync(0xffffffffu, rv[u], 4 * j4 + 3), z);
     }
+    if (mb.dcoarse) {
+      const int dom = dom0 + u * step;
+      if (dom < d.D) z += coarse_share(mb, dom, rv[u], d.domStart[dom + 1] - d.domStart[dom]);
+    }
     if (act[u]) {
       if (pin[u]) z = 0.f;
       mb.z[gi[u]] = z;

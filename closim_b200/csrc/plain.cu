@@ -324,6 +324,65 @@ __global__ void __launch_bounds__(kSchwarzWarps * 32) k_schwarz_factor(Dev d) {
   if (lane == 0) d.domFlag[dom] = ok ? 1 : 0;
 }
 
+// Two-level Schwarz (src/solver/mas.ts buildCoarseDiag, mas.ts:57-101): the
+// coarse diagonal of each domain, one thread per domain, in the reference's
+// accumulation order: the domain's triangles in ascending order, their
+// within-domain (ci, cj) pairs, then the Jacobi diagonal over the members.
+constexpr int kCoarseTris = 96;  // triangles touching a domain of <= 8 vertices
+__global__ void __launch_bounds__(kThreads) k_coarse_diag(Dev d) {
+  const int dom = blockIdx.x * blockDim.x + threadIdx.x;
+  if (dom >= d.D) return;
+  const int start = d.domStart[dom], dv = d.domStart[dom + 1] - start;
+  int tris[kCoarseTris];
+  int nt = 0;
+  for (int l = 0; l < dv; l++) {
+    const int v = d.domVerts[start + l];
+    for (int k = d.v2tOff[v]; k < d.v2tOff[v + 1]; k++) {
+      const int t = d.v2t[k];
+      int pos = nt;  // insertion into the sorted list, duplicates skipped
+      bool dup = false;
+      for (int q = 0; q < nt; q++) {
+        if (tris[q] == t) { dup = true; break; }
+        if (tris[q] > t) { pos = q; break; }
+      }
+      if (dup || nt >= kCoarseTris) continue;
+      for (int q = nt; q > pos; q--) tris[q] = tris[q - 1];
+      tris[pos] = t;
+      nt++;
+    }
+  }
+  auto inDom = [&](int v) {
+    for (int l = 0; l < dv; l++)
+      if (d.domVerts[start + l] == v) return true;
+    return false;
+  };
+  double dc[3] = {0, 0, 0};
+  for (int q = 0; q < nt; q++) {
+    const int t = tris[q];
+    const int cvs[3] = {(int)d.idx[t * 3], (int)d.idx[t * 3 + 1], (int)d.idx[t * 3 + 2]};
+    const bool in[3] = {inDom(cvs[0]), inDom(cvs[1]), inDom(cvs[2])};
+    double p0[3], p1[3], p2[3];
+    load3(d.x, cvs[0], p0); load3(d.x, cvs[1], p1); load3(d.x, cvs[2], p2);
+    const float4 iv = d.inv[t];
+    for (int ci = 0; ci < 3; ci++) {
+      if (!in[ci]) continue;
+      double h27[27];  // rows ci*3 .. ci*3+2 of the 9x9 block
+      tri_hessian9_rows<double>(p0, p1, p2, iv.x, iv.y, iv.z, iv.w, d.area[t], d.mat, ci * 3, ci * 3 + 3, h27);
+      for (int cj = 0; cj < 3; cj++) {
+        if (!in[cj]) continue;
+        const double s = 1.0 / (double)dv;
+        for (int a = 0; a < 3; a++) dc[a] += s * h27[a * 9 + cj * 3 + a];
+      }
+    }
+  }
+  for (int l = 0; l < dv; l++) {
+    const int v = d.domVerts[start + l];
+    const double s = 1.0 / (double)dv;
+    for (int a = 0; a < 3; a++) dc[a] += s * d.diag[v * 3 + a];
+  }
+  for (int a = 0; a < 3; a++) d.dcoarse[dom * 3 + a] = dc[a];
+}
+
 // z = M^-1 r on one domain; returns sum r.z over its (pin-filtered) dofs.
 __device__ double schwarz_apply_domain(const Dev& d, int dom) {
   const int start = d.domStart[dom], dv = d.domStart[dom + 1] - start, dw = dv * 3;
@@ -351,11 +410,27 @@ __device__ double schwarz_apply_domain(const Dev& d, int dom) {
       sol[i] = s;
     }
   }
+  // two-level: + P (omega Dc^-1) R r on this domain (applyMasTwoLevel,
+  // mas.ts:120-139, omega = 0.5; the coarse vector of a domain is constant per
+  // component over its members, scaled by 1/sqrt(|d|) both ways)
+  double cz[3] = {0, 0, 0};
+  const double sc = 1 / sqrt((double)dv);
+  if (d.precond == 2) {
+    double rc[3] = {0, 0, 0};
+    for (int l = 0; l < dv; l++)
+      for (int k = 0; k < 3; k++) rc[k] += rhs[l * 3 + k] * sc;
+    for (int k = 0; k < 3; k++) {
+      const double dd = d.dcoarse[dom * 3 + k];
+      cz[k] = dd > 1e-12 ? (0.5 * rc[k]) / dd : 0.0;
+    }
+  }
   for (int l = 0; l < dv; l++) {
     const int v = d.domVerts[start + l];
     const bool pin = d.pinned[v];
     for (int k = 0; k < 3; k++) {
-      const double zz = pin ? 0.0 : 0.0 + sol[l * 3 + k];
+      double zz = 0.0 + sol[l * 3 + k];
+      if (d.precond == 2) zz += cz[k] * sc;
+      if (pin) zz = 0.0;
       d.z[v * 3 + k] = zz;
       d.T2[v * 3 + k] = d.r[v * 3 + k] * zz;
     }
@@ -869,6 +944,7 @@ void launch_diag_init(const Dev& d, double beta, cudaStream_t s) {
 }
 void launch_schwarz_factor(const Dev& d, cudaStream_t s) {
   k_schwarz_factor<<<(d.D + kSchwarzWarps - 1) / kSchwarzWarps, kSchwarzWarps * 32, 0, s>>>(d);
+  if (d.precond == 2) k_coarse_diag<<<nblk(d.D), kThreads, 0, s>>>(d);
 }
 int pcg_grid_blocks(const Dev& d) {
   int dev = 0, sms = 0, per = 0;

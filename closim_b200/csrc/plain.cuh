@@ -97,7 +97,8 @@ struct Dev {
   const int* v2t;          // 3m
   double* L;               // D x 576 (24x24 row-major), Cholesky or inverse diagonal
   uint8_t* domFlag;        // D
-  int precond;             // 0 Jacobi, 1 Schwarz
+  double* dcoarse;         // 3D: coarse diagonal of the two-level Schwarz (precond 2)
+  int precond;             // 0 Jacobi, 1 one-level Schwarz, 2 two-level Schwarz (mas2)
   int hasContact;
   Contact c;               // valid when hasContact
 };

@@ -71,7 +71,8 @@ int cs_set_contact(cs_solver* h, const cs_contact_params* p, int floor_on, doubl
 int cs_set_stepper_options(cs_solver* h, const cs_stepper_options* o) {
   return guarded(h, [&] {
     if (!o || o->newton_iters < 0 || o->pcg_max_iters < 0 || o->ls_iters < 0) throw std::invalid_argument("bad options");
-    if (o->precond != CS_PRECOND_JACOBI && o->precond != CS_PRECOND_SCHWARZ) throw std::invalid_argument("bad precond");
+    if (o->precond != CS_PRECOND_JACOBI && o->precond != CS_PRECOND_SCHWARZ && o->precond != CS_PRECOND_MAS2)
+      throw std::invalid_argument("bad precond");
     h->s.opts = *o;
   });
 }

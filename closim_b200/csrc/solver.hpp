@@ -100,11 +100,12 @@ class Solver {
   DBuf<double> vx, vv, vx0, vyHat, vg, vdiag, vdx, vr, vz, vp, vAp, vxt, vcgrad, vcHp, elem, helem, part, scal, L;
   DBuf<double> T0, T1, T2, T3, Tc;
   DBuf<uint8_t> domFlag;
+  DBuf<double> dcoarse;
   double* hscal = nullptr;  // pinned host mirror of scal
   int pcgBlocks = 1;
   // mixed-precision path
   DBuf<float> fr, fz, fp, fAp, fx, felem, ftris, fh9, fLinv, fp2;
-  DBuf<float4> fvrec;
+  DBuf<float4> fvrec, fdc;
   DBuf<uint32_t> triSlot;
   MixBufs mb{};
   int mxBlocks = 1;
@@ -149,11 +150,11 @@ class Solver {
       // CSR offset; Schwarz reads one 24x24 FP32 inverse per domain.
       const double tri = 64 + 12 + 72 + 12;
       const double vert = 12 + 4 + 12 + 9 * 12 + 4;
-      const double dom = d.precond == 1 ? 2304.0 + 2 * 96 : 0.0;
+      const double dom = d.precond >= 1 ? 2304.0 + 2 * 96 : 0.0;
       return 5 * 12 * n + iters * (tri * m + vert * n + dom * mesh.D) + 4 * 24 * n;
     }
     double hvp = 2 * 24 * n + 32 * m + 2 * 144 * m + 4 * n + 24 * n;
-    double vec = 9 * 24 * n + (d.precond == 1 ? 4608.0 * mesh.D : 0.0);
+    double vec = 9 * 24 * n + (d.precond >= 1 ? 4608.0 * mesh.D : 0.0);
     double init = 6 * 24 * n;
     double post = 4 * 24 * n;
     return init + iters * (hvp + vec) + post;
@@ -186,6 +187,11 @@ class Solver {
     CK(cudaMallocHost(&hscal, S_NSCALARS * sizeof(double)));
     CK(cudaEventCreate(&pev0));
     CK(cudaEventCreate(&pev1));
+  }
+
+  // d.precond: 0 Jacobi, 1 one-level Schwarz, 2 two-level Schwarz (mas2).
+  int precond_code() const {
+    return opts.precond == CS_PRECOND_SCHWARZ ? 1 : opts.precond == CS_PRECOND_MAS2 ? 2 : 0;
   }
 
   void set_material(const cs_material& m) {
@@ -246,6 +252,7 @@ class Solver {
     domVerts.upload(mesh.domVerts.data(), mesh.domVerts.size(), stream);
     domFlag.alloc(std::max(mesh.D, 1));
     L.alloc((size_t)std::max(mesh.D, 1) * 576);
+    dcoarse.alloc((size_t)std::max(mesh.D, 1) * 3);
     for (DBuf<double>* b : {&vx, &vv, &vx0, &vyHat, &vg, &vdiag, &vdx, &vr, &vz, &vp, &vAp, &vxt, &vcgrad, &vcHp})
       b->alloc(n3);
     CK(cudaMemsetAsync(vcgrad.p, 0, n3 * 8, stream));
@@ -273,7 +280,7 @@ class Solver {
     d.r = vr.p; d.z = vz.p; d.p = vp.p; d.Ap = vAp.p; d.xt = vxt.p; d.cgrad = vcgrad.p; d.cHp = vcHp.p;
     d.elem = elem.p; d.helem = helem.p; d.part = part.p; d.partStride = partStride; d.scal = scal.p;
     d.D = mesh.D; d.domStart = domStart.p; d.domVerts = domVerts.p; d.v2tOff = v2tOff.p; d.v2t = v2t.p;
-    d.L = L.p; d.domFlag = domFlag.p;
+    d.L = L.p; d.domFlag = domFlag.p; d.dcoarse = dcoarse.p;
     d.T0 = T0.p; d.T1 = T1.p; d.T2 = T2.p; d.T3 = T3.p; d.Tc = Tc.p;
     set_material(m);
     for (int k = 0; k < 3; k++) d.gravity[k] = gravity[k];
@@ -284,6 +291,7 @@ class Solver {
       ftris.alloc((size_t)cm.m * 16);
       fh9.alloc((size_t)cm.m * 81);
       fLinv.alloc((size_t)std::max(mesh.D, 1) * 576);
+      fdc.alloc((size_t)std::max(mesh.D, 1));
       mb.r = fr.p; mb.z = fz.p; mb.p = fp.p; mb.Ap = fAp.p; mb.x = fx.p;
       mb.elem = felem.p; mb.tris = ftris.p; mb.h9 = fh9.p; mb.Linv = fLinv.p;
       mxBlocks = mx_pcg_grid_blocks(d);
@@ -365,7 +373,7 @@ class Solver {
     d.h = h;
     d.invH2 = 1 / (h * h);
     for (int k = 0; k < 3; k++) d.gravity[k] = gravity[k];
-    d.precond = opts.precond == CS_PRECOND_SCHWARZ ? 1 : 0;
+    d.precond = precond_code();
     d.hasContact = contact ? 1 : 0;
     int64_t& lc = launch_counter();
     if (profPhases) { CK(cudaStreamSynchronize(stream)); phaseT0 = std::chrono::steady_clock::now(); curPhase = PH_OTHER; }
@@ -435,11 +443,12 @@ class Solver {
       const bool exactMixed = newtonMode == 1 && mixed() && mxCluster > 0;
       mb.psd = exactMixed ? 1 : 0;
       mb.hrec = exactMixed && d.kb > 0 && d.hg > 0 ? ensure_hrec() : nullptr;
+      mb.dcoarse = d.precond == 2 ? fdc.p : nullptr;
       if (newtonMode == 1 && !exactMixed) {
-        if (d.precond == 1) { launch_schwarz_factor(d, stream); lc += 1; }
+        if (d.precond >= 1) { launch_schwarz_factor(d, stream); lc += d.precond; }
       } else if (mixed()) {
-        mx_prepare(d, mb, d.precond == 1, stream, &lc);
-      } else if (d.precond == 1) {
+        mx_prepare(d, mb, d.precond >= 1, stream, &lc);
+      } else if (d.precond >= 1) {
         launch_schwarz_factor(d, stream);
         lc += 1;
       }
@@ -715,7 +724,7 @@ class Solver {
           contact->update_active_set(*this, x1);
         }
         launch_diag_init(d, beta, stream);
-        if (d.precond == 1) launch_schwarz_factor(d, stream);
+        if (d.precond >= 1) launch_schwarz_factor(d, stream);
         adj_rhs(d, adjLamX.p, adjLamV.p, damp, adjRhs.p, stream);
         AdjArgs a{d, adjRhs.p, adjMu.p, adjR.p, adjZ.p, adjP.p, adjAp.p, adjTri.p, adjHin.p, d.kb, 0, maxIters, tol,
                   adjOut.p};

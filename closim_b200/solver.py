@@ -192,7 +192,8 @@ class CudaSolver:
 
     precision: "fp64" (plain path, op-for-op with the reference arithmetic) or
     "mixed". options: StepperOptions (newtonIters, pcgMaxIters, gradTol,
-    lineSearchIters) plus precond ("jacobi" | "schwarz").
+    lineSearchIters) plus precond ("jacobi" | "schwarz" | "mas2": two-level
+    Schwarz, src/solver/mas.ts).
     """
 
     def __init__(self, precision: str = "fp64", device: int = 0, **options):
@@ -227,7 +228,7 @@ class CudaSolver:
     def setOptions(self, **o):
         self._options.update(o)
         oo = self._options
-        pc = {"jacobi": L.CS_PRECOND_JACOBI, "schwarz": L.CS_PRECOND_SCHWARZ}[oo["precond"]]
+        pc = {"jacobi": L.CS_PRECOND_JACOBI, "schwarz": L.CS_PRECOND_SCHWARZ, "mas2": L.CS_PRECOND_MAS2}[oo["precond"]]
         opts = L.cs_stepper_options(int(oo["newtonIters"]), int(oo["pcgMaxIters"]), int(oo["lineSearchIters"]),
                                     pc, float(oo["gradTol"]))
         self._check(self._lib.cs_set_stepper_options(self._h, C.byref(opts)))

@@ -324,8 +324,9 @@ napi_value SetStepperOptions(napi_env env, napi_callback_info info) {
     return nullptr;
   if (std::strcmp(pc, "jacobi") == 0) o.precond = CS_PRECOND_JACOBI;
   else if (std::strcmp(pc, "schwarz") == 0) o.precond = CS_PRECOND_SCHWARZ;
+  else if (std::strcmp(pc, "mas2") == 0) o.precond = CS_PRECOND_MAS2;
   else {
-    napi_throw_range_error(env, nullptr, "preconditioner must be \"jacobi\" or \"schwarz\"");
+    napi_throw_range_error(env, nullptr, "preconditioner must be \"jacobi\", \"schwarz\" or \"mas2\"");
     return nullptr;
   }
   cs_ok(env, h, cs_set_stepper_options(h, &o));

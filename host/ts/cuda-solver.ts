@@ -68,7 +68,7 @@ interface CudaAddon {
 /** Opaque solver handle owned by the addon. */
 export type CudaHandle = { readonly __brand: "closim_cuda_handle" };
 export type Precision = "fp64" | "mixed";
-export type Preconditioner = "jacobi" | "schwarz";
+export type Preconditioner = "jacobi" | "schwarz" | "mas2";
 
 export interface CudaSolverOptions extends StepperOptions {
   /** "fp64": the reference's arithmetic, op for op; "mixed": FP32 linear solve. */

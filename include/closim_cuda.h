@@ -32,7 +32,10 @@ enum {
 };
 
 enum { CS_PRECISION_FP64 = 0, CS_PRECISION_MIXED = 1 };
-enum { CS_PRECOND_JACOBI = 0, CS_PRECOND_SCHWARZ = 1 };
+/* Preconditioners: Jacobi; one-level additive Schwarz on <= 8-vertex domains
+ * (src/solver/schwarz.ts); two-level additive Schwarz with the damped-Jacobi
+ * coarse correction over the same domains (src/solver/mas.ts, omega = 0.5). */
+enum { CS_PRECOND_JACOBI = 0, CS_PRECOND_SCHWARZ = 1, CS_PRECOND_MAS2 = 2 };
 
 /* ClothMaterial (src/physics/types.ts:1-12). */
 typedef struct cs_material {

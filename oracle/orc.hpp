@@ -300,7 +300,7 @@ struct Scene {
 void enforce_pins(const Scene& s, double* x);
 void pin_filter(const Scene& s, double* v);
 
-enum Precond { PRECOND_JACOBI = 0, PRECOND_SCHWARZ = 1, PRECOND_BLOCK = 2 };
+enum Precond { PRECOND_JACOBI = 0, PRECOND_SCHWARZ = 1, PRECOND_BLOCK = 2, PRECOND_MAS2 = 3 };
 struct StepperOptions {
   int newtonIters = 10, pcgMaxIters = 60;
   double gradTol = 1e-5;

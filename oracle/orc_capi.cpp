@@ -300,7 +300,7 @@ int orc_step(void* h, double dt, int newtonIters, int pcgMaxIters, double gradTo
   StepperOptions o;
   o.newtonIters = newtonIters; o.pcgMaxIters = pcgMaxIters; o.gradTol = gradTol; o.lsIters = lsIters;
   o.precond = precond;
-  if (precond == PRECOND_SCHWARZ && !b->hasDom) {
+  if ((precond == PRECOND_SCHWARZ || precond == PRECOND_MAS2) && !b->hasDom) {
     b->dom = build_schwarz_domains(b->s.mesh, b->s.mesh.rest.data(), 8, 1, 8);
     b->hasDom = true;
   }

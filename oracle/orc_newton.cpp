@@ -186,9 +186,15 @@ StepStats implicit_step(Scene& scene, double h, const StepperOptions& opts,
       }
     };
     std::function<void(const Vec&, Vec&)> prec;
+    Vec coarseDiag;
     if (opts.precond == PRECOND_SCHWARZ) {
       build_schwarz_factors(x.data(), mesh, mat, diag.data(), *domains, sf);
       prec = [&](const Vec& r, Vec& z) { apply_schwarz(sf, r.data(), z.data(), n); };
+    } else if (opts.precond == PRECOND_MAS2) {
+      // two-level Schwarz (src/solver/mas.ts buildMasTwoLevel / applyMasTwoLevel, omega 0.5)
+      build_schwarz_factors(x.data(), mesh, mat, diag.data(), *domains, sf);
+      coarseDiag = build_coarse_diag(x.data(), mesh, mat, diag.data(), *domains);
+      prec = [&](const Vec& r, Vec& z) { apply_mas2(sf, coarseDiag, 0.5, r.data(), z.data(), n); };
     } else if (opts.precond == PRECOND_BLOCK) {
       build_block_factors(x.data(), mesh, mat, diag.data(), bf);
       prec = [&](const Vec& r, Vec& z) { apply_block_factors(bf, r.data(), z.data(), n); };

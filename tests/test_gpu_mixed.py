@@ -24,10 +24,12 @@ pytestmark = pytest.mark.gpu
 POS_TOL = 1e-5
 
 
-def trajectory(cfg, precision, steps):
+def trajectory(cfg, precision, steps, exact=None):
     sc = configs.make_scene(cfg)
     s = cb.CudaSolver(precision, **cfg["options"])
     s.initialize(sc)
+    if exact:
+        s.setNewtonMode("exact", exact)
     out, conv = [], 0
     for k in range(steps):
         sc.pinned.clear()
@@ -91,13 +93,22 @@ def test_strip_pull_mixed_within_fp64_budget_sensitivity():
 
 
 def test_floor_drape_mixed_no_intersection():
+    """32 x 32 drape started 2 cm above the floor, through landing and 60 steps
+    of contact, in exact-Newton mode at a converging budget (40 Newton, 3000
+    PCG, gradTol 1e-8, Newton tolerance 1e-6): every step of both paths
+    converges, the mixed trajectory stays within POS_TOL of FP64, and no
+    vertex comes closer to the floor than dMin."""
     cfg = configs.floor_drape(nx=31, ny=31, w=0.4, hgt=0.4, steps=60)
     cfg["x"][1::3] -= 0.28  # start 2 cm above the floor so contact engages early
-    a, _, _ = trajectory(cfg, "fp64", cfg["steps"])
-    b, s, _ = trajectory(cfg, "mixed", cfg["steps"])
+    cfg["options"] = dict(cfg["options"], newtonIters=40, pcgMaxIters=3000, gradTol=1e-8)
+    a, _, ca = trajectory(cfg, "fp64", cfg["steps"], exact=1e-6)
+    b, s, cb_ = trajectory(cfg, "mixed", cfg["steps"], exact=1e-6)
     err = rel_err(b, a)
     miny = min(float(x[1::3].min()) for x in b)
-    print(f"floor drape 32x32 mixed vs fp64 over {cfg['steps']} steps: max rel pos err {err:.3e}, min y {miny:.3e}")
+    print(f"floor drape 32x32 mixed vs fp64 over {cfg['steps']} steps: max rel pos err {err:.3e}, "
+          f"min y {miny:.3e}, converged fp64 {ca} mixed {cb_}")
     assert np.all(np.isfinite(b[-1]))
+    assert ca == cfg["steps"] and cb_ == cfg["steps"]
+    assert err <= POS_TOL, err
     assert miny > cfg["contact"]["dMinM"] - 1e-12
     assert s.lastStats.contact["activePairs"] > 0
