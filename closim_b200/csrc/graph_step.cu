@@ -297,8 +297,8 @@ void Solver::graph_capture(double h) {
     g.push(hSolve, cudaGraphCondTypeIf);
     {
       mx_prepare(d, mb, d.precond >= 1, g.cur(), &lc);
-      GCK((cudaError_t)mx_launch_pcg_cluster(d, mb, fp.p, fp2.p, contact ? contact->dd : nullptr, opts.pcg_max_iters,
-                                             pcgTol, mxCluster, g.cur()));
+      GCK((cudaError_t)mx_launch_pcg_cluster(d, mb, cluster_plan_for(mb), fp.p, fp2.p, contact ? contact->dd : nullptr,
+                                             opts.pcg_max_iters, pcgTol, mxCluster, g.cur()));
       lc++;
       const cudaGraphConditionalHandle hTrial = g.handle(0);
       const cudaGraphConditionalHandle hAccept = g.handle(0);

@@ -41,14 +41,29 @@ __device__ __forceinline__ float coarse_share(const MixBufs& mb, int dom, float 
   return dc > 1e-12f ? 0.5f * rc * sc2 / dc : 0.f;
 }
 
+// Device copy of the one-cluster PCG's per-CTA element lists (cluster_plan.hpp).
+// resident = 1: phase A stages p on each CTA's halo in shared memory and runs
+// the element HVPs from shared memory; 0: the vertex-major record gathers.
+struct ClPlan {
+  int resident;
+  int smemBytes;  // dynamic shared memory of the launch
+  const int *vb, *haloOff, *halo, *triOff, *triId, *hinOff, *hinId, *incOff, *incHin, *ownHalo, *vDst;
+  const ushort4 *triLoc, *hinLoc;
+  const uint32_t* inc;
+};
+
 void mx_prepare(const Dev& d, const MixBufs& mb, bool schwarz, cudaStream_t s, int64_t* lc);
 int mx_pcg_grid_blocks(const Dev& d);
 int mx_launch_pcg(const Dev& d, const MixBufs& mb, int maxIters, double tol, int blocks, cudaStream_t s);
 // One-cluster PCG (mixed_cluster.cu): pA/pB are 3n-float direction buffers,
 // coef one double per active contact.
+constexpr int kClWarps = 16;  // warps per CTA of the one-cluster PCG (512 threads)
 int mx_cluster_size();
-int mx_launch_pcg_cluster(const Dev& d, const MixBufs& mb, float* pA, float* pB, double* coef, int maxIters,
-                          double tol, int clusterSize, cudaStream_t s);
+// True when a cluster of `clusterSize` CTAs with `smemBytes` of dynamic shared
+// memory each can be co-scheduled (sets the kernel's shared-memory limit).
+bool mx_cluster_resident_ok(int clusterSize, size_t smemBytes);
+int mx_launch_pcg_cluster(const Dev& d, const MixBufs& mb, const ClPlan& plan, float* pA, float* pB, double* coef,
+                          int maxIters, double tol, int clusterSize, cudaStream_t s);
 void mx_grad_final(const Dev& d, cudaStream_t s, int64_t* lc);
 void mx_energy_final(const Dev& d, cudaStream_t s, int64_t* lc);
 

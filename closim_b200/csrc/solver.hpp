@@ -15,6 +15,7 @@
 
 #include "../../include/closim_cuda.h"
 #include "adjoint.cuh"
+#include "cluster_plan.hpp"
 #include "contact_host.hpp"
 #include "mixed.cuh"
 #include "plain.cuh"
@@ -110,6 +111,14 @@ class Solver {
   MixBufs mb{};
   int mxBlocks = 1;
   int mxCluster = 0;  // CTAs of the one-cluster PCG (0: grid-wide cooperative PCG)
+  // Per-CTA element lists of the one-cluster PCG's resident phase A; clRes[k]
+  // (k = 1 with the Gauss-Newton bending term) says whether they fit.
+  ClusterPlanHost clHost;
+  DBuf<int> clVb, clHaloOff, clHalo, clTriOff, clTriId, clHinOff, clHinId, clIncOff, clIncHin, clOwnHalo, clVDst;
+  DBuf<uint16_t> clTriLoc, clHinLoc;
+  DBuf<uint32_t> clInc;
+  ClPlan clPlan{};
+  bool clRes[2] = {false, false};
   Dev d{};
   // profiling of the linear-solve kernel
   bool prof = false;
@@ -312,6 +321,7 @@ class Solver {
         fvrec.alloc(5 * 3 * (size_t)cm.m);
         mb.vrec = fvrec.p;
         mb.triSlot = triSlot.p;
+        build_cluster_resident();
       }
     }
     upload_pins();
@@ -461,7 +471,7 @@ class Solver {
         CK((cudaError_t)newton_exact_solve(a, adj_grid_blocks(d), stream));
         lc += 3;
       } else if (mixed() && mxCluster > 0)
-        CK((cudaError_t)mx_launch_pcg_cluster(d, mb, fp.p, fp2.p, d.hasContact ? d.c.dd : nullptr,
+        CK((cudaError_t)mx_launch_pcg_cluster(d, mb, cluster_plan_for(mb), fp.p, fp2.p, d.hasContact ? d.c.dd : nullptr,
                                               opts.pcg_max_iters, exactMixed ? std::max(newtonTol, kMixedTolFloor) : 1e-3,
                                               mxCluster, stream));
       else if (mixed()) CK((cudaError_t)mx_launch_pcg(d, mb, opts.pcg_max_iters, 1e-3, mxBlocks, stream));
@@ -636,6 +646,53 @@ class Solver {
   // Relative PCG tolerance the FP32 solve of the exact-Newton mode is held to
   // at the tightest (single precision cannot resolve residuals much below it).
   static constexpr double kMixedTolFloor = 1e-5;
+  // Per-CTA lists for the resident phase A of the one-cluster PCG, when the
+  // largest CTA's share fits in shared memory (CLOSIM_MX_RESIDENT=0 turns it off).
+  void build_cluster_resident() {
+    clRes[0] = clRes[1] = false;
+    clPlan = ClPlan{};
+    const char* env = std::getenv("CLOSIM_MX_RESIDENT");
+    if (env && std::string(env) == "0") return;
+    build_cluster_plan(mesh, mxCluster, kClWarps, clHost);
+    if (!clHost.ok) return;
+    clRes[1] = mx_cluster_resident_ok(mxCluster, clHost.smemHinge);
+    clRes[0] = clRes[1] || mx_cluster_resident_ok(mxCluster, clHost.smemNoHinge);
+    if (!clRes[0]) return;
+    auto up = [&](DBuf<int>& b, const std::vector<int>& v) {
+      b.alloc(std::max<size_t>(v.size(), 1));
+      b.upload(v.data(), v.size(), stream);
+      return (const int*)b.p;
+    };
+    clPlan.vb = up(clVb, clHost.vb);
+    clPlan.haloOff = up(clHaloOff, clHost.haloOff);
+    clPlan.halo = up(clHalo, clHost.halo);
+    clPlan.triOff = up(clTriOff, clHost.triOff);
+    clPlan.triId = up(clTriId, clHost.triId);
+    clPlan.hinOff = up(clHinOff, clHost.hinOff);
+    clPlan.hinId = up(clHinId, clHost.hinId);
+    clPlan.incOff = up(clIncOff, clHost.incOff);
+    clPlan.incHin = up(clIncHin, clHost.incHin);
+    clPlan.ownHalo = up(clOwnHalo, clHost.ownHalo);
+    clPlan.vDst = up(clVDst, clHost.vDst);
+    clTriLoc.alloc(std::max<size_t>(clHost.triLoc.size(), 4));
+    clTriLoc.upload(clHost.triLoc.data(), clHost.triLoc.size(), stream);
+    clHinLoc.alloc(std::max<size_t>(clHost.hinLoc.size(), 4));
+    clHinLoc.upload(clHost.hinLoc.data(), clHost.hinLoc.size(), stream);
+    clInc.alloc(std::max<size_t>(clHost.inc.size(), 1));
+    clInc.upload(clHost.inc.data(), clHost.inc.size(), stream);
+    clPlan.triLoc = reinterpret_cast<const ushort4*>(clTriLoc.p);
+    clPlan.hinLoc = reinterpret_cast<const ushort4*>(clHinLoc.p);
+    clPlan.inc = clInc.p;
+  }
+  // The plan for a launch: resident when this launch's lists fit.
+  ClPlan cluster_plan_for(const MixBufs& m) const {
+    ClPlan p = clPlan;
+    const int k = m.hrec ? 1 : 0;
+    p.resident = clRes[k] && clHost.nrank == mxCluster && d.precond >= 1 ? 1 : 0;
+    p.smemBytes = p.resident ? (int)(k ? clHost.smemHinge : clHost.smemNoHinge) : 0;
+    return p;
+  }
+
   DBuf<float4> hrecBuf;
   float4* ensure_hrec() {
     if (hrecBuf.n < 4 * (size_t)mesh.hg) hrecBuf.alloc(4 * (size_t)mesh.hg);

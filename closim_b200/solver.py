@@ -442,10 +442,10 @@ class CudaSolver:
                     forwardConverged=int(out[4]))
 
     def launchInfo(self) -> dict:
-        out = np.zeros(4, np.int32)
+        out = np.zeros(6, np.int32)
         self._check(self._lib.cs_solver_info(self._h, L.ptr(out), len(out)))
         return dict(pcgClusterCtas=int(out[0]), pcgGridCtas=int(out[1]), fp64PcgCtas=int(out[2]),
-                    schwarzDomains=int(out[3]))
+                    schwarzDomains=int(out[3]), residentSmem=int(out[4]), residentSmemExact=int(out[5]))
 
     def profilePhases(self) -> dict:
         out = np.zeros(len(self.PHASES))

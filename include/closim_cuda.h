@@ -192,7 +192,10 @@ int cs_profile_read(cs_solver* s, double* out5);
 int cs_profile_phases(cs_solver* s, double* out, int32_t n);
 /* Launch shapes chosen at cs_initialize (diagnostic): out[0] CTAs of the
  * one-cluster mixed PCG (0 = the grid-wide kernel is used), out[1] CTAs of the
- * grid-wide mixed PCG, out[2] CTAs of the FP64 PCG, out[3] Schwarz domains. */
+ * grid-wide mixed PCG, out[2] CTAs of the FP64 PCG, out[3] Schwarz domains,
+ * out[4] / out[5] dynamic shared memory per CTA (bytes) of the one-cluster
+ * PCG's resident element lists without / with the Gauss-Newton bending term
+ * (0 = they do not fit and the kernel gathers from global memory). */
 int cs_solver_info(cs_solver* s, int32_t* out, int32_t n);
 
 /* ---- SimulationSession.doStep hand-off (src/view/sim-session.ts:132-150) ----
