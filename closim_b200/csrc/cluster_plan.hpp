@@ -32,12 +32,22 @@ struct HostMesh;
 
 // Byte offsets of one CTA's shared-memory regions (16-byte aligned).
 struct ClSmem {
-  int pH, triD, triO, hinG, hinL, hinS, inc, incOff, incHin, ownH, ownMP, cOff, ownDst, bufB, Lp, halo, total;
+  int pH, triD, triO, hinG, hinL, hinS, inc, incOff, incHin, ownH, ownMP, cOff, ownDst, bufB, Lp, halo, cShare, cRec,
+      cCap, total;
 };
+
+// Bytes of shared memory per on-chip contact record (id + 3 FP32 shares).
+constexpr int kClRecBytes = 16;
+// Dynamic shared memory a CTA of the one-cluster PCG may take: the 227 KB
+// opt-in limit less the kernel's static shared memory (about 2.2 KB) and a margin.
+constexpr int kClMaxDynSmem = 227 * 1024 - 4096;
 
 CL_HD inline int cl_up16(int b) { return (b + 15) & ~15; }
 
-CL_HD inline ClSmem cl_smem_layout(int nHalo, int nTri, int nHin, int nInc, int nOwned, int nSlots, bool hinges) {
+// cap: contact records kept on chip (the rest of the CTA's records use global
+// scratch); sized on the host to fill the launch's shared memory.
+CL_HD inline ClSmem cl_smem_layout(int nHalo, int nTri, int nHin, int nInc, int nOwned, int nSlots, bool hinges,
+                                   int cap = 0) {
   ClSmem s;
   int o = 0;
   // first: peers write into it through distributed shared memory at the same
@@ -45,7 +55,7 @@ CL_HD inline ClSmem cl_smem_layout(int nHalo, int nTri, int nHin, int nInc, int 
   s.bufB = o; o += cl_up16(nSlots * 24 * 16);  // per domain dof: Ap, p, x, r
   s.pH = o;   o += cl_up16(nHalo * 16);        // p on the halo, float4
   s.triD = o; o += cl_up16(nTri * 64);         // triangle record: 14 floats + packed local ids
-  s.triO = o; o += cl_up16(nTri * 24);         // triangle output: g1, g2 (corner 0 is -(g1 + g2))
+  s.triO = o; o += cl_up16(nTri * 36);         // triangle output: the three corner shares
   const int nh = hinges ? nHin : 0;
   s.hinG = o; o += cl_up16(nh * 48);           // Gauss-Newton factor g (12 floats)
   s.hinL = o; o += cl_up16(nh * 8);            // 4 local ids
@@ -59,6 +69,9 @@ CL_HD inline ClSmem cl_smem_layout(int nHalo, int nTri, int nHin, int nInc, int 
   s.ownDst = o; o += cl_up16(nOwned * 4);      // vDst of the owned vertices
   s.Lp = o;   o += cl_up16(nSlots * 300 * 4);  // packed lower triangle of each domain's inverse
   s.halo = o; o += cl_up16(nHalo * 4);         // global vertex ids of the halo
+  s.cCap = cap;
+  s.cShare = o; o += cl_up16(cap * 12);        // contact shares (FP32) of the on-chip records
+  s.cRec = o; o += cl_up16(cap * 4);           // their record ids
   s.total = o;
   return s;
 }

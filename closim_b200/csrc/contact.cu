@@ -437,10 +437,43 @@ __global__ void k_contact_prep(CView v, const double* x, int na) {
   v.tf[i] = fr[0] * u[0] + fr[1] * u[1] + fr[2] * u[2];
 }
 
-__global__ void k_contact_chains(CView v, int na) {
+// Barrier energy and friction work of the step's diagnostics. The FP64 path
+// adds the terms left to right like the reference; the mixed path (tree = 1)
+// uses a fixed-order block tree: each of the 1024 threads adds a strided
+// subset, then warp and block trees (same bits on every run).
+__global__ void __launch_bounds__(1024) k_contact_chains(CView v, int na, int tree) {
   if (na < 0) na = v.acnt ? v.acnt[AC_NA] : 0;
-  if (threadIdx.x == 0) v.diag->barrierEnergy = seq_sum(v.tc, na);
-  if (threadIdx.x == 32) v.diag->frictionWork = v.diag->frictionWork + seq_sum(v.tf, na);
+  if (!tree) {
+    if (threadIdx.x == 0) v.diag->barrierEnergy = seq_sum(v.tc, na);
+    if (threadIdx.x == 32) v.diag->frictionWork = v.diag->frictionWork + seq_sum(v.tf, na);
+    return;
+  }
+  __shared__ double ws[2][32];
+  double a = 0, b = 0;
+  for (int i = threadIdx.x; i < na; i += blockDim.x) {
+    a += v.tc[i];
+    b += v.tf[i];
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    a += __shfl_down_sync(0xffffffffu, a, o);
+    b += __shfl_down_sync(0xffffffffu, b, o);
+  }
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) { ws[0][w] = a; ws[1][w] = b; }
+  __syncthreads();
+  if (w == 0) {
+    const int nw = blockDim.x >> 5;
+    a = lane < nw ? ws[0][lane] : 0.0;
+    b = lane < nw ? ws[1][lane] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) {
+      a += __shfl_down_sync(0xffffffffu, a, o);
+      b += __shfl_down_sync(0xffffffffu, b, o);
+    }
+    if (lane == 0) {
+      v.diag->barrierEnergy = a;
+      v.diag->frictionWork = v.diag->frictionWork + b;
+    }
+  }
 }
 
 // The contact gradient in two passes: one thread per (contact, slot) record
@@ -1276,10 +1309,10 @@ void ContactHost::gradient_terms(Solver& s) {
   CView v = view(*this, s);
   if (na > 0) {
     k_contact_prep<<<cnb(na), kCT, 0, st>>>(v, s.d.x, na);
-    k_contact_chains<<<1, 64, 0, st>>>(v, na);
+    k_contact_chains<<<1, s.mixed() ? 1024 : 64, 0, st>>>(v, na, s.mixed() ? 1 : 0);
     lc += 2;
   } else {
-    k_contact_chains<<<1, 64, 0, st>>>(v, 0);
+    k_contact_chains<<<1, 64, 0, st>>>(v, 0, 0);
     lc++;
   }
   if (na > 0) {
@@ -1643,7 +1676,7 @@ void ContactHost::cap_gradient_terms(Solver& s, GraphCtx& g) {
   CView v = cview(*this, s);
   const long cap = (long)actCap;
   k_contact_prep<<<cnb(cap), kCT, 0, st>>>(v, s.d.x, -1);
-  k_contact_chains<<<1, 64, 0, st>>>(v, -1);
+  k_contact_chains<<<1, s.mixed() ? 1024 : 64, 0, st>>>(v, -1, s.mixed() ? 1 : 0);
   k_contact_grad_rec<<<cnb(4 * cap), kCT, 0, st>>>(v, (int)(4 * cap));
   k_contact_grad_gather<<<cnb(n), kCT, 0, st>>>(v, s.d.cgrad);
   k_contact_curv<<<cnb(cap), kCT, 0, st>>>(v, s.d.x, -1);

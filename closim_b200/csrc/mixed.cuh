@@ -47,6 +47,7 @@ __device__ __forceinline__ float coarse_share(const MixBufs& mb, int dom, float 
 struct ClPlan {
   int resident;
   int smemBytes;  // dynamic shared memory of the launch
+  int cCap;       // contact records per CTA kept on chip
   const int *vb, *haloOff, *halo, *triOff, *triId, *hinOff, *hinId, *incOff, *incHin, *ownHalo, *vDst;
   const ushort4 *triLoc, *hinLoc;
   const uint32_t* inc;

@@ -42,9 +42,6 @@ namespace cs {
 
 constexpr int kClT = 512;
 static_assert(kClT == 32 * kClWarps, "the per-CTA lists assume kClWarps warps per CTA");
-// Dynamic shared memory a CTA may take: the 227 KB opt-in limit less this
-// kernel's static shared memory (about 1.2 KB) and a margin.
-constexpr size_t kClMaxDynSmem = 227 * 1024 - 4096;
 
 struct ClArgs {
   Dev d;
@@ -62,27 +59,21 @@ struct ClArgs {
 // reads only its own shared memory.
 typedef double RedBank[16][4];
 
-// Cluster-wide totals of K partials from the local bank: lane r of warp 0
-// reads CTA r's row, a fixed shuffle tree adds them, and the result is
-// broadcast through shared memory: identical bits in every CTA.
+// Cluster-wide totals of K partials from the local bank: in every warp, lane r
+// reads CTA r's row and a fixed shuffle tree adds the rows, so every warp of
+// every CTA holds identical bits without a block barrier. The bank is
+// rewritten only after the next cluster barrier, which no thread passes
+// before its own read.
 template <int K>
-__device__ __forceinline__ void cl_totals(const RedBank& bank, int nrank, double* out, double* bc) {
-  if (threadIdx.x < 32) {
-    double v[K];
+__device__ __forceinline__ void cl_totals(const RedBank& bank, int nrank, double* out) {
+  const int lane = threadIdx.x & 31;
 #pragma unroll
-    for (int k = 0; k < K; k++) v[k] = threadIdx.x < nrank ? bank[threadIdx.x][k] : 0.0;
+  for (int k = 0; k < K; k++) {
+    double s = lane < nrank ? bank[lane][k] : 0.0;
 #pragma unroll
-    for (int k = 0; k < K; k++) {
-      double s = v[k];
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-      if (threadIdx.x == 0) bc[k] = s;
-    }
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    out[k] = __shfl_sync(0xffffffffu, s, 0);
   }
-  __syncthreads();
-#pragma unroll
-  for (int k = 0; k < K; k++) out[k] = bc[k];
-  // no trailing barrier: consecutive calls alternate between two bc banks
 }
 
 // This CTA's sums of K per-thread values, pushed as row `rank` of every peer's
@@ -165,12 +156,18 @@ __device__ __forceinline__ void cl_slip_jvp(const Frozen& f, const float* z, con
 // Frozen-contact shares of the contact records [r0, r1) (vertex-major, one
 // record per thread: a vertex may sit in many contacts), written to the record
 // scratch and summed per vertex later in record order.
+//
+// Resident kernel: the first `cap` records' ids come from recS (copied at
+// launch) and their shares go to shareS (shared memory, FP64, 3 per record);
+// records beyond cap use the global record list and scratch.
 __device__ __forceinline__ void cl_contact_records(const Dev& d, const MixBufs& mb, const double* coef,
                                                    const float* pc, float beta, bool first, uint32_t r0,
-                                                   uint32_t r1) {
+                                                   uint32_t r1, const uint32_t* recS = nullptr,
+                                                   double* shareS = nullptr, uint32_t cap = 0) {
   const Contact& c = d.c;
   for (uint32_t q = r0 + threadIdx.x; q < r1; q += blockDim.x) {
-    const uint32_t rec = c.cRec[q];
+    const bool onChip = q - r0 < cap;
+    const uint32_t rec = onChip ? recS[q - r0] : c.cRec[q];
     const double g = coef[rec >> 2];
     double ch[3] = {0, 0, 0};
     if (g != 0) {
@@ -187,7 +184,7 @@ __device__ __forceinline__ void cl_contact_records(const Dev& d, const MixBufs& 
         slip_jt_slot(f, rec & 3, F, ch);
       }
     }
-    double* o = c.recScratch + (size_t)q * 3;
+    double* o = onChip ? shareS + (size_t)(q - r0) * 3 : c.recScratch + (size_t)q * 3;
     o[0] = ch[0]; o[1] = ch[1]; o[2] = ch[2];
   }
 }
@@ -219,6 +216,107 @@ __device__ __forceinline__ DomFacts cl_domain_facts(const Dev& d, int dom0, int 
     }
   }
   return f;
+}
+
+// Resident kernel's contact records, in FP32 like the rest of the operator:
+// everything a record reads from global memory (its frozen contact's ids,
+// weights and normal, the barrier curvature and the friction terms) is issued
+// at once, then the p of its stencil, from the halo when the vertex is owned by
+// this CTA (always, for floor contacts) and from global memory otherwise. The
+// terms are cl_contact_records' (dist_grad_slot, slip_jvp, fric_hess_apply,
+// slip_jt_slot) on the same p values. On-chip shares are FP32 (shareS);
+// records beyond cap go to the global scratch as FP64.
+__device__ __forceinline__ void cl_contact_records_res(const Dev& d, const MixBufs& mb, const double* coef,
+                                                       const float* pc, float beta, bool first, uint32_t r0,
+                                                       uint32_t r1, const uint32_t* recS, float* shareS, uint32_t cap,
+                                                       const float4* pH, const int* ownHS, int vb0, int nOwn) {
+  const Contact& c = d.c;
+  for (uint32_t q = r0 + threadIdx.x; q < r1; q += blockDim.x) {
+    const bool onChip = q - r0 < cap;
+    const uint32_t rec = onChip ? recS[q - r0] : c.cRec[q];
+    const int ci = (int)(rec >> 2), slot = (int)(rec & 3);
+    const Frozen* fr = c.active + ci;
+    const int kind = fr->kind;
+    // stencil: kind 0 (p, a, b, c), kind 1 (a, b, c, d), kind 2 (p)
+    const int vs[4] = {kind == 1 ? fr->a : fr->p, kind == 1 ? fr->b : fr->a, kind == 1 ? fr->c : fr->b,
+                       kind == 1 ? fr->d : fr->c};
+    const float w[4] = {(float)fr->w0, (float)fr->w1, (float)fr->w2, (float)fr->w3};
+    const float nx = (float)fr->nx, ny = (float)fr->ny, nz = (float)fr->nz;
+    const float g = (float)coef[ci];
+    float fs = 0.f, ft[3] = {0.f, 0.f, 0.f}, fn[3] = {0.f, 0.f, 0.f};
+    if (c.fric) {
+      const double* h = c.fh + (size_t)ci * 8;
+      fs = (float)h[1];
+      ft[0] = (float)h[2]; ft[1] = (float)h[3]; ft[2] = (float)h[4];
+      fn[0] = (float)h[5]; fn[1] = (float)h[6]; fn[2] = (float)h[7];
+    }
+    float3 P[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      P[k] = make_float3(0.f, 0.f, 0.f);
+      const int v = vs[k];
+      if (v < 0 || (kind == 2 && k > 0)) continue;
+      const int lv = v - vb0;
+      if (lv >= 0 && lv < nOwn) {
+        const float4 t = pH[ownHS[lv]];
+        P[k] = make_float3(t.x, t.y, t.z);
+      } else {
+        P[k] = ld_p(mb.z, pc, beta, first, v);
+      }
+    }
+    float ch[3] = {0.f, 0.f, 0.f};
+    if (g != 0.f) {
+      float jvp;
+      if (kind == 2) {
+        jvp = P[0].y;
+      } else {
+        float nv[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) nv[k] = nx * P[k].x + ny * P[k].y + nz * P[k].z;
+        jvp = kind == 0 ? nv[0] - w[0] * nv[1] - w[1] * nv[2] - w[2] * nv[3]
+                        : w[0] * nv[0] + w[1] * nv[1] + w[2] * nv[2] + w[3] * nv[3];
+      }
+      const float gj = g * jvp;
+      if (kind == 2) {
+        ch[1] += gj;
+      } else {
+        // dist_grad_slot: slot weight times the normal
+        const float ws = kind == 0 ? (slot == 0 ? 1.f : -(slot == 1 ? w[0] : slot == 2 ? w[1] : w[2]))
+                                   : (slot == 0 ? w[0] : slot == 1 ? w[1] : slot == 2 ? w[2] : w[3]);
+        ch[0] += gj * ws * nx; ch[1] += gj * ws * ny; ch[2] += gj * ws * nz;
+      }
+    }
+    if (fs != 0.f) {  // exact-Newton mode: friction potential Hessian (slip_jvp, fric_hess_apply)
+      float du[3];
+      if (kind == 2) {
+        du[0] = P[0].x; du[1] = P[0].y; du[2] = P[0].z;
+      } else if (kind == 0) {
+        du[0] = P[0].x - w[0] * P[1].x - w[1] * P[2].x;
+        du[1] = P[0].y - w[0] * P[1].y - w[1] * P[2].y;
+        du[2] = P[0].z - w[0] * P[1].z - w[1] * P[2].z;
+      } else {
+        du[0] = w[0] * P[0].x + w[1] * P[1].x + w[2] * P[2].x + w[3] * P[3].x;
+        du[1] = w[0] * P[0].y + w[1] * P[1].y + w[2] * P[2].y + w[3] * P[3].y;
+        du[2] = w[0] * P[0].z + w[1] * P[1].z + w[2] * P[2].z + w[3] * P[3].z;
+      }
+      const float nd = fn[0] * du[0] + fn[1] * du[1] + fn[2] * du[2];
+      const float pu[3] = {du[0] - nd * fn[0], du[1] - nd * fn[1], du[2] - nd * fn[2]};
+      const float td = ft[0] * pu[0] + ft[1] * pu[1] + ft[2] * pu[2];
+      // slip_jt_slot weight of this slot
+      const float wj = kind == 2 ? (slot == 0 ? 1.f : 0.f)
+                       : kind == 0 ? (slot == 0 ? 1.f : slot == 1 ? -w[0] : slot == 2 ? -w[1] : 0.f)
+                                   : (slot == 0 ? w[0] : slot == 1 ? w[1] : slot == 2 ? w[2] : w[3]);
+#pragma unroll
+      for (int k = 0; k < 3; k++) ch[k] += wj * (fs * (pu[k] - td * ft[k]));
+    }
+    if (onChip) {
+      float* o = shareS + (size_t)(q - r0) * 3;
+      o[0] = ch[0]; o[1] = ch[1]; o[2] = ch[2];
+    } else {
+      double* o = c.recScratch + (size_t)q * 3;
+      o[0] = ch[0]; o[1] = ch[1]; o[2] = ch[2];
+    }
+  }
 }
 
 // Phase B on K Schwarz domains dom0, dom0 + step, ... at once (one warp, lane =
@@ -439,7 +537,7 @@ __global__ void __launch_bounds__(kClT, 1) k_mx_pcg_cluster(ClArgs A) {
       const int first = rank * W + u * nwarps;
       if (first < d.D) nSlots = u * W + min(W, d.D - first);
     }
-    const ClSmem L = cl_smem_layout(nHalo, nTri, nHin, nInc, nOwn, nSlots, useHin);
+    const ClSmem L = cl_smem_layout(nHalo, nTri, nHin, nInc, nOwn, nSlots, useHin, P.cCap);
     if (threadIdx.x == 0) {
       Ls = L;
       Lc[0] = vb0; Lc[1] = nOwn; Lc[2] = nHalo; Lc[3] = nTri; Lc[4] = nHin; Lc[5] = nSlots;
@@ -487,6 +585,12 @@ __global__ void __launch_bounds__(kClT, 1) k_mx_pcg_cluster(ClArgs A) {
     int* ownHS = reinterpret_cast<int*>(cl_dyn + L.ownH);
     float2* ownMP = reinterpret_cast<float2*>(cl_dyn + L.ownMP);
     uint32_t* cOffS = reinterpret_cast<uint32_t*>(cl_dyn + L.cOff);
+    if (d.hasContact) {
+      // this launch's contact records of the owned vertices: ids on chip up to the capacity
+      const uint32_t r0 = d.c.cOff[vb0], nr = min(d.c.cOff[vb0 + nOwn] - r0, (uint32_t)L.cCap);
+      uint32_t* recS = reinterpret_cast<uint32_t*>(cl_dyn + L.cRec);
+      for (uint32_t q = threadIdx.x; q < nr; q += blockDim.x) recS[q] = d.c.cRec[r0 + q];
+    }
     for (int lv = threadIdx.x; lv <= nOwn; lv += blockDim.x) {
       incOffS[lv] = P.incOff[vb0 + lv] - i0;
       if (d.hasContact) cOffS[lv] = d.c.cOff[vb0 + lv];
@@ -529,7 +633,7 @@ __global__ void __launch_bounds__(kClT, 1) k_mx_pcg_cluster(ClArgs A) {
   }
   cl.sync();
   double tot[3];
-  cl_totals<3>(red[round & 1], nrank, tot, BC);
+  cl_totals<3>(red[round & 1], nrank, tot);
   round++;
   double rzCur = tot[2];
   const double bNorm = sqrt(tot[0]);
@@ -562,16 +666,19 @@ __global__ void __launch_bounds__(kClT, 1) k_mx_pcg_cluster(ClArgs A) {
       const int* incHinS = reinterpret_cast<const int*>(cl_dyn + L.incHin);
       const int* ownHS = reinterpret_cast<const int*>(cl_dyn + L.ownH);
       const int* haloS = reinterpret_cast<const int*>(cl_dyn + L.halo);
-      // A0: p_k on the halo; contact records of the owned vertices
+      // A0: p_k on the halo
       for (int i = threadIdx.x; i < nHalo; i += blockDim.x) {
         const float3 pv = ld_p(mb.z, pc, beta, first, haloS[i]);
         pH[i] = make_float4(pv.x, pv.y, pv.z, 0.f);
       }
+      __syncthreads();
+      // contact records of the owned vertices (they read the halo)
       if (d.hasContact) {
         const uint32_t* cOffS = reinterpret_cast<const uint32_t*>(cl_dyn + L.cOff);
-        cl_contact_records(d, mb, A.coef, pc, beta, first, cOffS[0], cOffS[nOwn]);
+        cl_contact_records_res(d, mb, A.coef, pc, beta, first, cOffS[0], cOffS[nOwn],
+                               reinterpret_cast<const uint32_t*>(cl_dyn + L.cRec),
+                               reinterpret_cast<float*>(cl_dyn + L.cShare), (uint32_t)L.cCap, pH, ownHS, vb0, nOwn);
       }
-      __syncthreads();
       // A1: element HVPs from shared memory, triangles then hinges in one index space
       for (int e = threadIdx.x; e < nTri + nHin; e += blockDim.x) {
         if (e < nTri) {
@@ -580,9 +687,13 @@ __global__ void __launch_bounds__(kClT, 1) k_mx_pcg_cluster(ClArgs A) {
           float g1[3], g2[3];
           tri_hvp_g12(triD[e * 4], triD[e * 4 + 1], triD[e * 4 + 2], t3, pH[l01 & 0xffffu], pH[l01 >> 16], pH[l2],
                       C00, C11, C01, G, g1, g2);
-          float* o = triO + e * 6;
-          o[0] = g1[0]; o[1] = g1[1]; o[2] = g1[2];
-          o[3] = g2[0]; o[4] = g2[1]; o[5] = g2[2];
+          float* o = triO + e * 9;  // corner shares: -(g1 + g2), g1, g2
+#pragma unroll
+          for (int q = 0; q < 3; q++) {
+            o[q] = -(g1[q] + g2[q]);
+            o[3 + q] = g1[q];
+            o[6 + q] = g2[q];
+          }
         } else {
           const int sl = e - nTri;
           const ushort4 l = hinL[sl];
@@ -613,10 +724,9 @@ __global__ void __launch_bounds__(kClT, 1) k_mx_pcg_cluster(ClArgs A) {
 #pragma unroll
             for (int u = 0; u < 4; u++) {
               if (rec[u] == 0xffffffffu) continue;
-              const float* o = triO + (rec[u] >> 2) * 6;
-              const uint32_t c = rec[u] & 3;
+              const float* o = triO + (rec[u] >> 2) * 9 + (rec[u] & 3) * 3;
 #pragma unroll
-              for (int q = 0; q < 3; q++) sp[q] += c == 0 ? -(o[q] + o[3 + q]) : c == 1 ? o[q] : o[3 + q];
+              for (int q = 0; q < 3; q++) sp[q] += o[q];
             }
           }
           if (useHin) {
@@ -628,15 +738,11 @@ __global__ void __launch_bounds__(kClT, 1) k_mx_pcg_cluster(ClArgs A) {
               for (int u = 0; u < 4; u++) {
                 if (rec[u] == 0xffffffffu) continue;
                 const float gs = hinS[rec[u] >> 2];
-                const float4* g = hinG + (rec[u] >> 2) * 3;
-                const uint32_t c = rec[u] & 3;  // this vertex's 3 values of g, selected without local memory
-                const float4 g0 = g[0], g1 = g[1], g2 = g[2];
-                const float ga = c == 0 ? g0.x : c == 1 ? g0.w : c == 2 ? g1.z : g2.y;
-                const float gb = c == 0 ? g0.y : c == 1 ? g1.x : c == 2 ? g1.w : g2.z;
-                const float gc = c == 0 ? g0.z : c == 1 ? g1.y : c == 2 ? g2.x : g2.w;
-                sp[0] += gs * ga;
-                sp[1] += gs * gb;
-                sp[2] += gs * gc;
+                // this vertex's 3 values of g: floats 3c .. 3c + 2 of the hinge's 12
+                const float* gc = reinterpret_cast<const float*>(hinG + (rec[u] >> 2) * 3) + (rec[u] & 3) * 3;
+                sp[0] += gs * gc[0];
+                sp[1] += gs * gc[1];
+                sp[2] += gs * gc[2];
               }
             }
           }
@@ -652,9 +758,16 @@ __global__ void __launch_bounds__(kClT, 1) k_mx_pcg_cluster(ClArgs A) {
         double ch[3] = {0, 0, 0};
         if (d.hasContact) {
           const Contact& c = d.c;
+          const float* shareS = reinterpret_cast<const float*>(cl_dyn + L.cShare);
+          const uint32_t r0 = cOffS[0], cap = (uint32_t)L.cCap;
           for (uint32_t q = cOffS[lv]; q < cOffS[lv + 1]; q++) {
-            const double* o = c.recScratch + (size_t)q * 3;
-            ch[0] += o[0]; ch[1] += o[1]; ch[2] += o[2];
+            if (q - r0 < cap) {
+              const float* o = shareS + (size_t)(q - r0) * 3;
+              ch[0] += o[0]; ch[1] += o[1]; ch[2] += o[2];
+            } else {
+              const double* o = c.recScratch + (size_t)q * 3;
+              ch[0] += o[0]; ch[1] += o[1]; ch[2] += o[2];
+            }
           }
         }
         const float2 mp = ownMP[lv];
@@ -773,7 +886,7 @@ __global__ void __launch_bounds__(kClT, 1) k_mx_pcg_cluster(ClArgs A) {
     }
     block_partials<1>(cl, &pAp, red[round & 1], rank, nrank, wsm);
     cl.sync();
-    cl_totals<1>(red[round & 1], nrank, tot, BC);
+    cl_totals<1>(red[round & 1], nrank, tot);
     round++;
     const double pApT = tot[0];
     if (!(pApT > 1e-30)) { iters = k; done = true; break; }
@@ -796,7 +909,7 @@ __global__ void __launch_bounds__(kClT, 1) k_mx_pcg_cluster(ClArgs A) {
     }
     cl.sync();
     double t2[2];
-    cl_totals<2>(red[round & 1], nrank, t2, BC);
+    cl_totals<2>(red[round & 1], nrank, t2);
     round++;
     residual = sqrt(t2[0]);
     if (residual < absTol) { iters = k + 1; done = true; break; }
@@ -828,7 +941,7 @@ __global__ void __launch_bounds__(kClT, 1) k_mx_pcg_cluster(ClArgs A) {
   block_partials<1>(cl, &gt, red[round & 1], rank, nrank, wsm);
   cl.sync();
   double t1[1];
-  cl_totals<1>(red[round & 1], nrank, t1, BC);
+  cl_totals<1>(red[round & 1], nrank, t1);
   round++;
   double gtdx = t1[0];
   bool fallback = false;
@@ -842,7 +955,7 @@ __global__ void __launch_bounds__(kClT, 1) k_mx_pcg_cluster(ClArgs A) {
     }
     block_partials<1>(cl, &gt, red[round & 1], rank, nrank, wsm);
     cl.sync();
-    cl_totals<1>(red[round & 1], nrank, t1, BC);
+    cl_totals<1>(red[round & 1], nrank, t1);
     round++;
     gtdx = t1[0];
   }
@@ -907,7 +1020,7 @@ int mx_cluster_size() {
 }
 
 bool mx_cluster_resident_ok(int clusterSize, size_t smemBytes) {
-  if (clusterSize < 1 || smemBytes > kClMaxDynSmem) return false;
+  if (clusterSize < 1 || smemBytes > (size_t)kClMaxDynSmem) return false;
   // The kernel's limit is process-wide: it only grows, so a launch sized for
   // an earlier solver's mesh stays valid.
   static std::mutex mu;

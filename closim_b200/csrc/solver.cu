@@ -269,7 +269,7 @@ int cs_solver_info(cs_solver* h, int32_t* out, int32_t n) {
     if (!out || n <= 0) throw std::invalid_argument("null output");
     const auto& S = h->s;
     const int32_t v[6] = {S.mxCluster, S.mxBlocks, S.pcgBlocks, S.mesh.D,
-                          S.clRes[0] ? (int32_t)S.clHost.smemNoHinge : 0, S.clRes[1] ? (int32_t)S.clHost.smemHinge : 0};
+                          S.clRes[0] ? (int32_t)S.clSmem[0] : 0, S.clRes[1] ? (int32_t)S.clSmem[1] : 0};
     for (int i = 0; i < n; i++) out[i] = i < 6 ? v[i] : 0;
   });
 }

@@ -119,6 +119,8 @@ class Solver {
   DBuf<uint32_t> clInc;
   ClPlan clPlan{};
   bool clRes[2] = {false, false};
+  size_t clSmem[2] = {0, 0};  // launch's dynamic shared memory
+  int clCap[2] = {0, 0};      // on-chip contact records per CTA
   Dev d{};
   // profiling of the linear-solve kernel
   bool prof = false;
@@ -655,9 +657,16 @@ class Solver {
     if (env && std::string(env) == "0") return;
     build_cluster_plan(mesh, mxCluster, kClWarps, clHost);
     if (!clHost.ok) return;
-    clRes[1] = mx_cluster_resident_ok(mxCluster, clHost.smemHinge);
-    clRes[0] = clRes[1] || mx_cluster_resident_ok(mxCluster, clHost.smemNoHinge);
-    if (!clRes[0]) return;
+    // the shared memory left over holds contact records (up to 8192 per CTA)
+    for (int k = 0; k < 2; k++) {
+      const size_t base = k ? clHost.smemHinge : clHost.smemNoHinge;
+      const long room = (long)kClMaxDynSmem - (long)base - 32;
+      clCap[k] = room > 0 ? (int)std::min<long>(room / kClRecBytes, 8192) : 0;
+      clSmem[k] = base + 32 + (size_t)clCap[k] * kClRecBytes;
+    }
+    clRes[1] = mx_cluster_resident_ok(mxCluster, clSmem[1]);
+    clRes[0] = mx_cluster_resident_ok(mxCluster, clSmem[0]);
+    if (!clRes[0] && !clRes[1]) return;
     auto up = [&](DBuf<int>& b, const std::vector<int>& v) {
       b.alloc(std::max<size_t>(v.size(), 1));
       b.upload(v.data(), v.size(), stream);
@@ -689,7 +698,8 @@ class Solver {
     ClPlan p = clPlan;
     const int k = m.hrec ? 1 : 0;
     p.resident = clRes[k] && clHost.nrank == mxCluster && d.precond >= 1 ? 1 : 0;
-    p.smemBytes = p.resident ? (int)(k ? clHost.smemHinge : clHost.smemNoHinge) : 0;
+    p.smemBytes = p.resident ? (int)clSmem[k] : 0;
+    p.cCap = p.resident ? clCap[k] : 0;
     return p;
   }
 
