@@ -115,17 +115,44 @@ __global__ void __launch_bounds__(kMxWarps * 32) k_mx_schwarz_factor(Dev d, MixB
     const int lv = lane / 3, aa = lane % 3;
     const int v = dvs[wib][lv];
     double* row = a + lane * kFS;
-    for (int k = d.v2tOff[v]; k < d.v2tOff[v + 1]; k++) {
-      const int t = d.v2t[k];
-      const int cvs[3] = {(int)d.idx[t * 3], (int)d.idx[t * 3 + 1], (int)d.idx[t * 3 + 2]};
-      const int ci = cvs[0] == v ? 0 : cvs[1] == v ? 1 : 2;
-      const float* h = mb.h9 + (size_t)t * 81 + (ci * 3 + aa) * 9;
-      for (int cj = 0; cj < 3; cj++) {
-        int lw = -1;
-        for (int q = 0; q < dv; q++)
-          if (dvs[wib][q] == cvs[cj]) { lw = q; break; }
-        if (lw < 0) continue;
-        for (int bb = 0; bb < 3; bb++) row[lw * 3 + bb] += h[cj * 3 + bb];
+    if (mb.asmRec) {
+      // precomputed per (vertex, incident triangle) in the v2t order: the row
+      // block's offset in h9 and the corners' local members (15: outside the
+      // domain); four triangles' loads in flight at once
+      const uint32_t k1 = mb.asmOff[v + 1];
+      for (uint32_t k0 = mb.asmOff[v]; k0 < k1; k0 += 4) {
+        uint2 r[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) r[u] = k0 + u < k1 ? mb.asmRec[k0 + u] : make_uint2(0u, 0xfffu);
+        float hv[4][9];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+          const float* h = mb.h9 + (size_t)r[u].x + aa * 9;
+#pragma unroll
+          for (int e = 0; e < 9; e++) hv[u][e] = (r[u].y & 0xfffu) != 0xfffu ? h[e] : 0.f;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+#pragma unroll
+          for (int cj = 0; cj < 3; cj++) {
+            const int lw = (int)((r[u].y >> (4 * cj)) & 15u);
+            if (lw < 15)
+              for (int bb = 0; bb < 3; bb++) row[lw * 3 + bb] += hv[u][cj * 3 + bb];
+          }
+      }
+    } else {
+      for (int k = d.v2tOff[v]; k < d.v2tOff[v + 1]; k++) {
+        const int t = d.v2t[k];
+        const int cvs[3] = {(int)d.idx[t * 3], (int)d.idx[t * 3 + 1], (int)d.idx[t * 3 + 2]};
+        const int ci = cvs[0] == v ? 0 : cvs[1] == v ? 1 : 2;
+        const float* h = mb.h9 + (size_t)t * 81 + (ci * 3 + aa) * 9;
+        for (int cj = 0; cj < 3; cj++) {
+          int lw = -1;
+          for (int q = 0; q < dv; q++)
+            if (dvs[wib][q] == cvs[cj]) { lw = q; break; }
+          if (lw < 0) continue;
+          for (int bb = 0; bb < 3; bb++) row[lw * 3 + bb] += h[cj * 3 + bb];
+        }
       }
     }
     row[lane] += d.diag[v * 3 + aa];

@@ -26,6 +26,13 @@ struct MixBufs {
   // Two-level Schwarz (mas2): per domain the coarse diagonal (x, y, z) of
   // R A P; null for the one-level preconditioner.
   float4* dcoarse;
+  // Schwarz assembly records per (vertex, incident triangle), in the v2t
+  // order: x = the vertex's 3-row block offset in h9 (t * 81 + corner * 27),
+  // y = the triangle corners' member indices in the vertex's domain, 4 bits
+  // each (15: not a member); asmOff (n+1) indexes them per vertex. Null:
+  // the factor derives them from the mesh.
+  const uint32_t* asmOff;
+  const uint2* asmRec;
 };
 
 // Two-level Schwarz share of lane (member l, component c) of a domain warp:

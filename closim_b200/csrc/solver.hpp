@@ -305,6 +305,7 @@ class Solver {
       fdc.alloc((size_t)std::max(mesh.D, 1));
       mb.r = fr.p; mb.z = fz.p; mb.p = fp.p; mb.Ap = fAp.p; mb.x = fx.p;
       mb.elem = felem.p; mb.tris = ftris.p; mb.h9 = fh9.p; mb.Linv = fLinv.p;
+      build_schwarz_assembly();
       mxBlocks = mx_pcg_grid_blocks(d);
       // Sheets up to 20k vertices solve inside one thread-block cluster
       // (on-GPC barriers); larger ones use the grid-wide kernel.
@@ -701,6 +702,49 @@ class Solver {
     p.smemBytes = p.resident ? (int)clSmem[k] : 0;
     p.cCap = p.resident ? clCap[k] : 0;
     return p;
+  }
+
+  // Schwarz assembly records of the mixed factor (MixBufs::asmRec): static
+  // topology, built once per mesh.
+  DBuf<uint32_t> asmOffBuf;
+  DBuf<uint2> asmRecBuf;
+  void build_schwarz_assembly() {
+    mb.asmOff = nullptr;
+    mb.asmRec = nullptr;
+    if (mesh.D == 0 || mesh.maxDomain > 8) return;
+    const int n = mesh.n;
+    std::vector<int> domOf(n, -1), member(n, -1);
+    for (int dm = 0; dm < mesh.D; dm++)
+      for (int l = mesh.domStart[dm]; l < mesh.domStart[dm + 1]; l++) {
+        domOf[mesh.domVerts[l]] = dm;
+        member[mesh.domVerts[l]] = l - mesh.domStart[dm];
+      }
+    std::vector<uint32_t> off(n + 1, 0);
+    std::vector<uint2> rec;
+    rec.reserve(mesh.v2t.size());
+    for (int v = 0; v < n; v++) {
+      off[v] = (uint32_t)rec.size();
+      for (uint32_t k = mesh.v2tOff[v]; k < mesh.v2tOff[v + 1]; k++) {
+        const uint32_t t = mesh.v2t[k];
+        const int c0 = (int)mesh.idx[3 * (size_t)t], c1 = (int)mesh.idx[3 * (size_t)t + 1],
+                  c2 = (int)mesh.idx[3 * (size_t)t + 2];
+        const int ci = c0 == v ? 0 : c1 == v ? 1 : 2;
+        uint32_t lw = 0;
+        const int cs3[3] = {c0, c1, c2};
+        for (int cj = 0; cj < 3; cj++) {
+          const int w = cs3[cj];
+          const uint32_t m = domOf[w] == domOf[v] && domOf[v] >= 0 ? (uint32_t)member[w] : 15u;
+          lw |= m << (4 * cj);
+        }
+        rec.push_back(make_uint2(t * 81u + (uint32_t)ci * 27u, lw));
+      }
+    }
+    off[n] = (uint32_t)rec.size();
+    asmOffBuf.upload(off.data(), off.size(), stream);
+    asmRecBuf.alloc(std::max<size_t>(rec.size(), 1));
+    asmRecBuf.upload(rec.data(), rec.size(), stream);
+    mb.asmOff = asmOffBuf.p;
+    mb.asmRec = asmRecBuf.p;
   }
 
   DBuf<float4> hrecBuf;
