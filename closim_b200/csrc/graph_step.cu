@@ -199,7 +199,8 @@ std::vector<double> Solver::graph_key(double h) const {
   std::vector<double> k = {h, (double)opts.newton_iters, (double)opts.pcg_max_iters, (double)opts.ls_iters,
                            (double)opts.precond, opts.grad_tol, (double)newtonMode, newtonTol, (double)mxCluster,
                            (double)d.npins, (double)(uintptr_t)d.pinIds, (double)(uintptr_t)d.pinPos,
-                           (double)initEpoch, (double)(uintptr_t)hrecBuf.p, gravity[0], gravity[1], gravity[2]};
+                           (double)initEpoch, (double)(uintptr_t)hrecBuf.p, gravity[0], gravity[1], gravity[2],
+                           (double)driftGuess};
   const double m[9] = {mat.areal_density, mat.thickness, mat.stretch_warp, mat.stretch_weft, mat.stretch_coupling,
                        mat.shear, mat.bend_warp, mat.bend_weft, mat.damping};
   k.insert(k.end(), m, m + 9);
@@ -226,6 +227,7 @@ void Solver::graph_capture(double h) {
   for (int k = 0; k < 3; k++) d.gravity[k] = gravity[k];
   d.precond = precond_code();
   d.hasContact = contact ? 1 : 0;
+  d.driftGuess = newtonMode == 1 && driftGuess ? 1 : 0;
   d.x = vx.p;
   d.xt = vxt.p;
   const bool exactMode = newtonMode == 1;

@@ -76,6 +76,12 @@ __device__ __forceinline__ double block_chain(const double* t, int n, double* bu
 }
 
 // ---- predictor (newton.ts:41-50) -------------------------------------------
+// yHat = x0 + h v + h^2 g is the inertial target and, in the reference, the
+// first Newton iterate. Exact-Newton mode starts from x0 + h v instead: for a
+// sheet resting on a barrier, the gravity term pushes every contact vertex
+// into the barrier and Newton spends its first iterations damping back out
+// (on the floor drape, 10 iterations per step against 3 in free fall). The
+// converged step does not depend on the first iterate.
 __global__ void k_predict(Dev d) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= d.n) return;
@@ -84,9 +90,10 @@ __global__ void k_predict(Dev d) {
   for (int k = 0; k < 3; k++) {
     const double x0 = d.x[i * 3 + k];
     d.x0[i * 3 + k] = x0;
-    const double y = x0 + h * d.v[i * 3 + k] + h * h * d.gravity[k];
+    const double drift = x0 + h * d.v[i * 3 + k];
+    const double y = drift + h * h * d.gravity[k];
     d.yHat[i * 3 + k] = y;
-    d.x[i * 3 + k] = y;
+    d.x[i * 3 + k] = d.driftGuess ? drift : y;
   }
 }
 

@@ -99,6 +99,7 @@ struct Dev {
   uint8_t* domFlag;        // D
   double* dcoarse;         // 3D: coarse diagonal of the two-level Schwarz (precond 2)
   int precond;             // 0 Jacobi, 1 one-level Schwarz, 2 two-level Schwarz (mas2)
+  int driftGuess;          // 1: Newton starts from x0 + h v (exact-Newton mode), 0: from yHat (newton.ts:41-50)
   int hasContact;
   Contact c;               // valid when hasContact
 };

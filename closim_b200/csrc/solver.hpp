@@ -388,6 +388,7 @@ class Solver {
     for (int k = 0; k < 3; k++) d.gravity[k] = gravity[k];
     d.precond = precond_code();
     d.hasContact = contact ? 1 : 0;
+    d.driftGuess = newtonMode == 1 && driftGuess ? 1 : 0;
     int64_t& lc = launch_counter();
     if (profPhases) { CK(cudaStreamSynchronize(stream)); phaseT0 = std::chrono::steady_clock::now(); curPhase = PH_OTHER; }
     launch_predict(d, stream);
@@ -645,6 +646,12 @@ class Solver {
   // contact) solved to newtonTol, for rollouts that must converge tightly.
   int newtonMode = 0;
   double newtonTol = 1e-8;
+  // Exact-Newton mode starts Newton from x0 + h v rather than yHat (k_predict);
+  // CLOSIM_DRIFT_GUESS=0 keeps yHat.
+  bool driftGuess = [] {
+    const char* e = std::getenv("CLOSIM_DRIFT_GUESS");
+    return !(e && std::string(e) == "0");
+  }();
 
   // Relative PCG tolerance the FP32 solve of the exact-Newton mode is held to
   // at the tightest (single precision cannot resolve residuals much below it).
