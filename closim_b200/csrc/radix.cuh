@@ -151,6 +151,7 @@ __global__ void __launch_bounds__(kBlockSortThreads) k_block_radix(Key<KW>* k0, 
   __shared__ uint32_t orw[KW], andw[KW];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   constexpr int kWarps = kBlockSortThreads / 32;
+  constexpr int kB = KW <= 1 ? 8 : KW <= 4 ? 4 : 2;  // records per lane in flight
   const int chunk = ((n + kWarps - 1) / kWarps + 31) & ~31;
   const int lo = min(n, warp * chunk), hi = min(n, lo + chunk);
   const uint32_t lt = (1u << lane) - 1u;
@@ -187,12 +188,21 @@ __global__ void __launch_bounds__(kBlockSortThreads) k_block_radix(Key<KW>* k0, 
     for (int w = 0; w < kWarps; w++)
       if (threadIdx.x < 256) cnt[w][threadIdx.x] = 0;
     __syncthreads();
-    for (int base = lo; base < hi; base += 32) {
-      const int i = base + lane;
-      const int dg = i < hi ? (int)digit_of(ki[i], pass) : -1;
-      const uint32_t peers = __match_any_sync(0xffffffffu, dg);
-      if (dg >= 0 && (peers & lt) == 0) cnt[warp][dg] += __popc(peers);
-      __syncwarp();
+    // histogram: each lane loads kB keys of its warp's chunk before counting
+    // any, so the loads of a batch are in flight together
+    for (int base = lo; base < hi; base += 32 * kB) {
+      int dg[kB];
+#pragma unroll
+      for (int u = 0; u < kB; u++) {
+        const int i = base + u * 32 + lane;
+        dg[u] = i < hi ? (int)digit_of(ki[i], pass) : -1;
+      }
+#pragma unroll
+      for (int u = 0; u < kB; u++) {
+        const uint32_t peers = __match_any_sync(0xffffffffu, dg[u]);
+        if (dg[u] >= 0 && (peers & lt) == 0) cnt[warp][dg[u]] += __popc(peers);
+        __syncwarp();
+      }
     }
     __syncthreads();
     // exclusive offsets: digit-major, warp-minor
@@ -222,26 +232,33 @@ __global__ void __launch_bounds__(kBlockSortThreads) k_block_radix(Key<KW>* k0, 
     if (threadIdx.x < 256)
       for (int w = 0; w < kWarps; w++) cnt[w][threadIdx.x] += tot[threadIdx.x];
     __syncthreads();
-    for (int base = lo; base < hi; base += 32) {
-      const int i = base + lane;
-      const bool valid = i < hi;
-      Key<KW> k;
-      uint32_t pl = 0;
-      int dg = -1;
-      if (valid) {
-        k = ki[i];
-        pl = pi[i];
-        dg = (int)digit_of(k, pass);
+    // stable scatter in the same order, kB records per lane loaded at once
+    for (int base = lo; base < hi; base += 32 * kB) {
+      Key<KW> k[kB];
+      uint32_t pl[kB];
+#pragma unroll
+      for (int u = 0; u < kB; u++) {
+        const int i = base + u * 32 + lane;
+        if (i < hi) {
+          k[u] = ki[i];
+          pl[u] = pi[i];
+        }
       }
-      const uint32_t peers = __match_any_sync(0xffffffffu, dg);
-      if (valid) {
-        const uint32_t off = cnt[warp][dg] + __popc(peers & lt);
-        ko[off] = k;
-        po[off] = pl;
+#pragma unroll
+      for (int u = 0; u < kB; u++) {
+        const int i = base + u * 32 + lane;
+        const bool valid = i < hi;
+        const int dg = valid ? (int)digit_of(k[u], pass) : -1;
+        const uint32_t peers = __match_any_sync(0xffffffffu, dg);
+        if (valid) {
+          const uint32_t off = cnt[warp][dg] + __popc(peers & lt);
+          ko[off] = k[u];
+          po[off] = pl[u];
+        }
+        __syncwarp();
+        if (valid && (peers & lt) == 0) cnt[warp][dg] += __popc(peers);
+        __syncwarp();
       }
-      __syncwarp();
-      if (valid && (peers & lt) == 0) cnt[warp][dg] += __popc(peers);
-      __syncwarp();
     }
     __syncthreads();
   }
