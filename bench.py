@@ -359,6 +359,8 @@ def run_batch(args, world, rank, local):
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     total = 0.0
+    if args.profiler_range:
+        torch.cuda.profiler.start()  # ncu --profile-from-start off captures the timed steps only
     for _ in range(args.steps):
         with torch.cuda.stream(ext):
             flush.fill_(1.0)
@@ -367,6 +369,8 @@ def run_batch(args, world, rank, local):
         ev1.record(ext)
         ev1.synchronize()
         total += ev0.elapsed_time(ev1)
+    if args.profiler_range:
+        torch.cuda.profiler.stop()
     clocks = sampler.stop()
     # graph-replayed multi-step call (the production path)
     ev0.record(ext)

@@ -311,7 +311,9 @@ __global__ void k_csr_records(CView v, Key<1>* k, uint32_t* p, int na) {
   if (f.kind == 2) vert = slot == 0 ? f.p : -1;
   else if (f.kind == 0) vert = slot == 0 ? f.p : slot == 1 ? f.a : slot == 2 ? f.b : f.c;
   else vert = slot == 0 ? f.a : slot == 1 ? f.b : slot == 2 ? f.c : f.d;
-  k[i].w[0] = vert >= 0 ? (uint32_t)vert : 0xffffffffu;
+  // unused slots sort after every vertex (key n): with keys below 2^16 the
+  // sort skips its two high byte passes
+  k[i].w[0] = vert >= 0 ? (uint32_t)vert : (uint32_t)v.n;
   p[i] = (uint32_t)i;
 }
 
