@@ -1052,6 +1052,8 @@ void ContactHost::init(Solver& s, const cs_contact_params* prm, int floor_on, do
   dalloc(cint, CI_N);
   dalloc(acnt, AC_N);
   CK(cudaMemset(acnt, 0, AC_N * sizeof(int)));
+  dalloc(csrMemo, 2);
+  CK(cudaMemset(csrMemo, 0xff, 2 * sizeof(int)));
   CK(cudaMallocHost(&hint, CI_N * sizeof(int)));
   CK(cudaMallocHost(&hdiag, sizeof(DevDiag)));
   // Capacities sized from the mesh up front: a buffer that grows mid-run costs
@@ -1114,7 +1116,8 @@ void ContactHost::ensure_active(Solver& s, size_t na) {
   dalloc(recScratch, 24 * c);
   dalloc(fh, 8 * c);
   dalloc(fdd, 3 * c);
-  (void)s;
+  dalloc(csrIds, 5 * c);
+  if (csrMemo) CK(cudaMemsetAsync(csrMemo, 0xff, 2 * sizeof(int), s.stream));  // the saved list is gone
 }
 void ContactHost::ensure_lag(size_t nl) {
   if (nl <= lagCap) return;
@@ -1297,7 +1300,9 @@ void ContactHost::update_active_set(Solver& s, double* x) {
     }
     k_csr_offsets<<<cnb(n + 1), kCT, 0, st>>>(rk0, 4 * na, cOff, n);
     lc++;
+    CK(cudaMemsetAsync(csrMemo, 0xff, 2 * sizeof(int), st));  // captured steps must rebuild
   } else {
+    CK(cudaMemsetAsync(csrMemo, 0xff, 2 * sizeof(int), st));
     CK(cudaMemsetAsync(cOff, 0, ((size_t)n + 1) * 4, st));
   }
   bind(s);
@@ -1569,6 +1574,39 @@ __global__ void k_cap_active_counts(const int* cint, int* acnt, int candCap, int
 // commit's host bookkeeping: the lag table grows by the candidates when there
 // are any, the commit sequence advances when there is any contact.
 __global__ void k_cap_lag_total(int* acnt) { acnt[AC_NTOT] = acnt[AC_LAG] + acnt[AC_NCAND]; }
+// The vertex of record slot `slot` of a frozen contact (-1: unused), as k_csr_records.
+__device__ __forceinline__ int slot_vertex(const Frozen& f, int slot) {
+  if (f.kind == 2) return slot == 0 ? f.p : -1;
+  if (f.kind == 0) return slot == 0 ? f.p : slot == 1 ? f.a : slot == 2 ? f.b : f.c;
+  return slot == 0 ? f.a : slot == 1 ? f.b : slot == 2 ? f.c : f.d;
+}
+__global__ void k_cap_csr_same(CView v, const int* ids, int* memo, const int* acnt) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int na = acnt[AC_NA];
+  if (i >= na || memo[0] != na) return;  // a different count is decided below
+  const Frozen f = v.active[i];
+  const int* q = ids + (size_t)i * 5;
+  bool same = q[0] == f.kind;
+#pragma unroll
+  for (int sl = 0; sl < 4; sl++) same = same && q[1 + sl] == slot_vertex(f, sl);
+  if (!same) atomicOr(memo + 1, 1);
+}
+__global__ void k_cap_csr_decide(int* memo, const int* acnt, cudaGraphConditionalHandle h) {
+  const bool rebuild = memo[1] != 0 || memo[0] != acnt[AC_NA];
+  memo[1] = 0;
+  cudaGraphSetConditional(h, rebuild ? 1u : 0u);
+}
+__global__ void k_cap_csr_save(CView v, int* ids, int* memo, const int* acnt) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int na = acnt[AC_NA];
+  if (i == 0) memo[0] = na;
+  if (i >= na) return;
+  const Frozen f = v.active[i];
+  int* q = ids + (size_t)i * 5;
+  q[0] = f.kind;
+#pragma unroll
+  for (int sl = 0; sl < 4; sl++) q[1 + sl] = slot_vertex(f, sl);
+}
 __global__ void k_cap_lag_advance(int* acnt, int lagCap) {
   if (acnt[AC_NCAND] > 0) {
     if (acnt[AC_NTOT] > lagCap) acnt[AC_ERR] |= ACE_CAPACITY;
@@ -1663,12 +1701,26 @@ void ContactHost::cap_update_active_set(Solver& s, GraphCtx& g, const double* x)
                                       cand_key_bits(idBits, 0), cand.hist, st, &lc);
   k_cand_active<<<cnb(cand.cap), kCT, 0, st>>>(v, x, flip ? cand.p1 : cand.p0, -1);
   k_floor_compact<<<cnb(n), kCT, 0, st>>>(v, x);
-  k_csr_records<<<cnb(4l * (long)actCap), kCT, 0, st>>>(v, rk0, rp0, -1);
-  lc += 3;
-  // 32-bit keys: an even number of passes leaves the result in (rk0, rp0)
-  radix_sort_dev<1>(rk0, rp0, rk1, rp1, acnt + AC_NREC, 4 * (int)actCap, 32, rhist, st, &lc);
-  k_csr_offsets<<<cnb(n + 1), kCT, 0, st>>>(rk0, 0, cOff, n, acnt + AC_NA);
-  lc++;
+  lc += 2;
+  // the vertex -> record CSR depends only on each contact's kind and slot
+  // vertices: rebuild it only when those changed since the last build (a
+  // sheet at rest keeps the same floor contacts step after step)
+  k_cap_csr_same<<<cnb((long)actCap), kCT, 0, st>>>(v, csrIds, csrMemo, acnt);
+  const cudaGraphConditionalHandle h = g.handle(1);
+  k_cap_csr_decide<<<1, 1, 0, st>>>(csrMemo, acnt, h);
+  lc += 2;
+  g.push(h, cudaGraphCondTypeIf);
+  {
+    cudaStream_t sb = g.cur();
+    k_csr_records<<<cnb(4l * (long)actCap), kCT, 0, sb>>>(v, rk0, rp0, -1);
+    lc++;
+    // 32-bit keys: an even number of passes leaves the result in (rk0, rp0)
+    radix_sort_dev<1>(rk0, rp0, rk1, rp1, acnt + AC_NREC, 4 * (int)actCap, 32, rhist, sb, &lc);
+    k_csr_offsets<<<cnb(n + 1), kCT, 0, sb>>>(rk0, 0, cOff, n, acnt + AC_NA);
+    k_cap_csr_save<<<cnb((long)actCap), kCT, 0, sb>>>(v, csrIds, csrMemo, acnt);
+    lc += 2;
+  }
+  g.pop();
   cap_bind(s);
 }
 

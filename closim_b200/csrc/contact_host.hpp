@@ -91,6 +91,12 @@ class ContactHost {
   double* cg = nullptr;        // 4 per contact
   double* tc = nullptr;        // per-contact chain terms (merit)
   double* tf = nullptr;        // per-contact chain terms (friction work)
+  // Captured steps rebuild the vertex -> record CSR only when the active
+  // list's (kind, slot vertices) changed since the last build: csrIds holds
+  // them (5 ints per contact), csrMemo[0] their count (-1: no valid build,
+  // e.g. after a host-driven build), csrMemo[1] the mismatch flag.
+  int* csrIds = nullptr;
+  int* csrMemo = nullptr;
   Key<1>* rk0 = nullptr; Key<1>* rk1 = nullptr;
   uint32_t* rp0 = nullptr; uint32_t* rp1 = nullptr; uint32_t* rhist = nullptr;
   uint32_t* cOff = nullptr;    // n + 1
