@@ -1054,6 +1054,8 @@ void ContactHost::init(Solver& s, const cs_contact_params* prm, int floor_on, do
   CK(cudaMemset(acnt, 0, AC_N * sizeof(int)));
   dalloc(csrMemo, 2);
   CK(cudaMemset(csrMemo, 0xff, 2 * sizeof(int)));
+  dalloc(supMemo, 4);
+  CK(cudaMemset(supMemo, 0, 4 * sizeof(int)));
   CK(cudaMallocHost(&hint, CI_N * sizeof(int)));
   CK(cudaMallocHost(&hdiag, sizeof(DevDiag)));
   // Capacities sized from the mesh up front: a buffer that grows mid-run costs
@@ -1177,6 +1179,7 @@ void ContactHost::read_ints(Solver& s) {
 void ContactHost::build_superset(Solver& s, const double* x, double padSup) {
   cudaStream_t st = s.stream;
   int64_t& lc = launch_counter();
+  CK(cudaMemsetAsync(supMemo, 0, sizeof(int), st));  // captured steps rebuild their own
   CK(cudaMemcpyAsync(supBase, x, 3 * (size_t)n * 8, cudaMemcpyDeviceToDevice, st));
   bvh_build(bvh, s.d.x0, x, padSup, false, st, &lc);
   topoValid = true;
@@ -1507,6 +1510,7 @@ void ContactHost::update_static_positions(Solver& s, const float* sp, int nsv) {
   for (int i = 0; i < 3 * nsv; i++)
     if (!std::isfinite(sp[i])) throw std::invalid_argument("static positions must be finite");
   CK(cudaMemcpyAsync(spos, sp, 12 * (size_t)ns, cudaMemcpyHostToDevice, s.stream));
+  CK(cudaMemsetAsync(supMemo, 0, sizeof(int), s.stream));  // the static pairs moved
   CK(cudaStreamSynchronize(s.stream));  // sp is the caller's
   supValid = false;
   topoValid = false;
@@ -1574,6 +1578,22 @@ __global__ void k_cap_active_counts(const int* cint, int* acnt, int candCap, int
 // commit's host bookkeeping: the lag table grows by the candidates when there
 // are any, the commit sequence advances when there is any contact.
 __global__ void k_cap_lag_total(int* acnt) { acnt[AC_NTOT] = acnt[AC_LAG] + acnt[AC_NCAND]; }
+// After a captured superset build: its counts and validity for later steps.
+__global__ void k_cap_sup_save(const int* acnt, int* memo) {
+  memo[0] = (acnt[AC_ERR] & ACE_CAPACITY) ? 0 : 1;
+  memo[1] = acnt[AC_NSUP];
+  memo[2] = acnt[AC_NSUPS];
+}
+// Step start of a captured step: rebuild the superset unless the saved one is
+// valid and neither the step start nor the first iterate left its travel.
+__global__ void k_cap_sup_decide(const int* cint, const int* memo, int* acnt, cudaGraphConditionalHandle h) {
+  const bool rebuild = memo[0] != 1 || cint[CI_MOVED] != 0;
+  if (!rebuild) {
+    acnt[AC_NSUP] = memo[1];
+    acnt[AC_NSUPS] = memo[2];
+  }
+  cudaGraphSetConditional(h, rebuild ? 1u : 0u);
+}
 // The vertex of record slot `slot` of a frozen contact (-1: unused), as k_csr_records.
 __device__ __forceinline__ int slot_vertex(const Frozen& f, int slot) {
   if (f.kind == 2) return slot == 0 ? f.p : -1;
@@ -1655,7 +1675,28 @@ void ContactHost::cap_superset(Solver& s, GraphCtx& g, const double* x) {
   if (ms > 0) bvh_append_static(bvh, padSup, supSPairs, (uint32_t)supSCap, (uint32_t*)(cint + CI_STATIC), st, &lc);
   k_cap_sup_counts<<<1, 1, 0, st>>>(cint, acnt, (long)supCap, (long)supSCap, (long)pairCap, (long)spairCap,
                                     (long)flagCap, ms > 0 ? 1 : 0);
-  lc++;
+  k_cap_sup_save<<<1, 1, 0, st>>>(acnt, supMemo);
+  lc += 2;
+}
+
+// A superset swept x0 -> base with the pad widened by kSupTravel contains every
+// pair of a later query swept x0' -> x' when x0' and x' both stay within
+// kSupTravel (max norm) of base, whatever step the query belongs to. So a
+// captured step reuses the previous step's superset when its start x0 and its
+// first iterate x pass that test, and rebuilds it around x otherwise.
+void ContactHost::cap_superset_step(Solver& s, GraphCtx& g, const double* x) {
+  int64_t& lc = launch_counter();
+  cudaStream_t st = g.cur();
+  const int n3 = 3 * n;
+  CK(cudaMemsetAsync(cint, 0, CI_N * sizeof(int), st));
+  k_moved<<<std::min(1184, (n3 + 255) / 256), 256, 0, st>>>(s.d.x0, supBase, n3, kSupTravel, cint);
+  k_moved<<<std::min(1184, (n3 + 255) / 256), 256, 0, st>>>(x, supBase, n3, kSupTravel, cint);
+  const cudaGraphConditionalHandle h = g.handle(1);
+  k_cap_sup_decide<<<1, 1, 0, st>>>(cint, supMemo, acnt, h);
+  lc += 3;
+  g.push(h, cudaGraphCondTypeIf);
+  cap_superset(s, g, x);
+  g.pop();
 }
 
 // launch_query, then (conditional node) the superset rebuilt around x and the
@@ -1830,6 +1871,7 @@ void ContactHost::cap_grow(Solver& s, const int* ha, const int* hc) {
     dalloc(supSPairs, supSCap);
   }
   supValid = false;
+  CK(cudaMemsetAsync(supMemo, 0, sizeof(int), s.stream));
 }
 
 void set_contact(Solver& s, const cs_contact_params* p, int floor_on, double floor_y, const float* sp, int ns,

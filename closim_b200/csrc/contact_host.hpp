@@ -97,6 +97,12 @@ class ContactHost {
   // e.g. after a host-driven build), csrMemo[1] the mismatch flag.
   int* csrIds = nullptr;
   int* csrMemo = nullptr;
+  // Captured steps keep the pair superset across steps while the step start
+  // and the first iterate stay within kSupTravel of its base: supMemo[0] = 1
+  // when supPairs / supSPairs / supBase hold a superset of the current contact
+  // configuration, supMemo[1..2] its pair counts. Host-driven builds, static
+  // mesh moves and buffer growth clear it.
+  int* supMemo = nullptr;
   Key<1>* rk0 = nullptr; Key<1>* rk1 = nullptr;
   uint32_t* rp0 = nullptr; uint32_t* rp1 = nullptr; uint32_t* rhist = nullptr;
   uint32_t* cOff = nullptr;    // n + 1
@@ -168,6 +174,7 @@ class ContactHost {
   void cap_bind(Solver& s);
   void cap_begin_step(Solver& s, GraphCtx& g);
   void cap_superset(Solver& s, GraphCtx& g, const double* x);
+  void cap_superset_step(Solver& s, GraphCtx& g, const double* x);
   void cap_query(Solver& s, GraphCtx& g, const double* x, double pad);
   void cap_update_active_set(Solver& s, GraphCtx& g, const double* x);
   void cap_gradient_terms(Solver& s, GraphCtx& g);

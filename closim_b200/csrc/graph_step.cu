@@ -254,7 +254,7 @@ void Solver::graph_capture(double h) {
   lc += 2 + (d.npins > 0);
   if (contact) {
     contact->cap_begin_step(*this, g);
-    contact->cap_superset(*this, g, d.x);
+    contact->cap_superset_step(*this, g, d.x);
     contact->cap_trial(*this, g, d.x);
     const cudaGraphConditionalHandle hBis = g.handle(0);
     k_g_bis_init<<<1, 1, 0, g.cur()>>>(G.gs, cint, hBis);

@@ -6,7 +6,10 @@ host-driven step's bit for bit: positions, velocities and every counter of
 StepStats and ContactDiagnostics, on every step. Scenes: the strip pull
 (moving pins, no contact), a small floor drape through its landing (barrier,
 friction, restitution, superset rebuilds), the same drape in exact-Newton mode
-(friction potential, Gauss-Newton bending), and the 64 x 64 floor drape.
+(friction potential, Gauss-Newton bending), the 64 x 64 floor drape, and a
+garment under a moving collider (the static mesh moves between steps).
+Captured steps keep the contact CSR and the broadphase pair superset across
+steps when nothing they depend on changed; these comparisons cover both.
 """
 import numpy as np
 import pytest
@@ -74,3 +77,48 @@ def test_graph_equals_host_small_drape_exact_newton():
 def test_graph_equals_host_floor_drape_64x64():
     cfg = configs.floor_drape()
     compare(cfg, 45)
+
+
+def test_graph_equals_host_moving_collider_schwarz():
+    """Irregular garment (annulus) under a rising sphere collider, mixed path
+    with the Schwarz PCG: the collider's static mesh moves before every step,
+    which must invalidate the pair superset the captured steps keep across
+    steps."""
+    from closim_b200.avatar import AvatarCollider, LinearMotion, SphereGeometry, Transform, toCollisionObject
+    from closim_b200.garment import AssembledGarment, AvatarDriver, createFittingScene
+    from tests.test_gpu_garment import annulus
+    h, steps = 0.01, 16
+
+    def run(graph):
+        sphere = AvatarCollider("torso", "torso", SphereGeometry(0.08, 12, 6), 0.004,
+                                motion=LinearMotion(Transform((0.0, -0.1, 0.0)), Transform((0.0, 0.06, 0.0)), 0.0,
+                                                    steps * h))
+        pos, uv, idx = annulus()
+        material = cb.ClothMaterial(arealDensityKgM2=0.2, thickness=1.0, stretchWarp=5e3, stretchWeft=5e3,
+                                    stretchCoupling=0.0, shear=1e3, bendWarp=1e-4, bendWeft=1e-4, damping=0.0)
+        params = cb.ContactParams(dHatM=1e-3, kappaJ=50.0, dMinM=1e-4, frictionMu=0.3, frictionEpsM=1e-4)
+        fs = createFittingScene(AssembledGarment(pos, uv, idx), avatar=toCollisionObject(sphere, 0.0),
+                                material=material, contact=params, arealDensityKgM2=0.2)
+        s = cb.CudaSolver("mixed", newtonIters=10, pcgMaxIters=60, gradTol=1e-5, lineSearchIters=10,
+                          precond="schwarz")
+        s.initialize(fs.scene)
+        s.setGraphMode(graph)
+        driver = AvatarDriver([sphere], s)
+        out, active = [], 0
+        for k in range(steps):
+            driver.advance_to((k + 1) * h)
+            s.step(h)
+            st = s.lastStats
+            out.append((fs.scene.positions.copy(), {k2: getattr(st, k2) for k2 in KEYS}, dict(st.contact)))
+            active = max(active, st.contact["activePairs"])
+        return out, s.graphInfo(), active
+
+    host, _, active = run(False)
+    graph, gi, _ = run(True)
+    assert active > 0, "the collider never reached the garment"
+    assert gi["graphSteps"] > 0, gi
+    for k, (a, b) in enumerate(zip(host, graph)):
+        assert np.array_equal(a[0], b[0]), (k, float(np.max(np.abs(a[0] - b[0]))))
+        assert a[1] == b[1], (k, a[1], b[1])
+        for key in CKEYS:
+            assert a[2][key] == b[2][key], (k, key, a[2][key], b[2][key])
