@@ -238,7 +238,13 @@ PCG_DRAM_BYTES = {"k_mx_pcg_cluster": 3.418e6}
 
 
 CONVERGED = dict(newtonIters=40, pcgMaxIters=3000, gradTol=1e-8)
-EXACT_TOL = 1e-6   # relative PCG tolerance of the exact-Newton solves (FP32 floor 1e-5 on the mixed path)
+# Relative PCG tolerance of the exact-Newton solves, on both paths: the forcing
+# term of an inexact Newton method. Newton still stops only at gradTol 1e-8,
+# so the converged step does not depend on it; on the config-1 drape 3e-4 was
+# the fastest setting with the same Newton iteration count (1e-6: 2.81 ms per
+# step, 1e-4: 2.48, 3e-4: 2.28, 1e-3 (the reference's PCG tolerance, newton.ts:148):
+# 2.40 with 5% more Newton iterations), gate 1e-9.
+EXACT_TOL = 3e-4
 GATE_REL_ERR = 1e-5
 
 
@@ -588,7 +594,7 @@ def main():
             "config": {"workload": cfg["name"] + ("_32x32" if args.small else ""), "n": n, "m": len(cfg["idx"]) // 3,
                        "h": cfg["h"], "headline_path": head, "precond": cfg["options"]["precond"],
                        "budget": args.budget + (" (exact-Newton: 40 Newton, 3000 PCG iterations, gradTol 1e-8, "
-                                                "PCG rel. tol 1e-6 FP64 / 1e-5 FP32)" if args.budget == "converged"
+                                                "PCG rel. tol 3e-4 on both paths)" if args.budget == "converged"
                                                 else " (10 Newton, 60 PCG, PCG tol 1e-3)"),
                        "timed_steps": [args.warmup + args.skip, args.warmup + args.skip + args.steps - 1],
                        "parallelism": f"replicas x{world}", "l2": "flushed between timed steps (256 MiB write)",
