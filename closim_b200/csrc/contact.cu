@@ -1056,6 +1056,8 @@ void ContactHost::init(Solver& s, const cs_contact_params* prm, int floor_on, do
   CK(cudaMemset(csrMemo, 0xff, 2 * sizeof(int)));
   dalloc(supMemo, 4);
   CK(cudaMemset(supMemo, 0, 4 * sizeof(int)));
+  dalloc(actDirty, 1);
+  CK(cudaMemset(actDirty, 0, sizeof(int)));
   CK(cudaMallocHost(&hint, CI_N * sizeof(int)));
   CK(cudaMallocHost(&hdiag, sizeof(DevDiag)));
   // Capacities sized from the mesh up front: a buffer that grows mid-run costs
@@ -1541,12 +1543,21 @@ int ContactHost::read_active(Solver& s, int cap, int32_t* ids6, double* w7) {
 // grown buffers. Kernels and their arithmetic are the same, so a captured step
 // computes what the host-driven one does.
 
-__global__ void k_cap_begin(DevDiag* diag, int* acnt) {
+__global__ void k_cap_begin(DevDiag* diag, int* acnt, int* actDirty) {
   DevDiag z{};
   z.minDistance = INFINITY;
   z.minTOI = INFINITY;
   *diag = z;
   for (int k = 0; k < AC_N; k++) acnt[k] = 0;
+  *actDirty = 1;
+}
+__global__ void k_cap_set_flag(int* f, int v) { *f = v; }
+__global__ void k_cap_act_decide(const int* actDirty, cudaGraphConditionalHandle h) {
+  cudaGraphSetConditional(h, *actDirty ? 1u : 0u);
+}
+__global__ void k_cap_save_query(const int* cint, int* acnt) {
+  acnt[AC_QSELF] = cint[CI_SELF];
+  acnt[AC_QSTATIC] = cint[CI_STATIC];
 }
 // Superset sizes of a traversal into acnt, with the checks build_superset makes.
 __global__ void k_cap_sup_counts(const int* cint, int* acnt, long supCap, long supSCap, long pairCap,
@@ -1653,7 +1664,7 @@ int ContactHost::cand_blocks_cap() const {
 
 void ContactHost::cap_begin_step(Solver& s, GraphCtx& g) {
   cudaStream_t st = g.cur();
-  k_cap_begin<<<1, 1, 0, st>>>(diag, acnt);
+  k_cap_begin<<<1, 1, 0, st>>>(diag, acnt, actDirty);
   CK(cudaMemsetAsync(lagFloorOk, 0, (size_t)n, st));
   launch_counter()++;
   fricOn = false;
@@ -1725,10 +1736,34 @@ void ContactHost::cap_query(Solver& s, GraphCtx& g, const double* x, double pad)
   g.pop();
 }
 
+void ContactHost::cap_mark_moved(GraphCtx& g) {
+  k_cap_set_flag<<<1, 1, 0, g.cur()>>>(actDirty, 1);
+  launch_counter()++;
+}
+
+// The active set at x, as update_active_set. Positions that did not change
+// since the last update (the first Newton iteration after the step start's
+// update, the restitution pass after a converged Newton check) give the same
+// active set, CSR and diagnostics, so the update runs in an IF node on actDirty.
 void ContactHost::cap_update_active_set(Solver& s, GraphCtx& g, const double* x) {
+  int64_t& lc = launch_counter();
+  const cudaGraphConditionalHandle hAct = g.handle(1);
+  k_cap_act_decide<<<1, 1, 0, g.cur()>>>(actDirty, hAct);
+  lc++;
+  g.push(hAct, cudaGraphCondTypeIf);
+  cap_update_active_set_body(s, g, x);
+  k_cap_set_flag<<<1, 1, 0, g.cur()>>>(actDirty, 0);
+  lc++;
+  g.pop();
+  cap_bind(s);
+}
+
+void ContactHost::cap_update_active_set_body(Solver& s, GraphCtx& g, const double* x) {
   cap_query(s, g, x, p.dhat);
   cudaStream_t st = g.cur();
   int64_t& lc = launch_counter();
+  k_cap_save_query<<<1, 1, 0, st>>>(cint, acnt);
+  lc++;
   CView v = cview(*this, s);
   k_active_reset<<<1, 1, 0, st>>>(v);
   k_cand_flags<<<cand_blocks_cap(), kCT, 0, st>>>(v, x, cand.cap, cand.k0, cand.p0);
@@ -1762,7 +1797,6 @@ void ContactHost::cap_update_active_set(Solver& s, GraphCtx& g, const double* x)
     lc += 2;
   }
   g.pop();
-  cap_bind(s);
 }
 
 void ContactHost::cap_gradient_terms(Solver& s, GraphCtx& g) {
@@ -1845,7 +1879,8 @@ void ContactHost::cap_collect(const int* ha, const int* hc, double rejectionsDev
   commitNo = ha[AC_COMMIT];
   nSup = ha[AC_NSUP];
   nSupS = ha[AC_NSUPS];
-  candidatePairs = 15.0 * (uint32_t)hc[CI_SELF] + 12.0 * (uint32_t)(ms > 0 ? hc[CI_STATIC] : 0);
+  candidatePairs = 15.0 * (uint32_t)ha[AC_QSELF] + 12.0 * (uint32_t)(ms > 0 ? ha[AC_QSTATIC] : 0);
+  (void)hc;
   activePairs = nCand + nFloor;
   vtPairs = nVT;
   eePairs = nCand - nVT;

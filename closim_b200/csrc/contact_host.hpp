@@ -38,8 +38,10 @@ constexpr int kBadCap = 4096;
 // frozen set layout, the lag table, the superset sizes and an error word. In a
 // captured step every launch is sized for its buffer's capacity and the kernels
 // read these; the host reads them once, after the step.
+// AC_QSELF / AC_QSTATIC: the pair counts of the last active-set query (the
+// step's candidatePairs diagnostic).
 enum ACnt { AC_NCAND = 0, AC_NFLOOR, AC_NVT, AC_NA, AC_LAG, AC_COMMIT, AC_NSUP, AC_NSUPS, AC_ERR, AC_NREC, AC_NTOT,
-            AC_N = 16 };
+            AC_QSELF, AC_QSTATIC, AC_N = 16 };
 // AC_ERR bits: a buffer capacity was exceeded, or a query fell outside a
 // freshly rebuilt superset; the step is then repeated on the host-driven path.
 enum ACErr { ACE_CAPACITY = 1, ACE_SUPERSET = 2 };
@@ -103,6 +105,10 @@ class ContactHost {
   // configuration, supMemo[1..2] its pair counts. Host-driven builds, static
   // mesh moves and buffer growth clear it.
   int* supMemo = nullptr;
+  // Captured steps: 1 when x changed since the last active-set update (set at
+  // the step start and when a trial is accepted). An update at unchanged
+  // positions would rebuild the same active set, so it is skipped.
+  int* actDirty = nullptr;
   Key<1>* rk0 = nullptr; Key<1>* rk1 = nullptr;
   uint32_t* rp0 = nullptr; uint32_t* rp1 = nullptr; uint32_t* rhist = nullptr;
   uint32_t* cOff = nullptr;    // n + 1
@@ -175,6 +181,8 @@ class ContactHost {
   void cap_begin_step(Solver& s, GraphCtx& g);
   void cap_superset(Solver& s, GraphCtx& g, const double* x);
   void cap_superset_step(Solver& s, GraphCtx& g, const double* x);
+  void cap_mark_moved(GraphCtx& g);
+  void cap_update_active_set_body(Solver& s, GraphCtx& g, const double* x);
   void cap_query(Solver& s, GraphCtx& g, const double* x, double pad);
   void cap_update_active_set(Solver& s, GraphCtx& g, const double* x);
   void cap_gradient_terms(Solver& s, GraphCtx& g);

@@ -324,7 +324,10 @@ void Solver::graph_capture(double h) {
       g.push(hAccept, cudaGraphCondTypeIf);
       {
         GCK(cudaMemcpyAsync(d.x, d.xt, (size_t)n3 * 8, cudaMemcpyDeviceToDevice, g.cur()));
-        if (contact) contact->cap_commit(*this, g, d.x);
+        if (contact) {
+          contact->cap_commit(*this, g, d.x);
+          contact->cap_mark_moved(g);
+        }
       }
       g.pop();
       G.lAccept = lc - a0;
