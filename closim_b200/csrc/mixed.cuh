@@ -37,7 +37,7 @@ struct MixBufs {
 
 // Two-level Schwarz share of lane (member l, component c) of a domain warp:
 // omega Dc^-1 R r prolongated, = sc (omega / Dc[c]) sc sum_l' r[l', c] with
-// sc = 1 / sqrt(|d|) and omega = 0.5 (applyMasTwoLevel, mas.ts:120-139).
+// sc = 1 / sqrt(|d|) and omega = 0.5 (applyMasTwoLevel, mas.ts:110-145).
 __device__ __forceinline__ float coarse_share(const MixBufs& mb, int dom, float rv, int dv) {
   const int lane = threadIdx.x & 31, c = lane % 3;
   float rc = 0.f;

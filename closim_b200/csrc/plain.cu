@@ -418,7 +418,7 @@ __device__ double schwarz_apply_domain(const Dev& d, int dom) {
     }
   }
   // two-level: + P (omega Dc^-1) R r on this domain (applyMasTwoLevel,
-  // mas.ts:120-139, omega = 0.5; the coarse vector of a domain is constant per
+  // mas.ts:110-145, omega = 0.5; the coarse vector of a domain is constant per
   // component over its members, scaled by 1/sqrt(|d|) both ways)
   double cz[3] = {0, 0, 0};
   const double sc = 1 / sqrt((double)dv);

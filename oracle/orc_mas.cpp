@@ -64,7 +64,7 @@ Vec build_coarse_diag(const double* x, const Mesh& mesh, const Material& mat, co
   return dc;
 }
 
-// applyMasTwoLevel (mas.ts:120-139).
+// applyMasTwoLevel (mas.ts:110-145).
 void apply_mas2(const SchwarzFactors& sf, const Vec& dc, double omega, const double* r, double* out, int n) {
   apply_schwarz(sf, r, out, n);
   const SchwarzDomains& dom = *sf.dom;
