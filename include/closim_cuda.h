@@ -228,13 +228,16 @@ int cs_session_restore_stable(cs_solver* s, int32_t* stable_step);
 int cs_forward(cs_solver* s, double dt, int32_t steps, int32_t checkpoint_every);
 int cs_backward(cs_solver* s, const double* dL_dxN, double* dL_dtheta, double* dL_dv0);
 /* Newton linear solve (no counterpart in the reference). mode 0 (default) is
- * the reference's: matrix-free FD membrane HVP, PCG to relative 1e-3. mode 1
- * solves with the full FP64 Hessian (analytic membrane HVP with compressed
- * principal stresses clamped to zero, exact bending HVP, frozen contact) to the
- * relative tolerance tol, keeping the reference's descent safeguard, trust
- * region and Armijo search: the converged step is the same, reached in far
- * fewer iterations, as the adjoint's implicit-function theorem needs.
- * cs_set_stepper_options' PCG budget applies to both. */
+ * the reference's: matrix-free FD membrane HVP, PCG to relative 1e-3, Newton
+ * from the inertial target x0 + h v + h^2 g. mode 1 (exact-Newton) solves with
+ * the full Hessian (analytic membrane HVP with compressed principal stresses
+ * clamped to zero, exact bending HVP (Gauss-Newton on the mixed path), frozen
+ * contact, lagged friction as a frozen potential) to the relative PCG
+ * tolerance tol, takes the analytic hinge gradient, and starts Newton from
+ * x0 + h v; it keeps the reference's descent safeguard, trust region and
+ * Armijo search. The converged step is the same, reached in far fewer
+ * iterations, as the converged comparisons and the adjoint's implicit-function
+ * theorem need. cs_set_stepper_options' budgets apply to both. */
 int cs_set_newton_mode(cs_solver* s, int32_t mode, double tol);
 /* Adjoint PCG budget (default 2000 iterations, relative residual 1e-10). */
 int cs_set_adjoint_options(cs_solver* s, int32_t max_iters, double tol);
