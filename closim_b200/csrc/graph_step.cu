@@ -95,13 +95,14 @@ __global__ void k_g_energy0(GState* g, const double* scal, cudaGraphConditionalH
 }
 
 // Convergence test of a Newton iteration (newton.ts:126-130).
-__global__ void k_g_newton_check(GState* g, const double* scal, double gradTol, int fricExact,
+// meritAgain: the base energy was re-evaluated at x (exact-Newton mode).
+__global__ void k_g_newton_check(GState* g, const double* scal, double gradTol, int meritAgain,
                                  cudaGraphConditionalHandle hSolve, cudaGraphConditionalHandle hNewton) {
   g->used = g->ni + 1;
   const double gn = scal[S_GRADNORM];
   g->gradNorm = gn;
   g->maxStrain = scal[S_MAXSTRAIN];
-  if (fricExact) g->energy = scal[S_ENERGY_TRIAL];
+  if (meritAgain) g->energy = scal[S_ENERGY_TRIAL];
   bool solve = true;
   if (!isfinite(gn)) {
     g->nonfinite = 1;
@@ -235,6 +236,11 @@ void Solver::graph_capture(double h) {
   mb.hrec = exactMode && d.kb > 0 && d.hg > 0 ? ensure_hrec() : nullptr;
   mb.dcoarse = d.precond == 2 ? fdc.p : nullptr;
   const bool fricExact = exactMode && contact && contact->p.mu > 0;
+  // Exact-Newton mode re-evaluates the Armijo base energy at x after each
+  // active-set update (and friction freeze): contacts that enter the set while
+  // Newton moves the sheet would otherwise be missing from the base energy but
+  // present in every trial's, and the line search would reject every step.
+  const bool meritAgain = exactMode && contact;
   const double beta = std::max(std::max(mat.stretch_warp, mat.stretch_weft), mat.shear) * mat.thickness * 0.1 + 1e-6;
   const double damp = 1 - std::min(std::max(mat.damping, 0.0), 0.1);
   const double pcgTol = exactMode ? std::max(newtonTol, kMixedTolFloor) : 1e-3;
@@ -288,12 +294,10 @@ void Solver::graph_capture(double h) {
     launch_grad_terms(d, g.cur(), true);
     lc += 2 + (d.kb > 0 && d.hg > 0);
     mx_grad_final(d, g.cur(), &lc);
-    if (fricExact) {
-      contact->cap_friction_terms(*this, g);
-      energy(d.x);
-    }
+    if (fricExact) contact->cap_friction_terms(*this, g);
+    if (meritAgain) energy(d.x);
     const cudaGraphConditionalHandle hSolve = g.handle(0);
-    k_g_newton_check<<<1, 1, 0, g.cur()>>>(G.gs, scal.p, opts.grad_tol, fricExact ? 1 : 0, hSolve, hNewton);
+    k_g_newton_check<<<1, 1, 0, g.cur()>>>(G.gs, scal.p, opts.grad_tol, meritAgain ? 1 : 0, hSolve, hNewton);
     lc++;
     const int64_t s0 = lc;
     g.push(hSolve, cudaGraphCondTypeIf);

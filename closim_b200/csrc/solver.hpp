@@ -425,10 +425,13 @@ class Solver {
       // Exact-Newton mode: the lagged friction becomes a potential frozen for
       // this iteration (in the merit and the Newton matrix, so the Newton
       // direction is a descent direction of the merit), and the Armijo base
-      // energy is re-evaluated with it at x.
+      // energy is re-evaluated at x with it and with this iteration's active
+      // set (contacts that enter the set while Newton moves the sheet would
+      // otherwise be missing from the base energy but present in every trial's).
       const bool fricExact = newtonMode == 1 && contact && contact->p.mu > 0;
-      if (fricExact) {
-        contact->friction_terms(*this);
+      const bool meritAgain = newtonMode == 1 && contact;
+      if (fricExact) contact->friction_terms(*this);
+      if (meritAgain) {
         contact->merit_energy(*this, d.x);
         energy_of(d.x);
       }
@@ -444,7 +447,7 @@ class Solver {
         read_scalars();
         gradNorm = hscal[S_GRADNORM];
         maxStrain = hscal[S_MAXSTRAIN];
-        if (fricExact) energy = hscal[S_ENERGY_TRIAL];
+        if (meritAgain) energy = hscal[S_ENERGY_TRIAL];
         if (!std::isfinite(gradNorm)) throw NonFinite();
         if (gradNorm < opts.grad_tol) { converged = true; break; }
         gradRead = true;

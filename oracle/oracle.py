@@ -93,6 +93,13 @@ def lib():
         "orc_scene_get_state": (None, [VP, VP, VP]),
         "orc_scene_build_schwarz": (None, [VP, C.c_int, C.c_int, C.c_int]),
         "orc_step": (C.c_int, [VP, C.c_double, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int, F64P]),
+        "orc_step_exact": (C.c_int, [VP, C.c_double, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int,
+                                     C.c_double, C.c_int, F64P]),
+        "orc_hinge_grad_exact": (None, [F64P, F64P, C.c_double, F64P]),
+        "orc_stress_positive_part": (None, [F64P]),
+        "orc_eval_internal_exact": (None, [VP, F64P, F64P, F64P, F64P]),
+        "orc_internal_hvp_exact": (None, [VP, F64P, F64P, F64P, F64P]),
+        "orc_contact_friction_potential": (C.c_double, [VP, F64P, F64P, VP, VP, C.c_int]),
         "orc_lbvh_build": (VP, [F64P, F64P, U32P, C.c_int, C.c_double, C.c_long]),
         "orc_lbvh_destroy": (None, [VP]),
         "orc_lbvh_info": (None, [VP, np.ctypeslib.ndpointer(np.int64, flags="C_CONTIGUOUS")]),
@@ -190,6 +197,21 @@ def hinge_energy(q12, meta3, k):
                                   np.ascontiguousarray(meta3, np.float64), k)
 
 
+def hinge_grad_exact(q12, meta3, k):
+    """Exact gradient of hinge_energy over the 12 coordinates (exact-Newton mode)."""
+    g = np.zeros(12)
+    lib().orc_hinge_grad_exact(np.ascontiguousarray(q12, np.float64), np.ascontiguousarray(meta3, np.float64),
+                               k, g)
+    return g
+
+
+def stress_positive_part(s00, s11, s01):
+    """Positive part of the symmetric stress [[s00, s01], [s01, s11]]."""
+    s = np.array([s00, s11, s01], np.float64)
+    lib().orc_stress_positive_part(s)
+    return tuple(s.tolist())
+
+
 def tri_energy_grad(x0, x1, x2, inv, area, mat):
     out = np.zeros(13)
     lib().orc_tri_energy_grad(np.array([*x0, *x1, *x2], np.float64), np.array(inv, np.float64),
@@ -226,6 +248,23 @@ def eval_membrane(mesh: Mesh, mat, x):
     g = np.zeros(mesh.n * 3)
     e = lib().orc_eval_membrane(mesh.h, mat_array(mat), np.ascontiguousarray(x, np.float64), g)
     return e, g
+
+
+def eval_internal_exact(mesh: Mesh, mat, x):
+    """eval_internal with the exact hinge gradient (exact-Newton mode)."""
+    g = np.zeros(mesh.n * 3)
+    o = np.zeros(2)
+    lib().orc_eval_internal_exact(mesh.h, mat_array(mat), np.ascontiguousarray(x, np.float64), g, o)
+    return o[0], g, o[1]
+
+
+def internal_hvp_exact(mesh: Mesh, mat, x, p):
+    """Exact-Newton mode's internal Newton matrix along p: membrane HVP with the
+    positive part of the stress in its geometric term, plus the bending HVP."""
+    o = np.zeros(mesh.n * 3)
+    lib().orc_internal_hvp_exact(mesh.h, mat_array(mat), np.ascontiguousarray(x, np.float64),
+                                 np.ascontiguousarray(p, np.float64), o)
+    return o
 
 
 def membrane_hvp(mesh: Mesh, mat, x, p):
@@ -339,6 +378,16 @@ class ContactSystem:
 
     def commit(self, x):
         lib().orc_contact_commit(self.h, np.ascontiguousarray(x, np.float64))
+
+    def friction_potential(self, xf, x, v=None):
+        """Exact-Newton mode: the friction potential of the active contacts
+        frozen at xf, evaluated at x; with v, also its Hessian along v."""
+        xf = np.ascontiguousarray(xf, np.float64)
+        x = np.ascontiguousarray(x, np.float64)
+        va = None if v is None else np.ascontiguousarray(v, np.float64)
+        out = None if v is None else np.zeros(len(x))
+        e = lib().orc_contact_friction_potential(self.h, xf, x, _ptr(va), _ptr(out), len(x))
+        return e if v is None else (e, out)
 
     def check_trial(self, x):
         x = np.ascontiguousarray(x, np.float64)
@@ -462,9 +511,16 @@ class Scene:
     def build_schwarz(self, target=8, min_size=1, max_size=8):
         lib().orc_scene_build_schwarz(self.h, target, min_size, max_size)
 
-    def step(self, dt, newton_iters=10, pcg_max_iters=60, grad_tol=1e-5, ls_iters=10, precond="jacobi"):
+    def step(self, dt, newton_iters=10, pcg_max_iters=60, grad_tol=1e-5, ls_iters=10, precond="jacobi",
+             exact=False, pcg_tol=1e-6, drift=True):
+        """implicitStep; exact=True runs the CUDA solver's exact-Newton mode
+        (implicit_step_exact) with PCG tolerance pcg_tol and the drift start."""
         st = np.zeros(20)
-        rc = lib().orc_step(self.h, dt, newton_iters, pcg_max_iters, grad_tol, ls_iters, PRECOND[precond], st)
+        if exact:
+            rc = lib().orc_step_exact(self.h, dt, newton_iters, pcg_max_iters, grad_tol, ls_iters,
+                                      PRECOND[precond], pcg_tol, 1 if drift else 0, st)
+        else:
+            rc = lib().orc_step(self.h, dt, newton_iters, pcg_max_iters, grad_tol, ls_iters, PRECOND[precond], st)
         if rc == 2:
             raise FloatingPointError("non-finite gradient — blow up; reduce dt/stiffness")
         return dict(zip(STAT_KEYS, st.tolist()))

@@ -122,6 +122,16 @@ double add_hinge_gradient(const double* x, double* grad, int v0, int v1, int v2,
 
 struct FemEval { double energy; double maxStrain; };
 FemEval eval_internal(const double* x, const Mesh& mesh, const Material& mat, double* grad);
+
+// Exact-Newton mode pieces (orc_exact.cpp): the hinge gradient differentiated
+// exactly, eval_internal with it, the membrane HVP with the stress of its
+// geometric term replaced by its positive part plus the bending HVP, and the
+// positive part of a symmetric 2x2 stress.
+void hinge_grad_exact(const double* q12, double restAngle, double edgeLen, double areaSum, double k,
+                      double* g12);
+FemEval eval_internal_exact(const double* x, const Mesh& mesh, const Material& mat, double* grad);
+void internal_hvp_exact(const double* x, const double* p, const Mesh& mesh, const Material& mat, double* out);
+void stress_positive_part(double& s00, double& s11, double& s01);
 double internal_energy_only(const double* x, const Mesh& mesh, const Material& mat);
 double eval_membrane(const double* x, const Mesh& mesh, const Material& mat, double* grad);
 void membrane_hvp(const double* x, const double* p, const Mesh& mesh, const Material& mat,
@@ -243,6 +253,11 @@ Key4 contact_key(const Frozen& c);
 
 struct TrialResult { bool valid; double minDist, minTOI; };
 
+// Exact-Newton mode: one contact's friction potential mu lambda sqrt(|P u|^2 +
+// eps^2), frozen at a Newton iterate: ml = mu max(0, lambda), the normal n of
+// P = I - n n^T, and t = P u, r = sqrt(|t|^2 + eps^2) at the freeze point.
+struct FricTerm { double ml = 0, nx = 0, ny = 0, nz = 0, tx = 0, ty = 0, tz = 0, r = 1; };
+
 class ContactSystem {
  public:
   ContactParams params;
@@ -283,6 +298,12 @@ class ContactSystem {
   void relative_slip(const double* x, const Frozen& c, double u[3]) const;
   double dist_jvp(const Frozen& c, const double* v) const;
   double exact_dist(const double* x, const Cand& q) const;
+  // Exact-Newton mode (orc_exact.cpp): freeze the friction potential of every
+  // active contact at x, its value at x, and its Hessian along v.
+  std::vector<FricTerm> fric;
+  void friction_potential_freeze(const double* x);
+  double friction_potential(const double* x) const;
+  void friction_hvp(const double* v, double* out, int n3) const;
  private:
   std::vector<std::pair<int, int>> query_bvh_all(const std::vector<Aabb>& sBoxes) const;
 };
@@ -299,6 +320,7 @@ struct Scene {
 };
 void enforce_pins(const Scene& s, double* x);
 void pin_filter(const Scene& s, double* v);
+void kill_approach_velocity(ContactSystem& contact, Scene& scene, const double* x);
 
 enum Precond { PRECOND_JACOBI = 0, PRECOND_SCHWARZ = 1, PRECOND_BLOCK = 2, PRECOND_MAS2 = 3 };
 struct StepperOptions {
@@ -318,6 +340,12 @@ struct StepStats {
 };
 StepStats implicit_step(Scene& scene, double h, const StepperOptions& opts,
                         const SchwarzDomains* domains);
+// Exact-Newton mode of the CUDA solver (orc_exact.cpp): implicit_step with the
+// exact hinge gradient, the positive-semi-definite Newton matrix, friction as a
+// frozen potential, PCG to tolerance pcgTol, the drift start x0 + h v when
+// drift is set, and a CCD-valid full step taken once gradNorm < 1e-7.
+StepStats implicit_step_exact(Scene& scene, double h, const StepperOptions& opts,
+                              const SchwarzDomains* domains, double pcgTol, bool drift);
 
 // ---- FP32 LBVH mirror (src/backend/webgpu/gpu-broadphase.ts) -----------------
 struct LbvhMirror {

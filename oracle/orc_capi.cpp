@@ -83,6 +83,29 @@ double orc_hinge_energy(const double* x, const int* v4, const double* meta3, dou
   return hinge_energy(x, v4[0], v4[1], v4[2], v4[3], meta3[0], meta3[1], meta3[2], k);
 }
 
+void orc_hinge_grad_exact(const double* q12, const double* meta3, double k, double* g12) {
+  hinge_grad_exact(q12, meta3[0], meta3[1], meta3[2], k, g12);
+}
+void orc_stress_positive_part(double* s3) { stress_positive_part(s3[0], s3[1], s3[2]); }
+void orc_eval_internal_exact(void* mh, const double* mat, const double* x, double* grad, double* out2) {
+  FemEval ev = eval_internal_exact(x, *(Mesh*)mh, mat_of(mat), grad);
+  out2[0] = ev.energy; out2[1] = ev.maxStrain;
+}
+void orc_internal_hvp_exact(void* mh, const double* mat, const double* x, const double* p, double* out) {
+  internal_hvp_exact(x, p, *(Mesh*)mh, mat_of(mat), out);
+}
+// Friction potential of the active contacts frozen at xf: its value at x, its
+// Hessian along v (out, 3n) when v is given.
+double orc_contact_friction_potential(void* c, const double* xf, const double* x, const double* v, double* out,
+                                      int n3) {
+  ContactSystem* cs = (ContactSystem*)c;
+  cs->friction_potential_freeze(xf);
+  if (v) cs->friction_hvp(v, out, n3);
+  const double e = cs->friction_potential(x);
+  cs->fric.clear();
+  return e;
+}
+
 void orc_eval_internal(void* mh, const double* mat, const double* x, double* grad, double* out2) {
   FemEval ev = eval_internal(x, *(Mesh*)mh, mat_of(mat), grad);
   out2[0] = ev.energy; out2[1] = ev.maxStrain;
@@ -294,8 +317,10 @@ void orc_scene_build_schwarz(void* h, int target, int minSize, int maxSize) {
 // Stats out (double[20]): newtonIters, pcgIters, gradNorm, energy, maxStrain,
 // converged, hasContact, contact diag[11] (orc_contact_diag order),
 // newtonItersUsed, armijoTrials. Returns 0, or 2 on the non-finite-gradient throw.
-int orc_step(void* h, double dt, int newtonIters, int pcgMaxIters, double gradTol, int lsIters,
-             int precond, double* stats20) {
+// exact < 0: the reference step; otherwise exact-Newton mode with PCG tolerance
+// pcgTol and the drift start when exact == 1 (implicit_step_exact).
+static int step_any(void* h, double dt, int newtonIters, int pcgMaxIters, double gradTol, int lsIters,
+                    int precond, int exact, double pcgTol, double* stats20) {
   SceneBox* b = (SceneBox*)h;
   StepperOptions o;
   o.newtonIters = newtonIters; o.pcgMaxIters = pcgMaxIters; o.gradTol = gradTol; o.lsIters = lsIters;
@@ -305,7 +330,8 @@ int orc_step(void* h, double dt, int newtonIters, int pcgMaxIters, double gradTo
     b->hasDom = true;
   }
   try {
-    StepStats st = implicit_step(b->s, dt, o, &b->dom);
+    StepStats st = exact < 0 ? implicit_step(b->s, dt, o, &b->dom)
+                             : implicit_step_exact(b->s, dt, o, &b->dom, pcgTol, exact == 1);
     const ContactDiag& d = st.contact;
     double v[20] = {(double)st.newtonIters, (double)st.pcgIters, st.gradNorm, st.energy, st.maxStrain,
                     st.converged ? 1.0 : 0.0, st.hasContact ? 1.0 : 0.0, d.candidatePairs, d.activePairs,
@@ -317,6 +343,14 @@ int orc_step(void* h, double dt, int newtonIters, int pcgMaxIters, double gradTo
   } catch (const std::exception&) {
     return 2;
   }
+}
+int orc_step(void* h, double dt, int newtonIters, int pcgMaxIters, double gradTol, int lsIters,
+             int precond, double* stats20) {
+  return step_any(h, dt, newtonIters, pcgMaxIters, gradTol, lsIters, precond, -1, 0, stats20);
+}
+int orc_step_exact(void* h, double dt, int newtonIters, int pcgMaxIters, double gradTol, int lsIters,
+                   int precond, double pcgTol, int drift, double* stats20) {
+  return step_any(h, dt, newtonIters, pcgMaxIters, gradTol, lsIters, precond, drift ? 1 : 0, pcgTol, stats20);
 }
 
 // ---- FP32 LBVH mirror ----

@@ -24,7 +24,7 @@ void pin_filter(const Scene& s, double* v) {
 
 // src/solver/newton.ts:238-303 killApproachVelocity (restitution 0, one
 // deterministic sweep over the active list; each contact sees earlier updates).
-static void kill_approach_velocity(ContactSystem& contact, Scene& scene, const double* x) {
+void kill_approach_velocity(ContactSystem& contact, Scene& scene, const double* x) {
   const int n3 = (int)scene.positions.size();
   contact.update_active_set(x, n3);
   double* v = scene.velocities.data();

@@ -1,4 +1,4 @@
-"""Exact-Newton mode's first iterate.
+"""Exact-Newton mode: its first iterate, and the oracle's restatement of it.
 
 Exact-Newton mode starts Newton from x0 + h v instead of the reference's
 inertial target yHat = x0 + h v + h^2 g (CLOSIM_DRIFT_GUESS=0 restores it).
@@ -6,6 +6,10 @@ The energy still has yHat as its inertial target, so every converged step is
 the same: on a small drape through landing and rest, both starts converge on
 every step, to positions within 1e-7 of each other, and the drift start needs
 fewer Newton iterations once the sheet rests on the floor.
+
+The oracle restates the mode on the CPU (implicit_step_exact). On the same
+drape, with and without friction, both GPU paths converge on every step to
+the oracle's positions within 1e-7.
 """
 import os
 
@@ -14,16 +18,23 @@ import pytest
 
 import closim_b200 as cb
 from closim_b200 import configs
+from tests.helpers import oracle_scene, oracle_step_kwargs
 
 pytestmark = pytest.mark.gpu
 
 
-def run(drift, precision, steps=40):
+def drape(steps, mu=0.3):
+    cfg = configs.floor_drape(nx=15, ny=15, w=0.2, hgt=0.2, steps=steps, height=0.004)
+    cfg["contact"] = dict(cfg["contact"], frictionMu=mu)
+    cfg["options"] = dict(cfg["options"], newtonIters=40, pcgMaxIters=3000, gradTol=1e-8)
+    return cfg
+
+
+def run(drift, precision, steps=40, mu=0.3):
     old = os.environ.get("CLOSIM_DRIFT_GUESS")
     os.environ["CLOSIM_DRIFT_GUESS"] = "1" if drift else "0"
     try:
-        cfg = configs.floor_drape(nx=15, ny=15, w=0.2, hgt=0.2, steps=steps, height=0.004)
-        cfg["options"] = dict(cfg["options"], newtonIters=40, pcgMaxIters=3000, gradTol=1e-8)
+        cfg = drape(steps, mu)
         sc = configs.make_scene(cfg)
         s = cb.CudaSolver(precision, **cfg["options"])
         s.initialize(sc)
@@ -52,3 +63,30 @@ def test_first_iterate_does_not_change_the_converged_steps(precision):
           f"(last 10 steps {na[-10:].sum()} vs {nb[-10:].sum()})")
     assert err <= 1e-7, err
     assert na[-10:].sum() < nb[-10:].sum()
+
+
+_ORACLE = {}
+
+
+def oracle_run(mu, steps=40):
+    if mu not in _ORACLE:
+        cfg = drape(steps, mu)
+        osc = oracle_scene(cfg)
+        kw = oracle_step_kwargs(cfg)
+        xs, conv = [], 0
+        for _ in range(steps):
+            st = osc.step(cfg["h"], exact=True, pcg_tol=1e-6, drift=True, **kw)
+            xs.append(osc.positions)
+            conv += st["converged"] > 0
+        _ORACLE[mu] = (xs, conv)
+    return _ORACLE[mu]
+
+
+@pytest.mark.parametrize("precision,mu", [("fp64", 0.3), ("mixed", 0.3), ("fp64", 0.0), ("mixed", 0.0)])
+def test_exact_mode_matches_the_oracle_exact_mode(precision, mu):
+    xo, co = oracle_run(mu)
+    xg, _, cg = run(True, precision, mu=mu)
+    assert co == len(xo) and cg == len(xg), (co, cg)
+    err = max(float(np.max(np.abs(a - b)) / np.max(np.abs(b))) for a, b in zip(xg, xo))
+    print(f"{precision}, mu {mu}: GPU exact mode vs oracle exact mode {err:.3e}")
+    assert err <= 1e-7, err
