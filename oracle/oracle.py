@@ -96,6 +96,7 @@ def lib():
         "orc_step_exact": (C.c_int, [VP, C.c_double, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int,
                                      C.c_double, C.c_int, F64P]),
         "orc_hinge_grad_exact": (None, [F64P, F64P, C.c_double, F64P]),
+        "orc_hinge_hess_exact": (None, [F64P, F64P, C.c_double, F64P]),
         "orc_stress_positive_part": (None, [F64P]),
         "orc_eval_internal_exact": (None, [VP, F64P, F64P, F64P, F64P]),
         "orc_internal_hvp_exact": (None, [VP, F64P, F64P, F64P, F64P]),
@@ -203,6 +204,14 @@ def hinge_grad_exact(q12, meta3, k):
     lib().orc_hinge_grad_exact(np.ascontiguousarray(q12, np.float64), np.ascontiguousarray(meta3, np.float64),
                                k, g)
     return g
+
+
+def hinge_hess_exact(q12, meta3, k):
+    """Exact 12x12 Hessian of hinge_energy (hyper-dual numbers)."""
+    h = np.zeros(144)
+    lib().orc_hinge_hess_exact(np.ascontiguousarray(q12, np.float64), np.ascontiguousarray(meta3, np.float64),
+                               k, h)
+    return h.reshape(12, 12)
 
 
 def stress_positive_part(s00, s11, s01):

@@ -124,13 +124,18 @@ struct FemEval { double energy; double maxStrain; };
 FemEval eval_internal(const double* x, const Mesh& mesh, const Material& mat, double* grad);
 
 // Exact-Newton mode pieces (orc_exact.cpp): the hinge gradient differentiated
-// exactly, eval_internal with it, the membrane HVP with the stress of its
-// geometric term replaced by its positive part plus the bending HVP, and the
-// positive part of a symmetric 2x2 stress.
+// exactly and its Hessian, eval_internal with the exact gradient, the hinge Hessians of
+// a mesh (144 per hinge), the membrane HVP with the stress of its geometric
+// term replaced by its positive part plus the bending HVP (from hinH when
+// given), and the positive part of a symmetric 2x2 stress.
 void hinge_grad_exact(const double* q12, double restAngle, double edgeLen, double areaSum, double k,
                       double* g12);
 FemEval eval_internal_exact(const double* x, const Mesh& mesh, const Material& mat, double* grad);
-void internal_hvp_exact(const double* x, const double* p, const Mesh& mesh, const Material& mat, double* out);
+void hinge_hess_exact(const double* q12, double restAngle, double edgeLen, double areaSum, double k,
+                      double* h144);
+void hinge_hessians(const double* x, const Mesh& mesh, const Material& mat, std::vector<double>& out);
+void internal_hvp_exact(const double* x, const double* p, const Mesh& mesh, const Material& mat, double* out,
+                        const double* hinH = nullptr);
 void stress_positive_part(double& s00, double& s11, double& s01);
 double internal_energy_only(const double* x, const Mesh& mesh, const Material& mat);
 double eval_membrane(const double* x, const Mesh& mesh, const Material& mat, double* grad);

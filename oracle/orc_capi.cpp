@@ -86,6 +86,9 @@ double orc_hinge_energy(const double* x, const int* v4, const double* meta3, dou
 void orc_hinge_grad_exact(const double* q12, const double* meta3, double k, double* g12) {
   hinge_grad_exact(q12, meta3[0], meta3[1], meta3[2], k, g12);
 }
+void orc_hinge_hess_exact(const double* q12, const double* meta3, double k, double* h144) {
+  hinge_hess_exact(q12, meta3[0], meta3[1], meta3[2], k, h144);
+}
 void orc_stress_positive_part(double* s3) { stress_positive_part(s3[0], s3[1], s3[2]); }
 void orc_eval_internal_exact(void* mh, const double* mat, const double* x, double* grad, double* out2) {
   FemEval ev = eval_internal_exact(x, *(Mesh*)mh, mat_of(mat), grad);

@@ -2,9 +2,10 @@
 // exact-Newton mode, restated for the CPU so the mode's converged steps can be
 // checked against an independent implementation. The reference has no such
 // mode; each piece is the mathematics of a reference term:
-//   - the hinge gradient of bending.ts:7-16's energy, differentiated exactly
-//     (the reference takes central differences, bending.ts:19-42) through the
-//     signed bend angle, here with dual numbers over atan2;
+//   - the hinge gradient and Hessian of bending.ts:7-16's energy,
+//     differentiated exactly (the reference takes central differences,
+//     bending.ts:19-42) through the signed bend angle, with hyper-dual numbers
+//     over atan2;
 //   - the membrane Hessian of membrane-hvp.ts:18-75 with the stress of its
 //     geometric term replaced by its positive part;
 //   - the lagged Coulomb friction of friction.ts:14-23 as the potential
@@ -22,21 +23,37 @@ namespace orc {
 
 namespace {
 
-struct Dual {
-  double v, d;
+// Hyper-dual number v + a e1 + b e2 + ab e1 e2 (e1^2 = e2^2 = 0). One pass of
+// a function over it gives the value, the derivatives along the two seeds and
+// the mixed second derivative, all exact.
+struct HD {
+  double v, a, b, ab;
 };
-inline Dual operator+(Dual a, Dual b) { return {a.v + b.v, a.d + b.d}; }
-inline Dual operator-(Dual a, Dual b) { return {a.v - b.v, a.d - b.d}; }
-inline Dual operator*(Dual a, Dual b) { return {a.v * b.v, a.d * b.v + a.v * b.d}; }
-inline Dual operator/(Dual a, Dual b) { return {a.v / b.v, (a.d * b.v - a.v * b.d) / (b.v * b.v)}; }
-inline Dual dsqrt(Dual a) {
-  const double s = std::sqrt(a.v);
-  return {s, s > 0 ? a.d / (2 * s) : 0.0};
+inline HD operator+(HD x, HD y) { return {x.v + y.v, x.a + y.a, x.b + y.b, x.ab + y.ab}; }
+inline HD operator-(HD x, HD y) { return {x.v - y.v, x.a - y.a, x.b - y.b, x.ab - y.ab}; }
+inline HD operator*(HD x, HD y) {
+  return {x.v * y.v, x.a * y.v + x.v * y.a, x.b * y.v + x.v * y.b, x.ab * y.v + x.a * y.b + x.b * y.a + x.v * y.ab};
 }
-// d atan2(y, x) = (x dy - y dx) / (x^2 + y^2): stable at every angle
-inline Dual datan2(Dual y, Dual x) {
-  const double r2 = x.v * x.v + y.v * y.v;
-  return {std::atan2(y.v, x.v), r2 > 0 ? (x.v * y.d - y.v * x.d) / r2 : 0.0};
+// f(x) from f, f' and f'' at x.v
+inline HD chain(HD x, double f, double f1, double f2) {
+  return {f, f1 * x.a, f1 * x.b, f1 * x.ab + f2 * x.a * x.b};
+}
+inline HD operator/(HD x, HD y) {
+  const double r = 1 / y.v;
+  return x * chain(y, r, -r * r, 2 * r * r * r);
+}
+inline HD hsqrt(HD x) {
+  const double s = std::sqrt(x.v);
+  return chain(x, s, 0.5 / s, -0.25 / (s * s * s));
+}
+// atan2(y, x): first partials (x, -y) / r^2, second (-2xy, 2xy, y^2 - x^2) / r^4
+// for (yy, xx, xy); defined at every angle.
+inline HD hatan2(HD y, HD x) {
+  const double r2 = x.v * x.v + y.v * y.v, r4 = r2 * r2;
+  const double fy = x.v / r2, fx = -y.v / r2;
+  const double fyy = -2 * x.v * y.v / r4, fxx = 2 * x.v * y.v / r4, fxy = (y.v * y.v - x.v * x.v) / r4;
+  return {std::atan2(y.v, x.v), fy * y.a + fx * x.a, fy * y.b + fx * x.b,
+          fy * y.ab + fx * x.ab + fyy * y.a * y.b + fxx * x.a * x.b + fxy * (x.a * y.b + y.a * x.b)};
 }
 
 // Signed bend angle phi of a hinge (v0, v1 shared; v2, v3 the wings) from its
@@ -44,47 +61,92 @@ inline Dual datan2(Dual y, Dual x) {
 // (the second normal flipped, so a flat hinge has phi = 0),
 // phi = atan2((n1 x m2) . e0 / |e0|, n1 . m2). The reference's dihedral
 // (mesh.ts:129-140), acos of the normals' cosine, equals pi - |phi|.
-Dual bend_phi(const Dual* q) {
-  Dual e0[3], e1[3], e2[3];
+HD bend_phi(const HD* q) {
+  HD e0[3], e1[3], e2[3];
   for (int i = 0; i < 3; i++) {
     e0[i] = q[3 + i] - q[i];
     e1[i] = q[6 + i] - q[i];
     e2[i] = q[9 + i] - q[i];
   }
-  auto cross = [](const Dual* a, const Dual* b, Dual* o) {
+  auto cross = [](const HD* a, const HD* b, HD* o) {
     o[0] = a[1] * b[2] - a[2] * b[1];
     o[1] = a[2] * b[0] - a[0] * b[2];
     o[2] = a[0] * b[1] - a[1] * b[0];
   };
-  Dual n1[3], m2[3], c[3];
+  HD n1[3], m2[3], c[3];
   cross(e0, e1, n1);
   cross(e2, e0, m2);
   cross(n1, m2, c);
-  const Dual el = dsqrt(e0[0] * e0[0] + e0[1] * e0[1] + e0[2] * e0[2]);
-  const Dual s = (c[0] * e0[0] + c[1] * e0[1] + c[2] * e0[2]) / el;
-  const Dual co = n1[0] * m2[0] + n1[1] * m2[1] + n1[2] * m2[2];
-  return datan2(s, co);
+  const HD el = hsqrt(e0[0] * e0[0] + e0[1] * e0[1] + e0[2] * e0[2]);
+  const HD s = (c[0] * e0[0] + c[1] * e0[1] + c[2] * e0[2]) / el;
+  const HD co = n1[0] * m2[0] + n1[1] * m2[1] + n1[2] * m2[2];
+  return hatan2(s, co);
+}
+
+// phi, its gradient, and (when hphi) its 12x12 Hessian at q12.
+double bend_phi_derivs(const double* q12, double* dphi, double* hphi) {
+  HD q[12];
+  for (int j = 0; j < 12; j++) q[j] = {q12[j], 0.0, 0.0, 0.0};
+  double phi = 0;
+  for (int i = 0; i < 12; i++) {
+    q[i].a = 1;
+    if (!hphi) {
+      const HD p = bend_phi(q);
+      phi = p.v;
+      dphi[i] = p.a;
+    } else {
+      for (int j = i; j < 12; j++) {
+        q[j].b = 1;
+        const HD p = bend_phi(q);
+        q[j].b = 0;
+        phi = p.v;
+        if (j == i) dphi[i] = p.a;
+        hphi[i * 12 + j] = hphi[j * 12 + i] = p.ab;
+      }
+    }
+    q[i].a = 0;
+  }
+  return phi;
 }
 
 }  // namespace
 
+// E = k w (theta - rest)^2 / 2 with theta = pi - |phi|, w = edgeLen^2 / areaSum
+// (bending.ts:7-16): grad E = -k w (theta - rest) sgn(phi) grad phi.
 void hinge_grad_exact(const double* q12, double restAngle, double edgeLen, double areaSum, double k,
                       double* g12) {
   const double w = edgeLen * edgeLen / js_max(areaSum, 1e-12);
-  Dual q[12];
-  for (int j = 0; j < 12; j++) q[j] = {q12[j], 0.0};
-  double phi = 0, dphi[12];
-  for (int j = 0; j < 12; j++) {
-    q[j].d = 1;
-    const Dual p = bend_phi(q);
-    q[j].d = 0;
-    phi = p.v;
-    dphi[j] = p.d;
-  }
-  // E = k w (theta - rest)^2 / 2 with theta = pi - |phi|
+  double dphi[12];
+  const double phi = bend_phi_derivs(q12, dphi, nullptr);
   const double theta = M_PI - std::fabs(phi);
   const double c = -k * w * (theta - restAngle) * (phi >= 0 ? 1.0 : -1.0);
   for (int j = 0; j < 12; j++) g12[j] = c * dphi[j];
+}
+
+// Hessian of the same energy: k w (grad phi grad phi^T - (theta - rest) sgn(phi) Hess phi).
+void hinge_hess_exact(const double* q12, double restAngle, double edgeLen, double areaSum, double k,
+                      double* h144) {
+  const double w = edgeLen * edgeLen / js_max(areaSum, 1e-12);
+  double dphi[12], hphi[144];
+  const double phi = bend_phi_derivs(q12, dphi, hphi);
+  const double theta = M_PI - std::fabs(phi);
+  const double c = -(theta - restAngle) * (phi >= 0 ? 1.0 : -1.0);
+  for (int i = 0; i < 12; i++)
+    for (int j = 0; j < 12; j++) h144[i * 12 + j] = k * w * (dphi[i] * dphi[j] + c * hphi[i * 12 + j]);
+}
+
+void hinge_hessians(const double* x, const Mesh& mesh, const Material& mat, std::vector<double>& out) {
+  const double kb = 0.5 * (mat.bendWarp + mat.bendWeft);
+  out.assign(mesh.hinges.size() * 144, 0.0);
+  if (kb <= 0) return;
+  for (size_t hI = 0; hI < mesh.hinges.size(); hI++) {
+    const Hinge& h = mesh.hinges[hI];
+    const int vs[4] = {h.v0, h.v1, h.v2, h.v3};
+    double q[12];
+    for (int a = 0; a < 4; a++)
+      for (int i = 0; i < 3; i++) q[a * 3 + i] = x[vs[a] * 3 + i];
+    hinge_hess_exact(q, h.restAngle, h.edgeLen, h.areaSum, kb, out.data() + hI * 144);
+  }
 }
 
 FemEval eval_internal_exact(const double* x, const Mesh& mesh, const Material& mat, double* grad) {
@@ -171,7 +233,8 @@ static void tri_hvp_psd(const double* x0, const double* x1, const double* x2, co
   }
 }
 
-void internal_hvp_exact(const double* x, const double* p, const Mesh& mesh, const Material& mat, double* out) {
+void internal_hvp_exact(const double* x, const double* p, const Mesh& mesh, const Material& mat, double* out,
+                        const double* hinH) {
   std::fill(out, out + mesh.n * 3, 0.0);
   for (int t = 0; t < mesh.m; t++) {
     const uint32_t vs[3] = {mesh.idx[t * 3], mesh.idx[t * 3 + 1], mesh.idx[t * 3 + 2]};
@@ -183,26 +246,28 @@ void internal_hvp_exact(const double* x, const double* p, const Mesh& mesh, cons
     for (int v = 0; v < 3; v++)
       for (int i = 0; i < 3; i++) out[vs[v] * 3 + i] += o[v * 3 + i];
   }
-  // bending: central difference of the exact hinge gradient along p, per hinge
+  // bending: the exact hinge Hessian along p (precomputed in hinH, 144 per hinge, or here)
   const double kb = 0.5 * (mat.bendWarp + mat.bendWeft);
   if (kb <= 0) return;
-  for (const Hinge& h : mesh.hinges) {
+  double own[144];
+  for (size_t hI = 0; hI < mesh.hinges.size(); hI++) {
+    const Hinge& h = mesh.hinges[hI];
     const int vs[4] = {h.v0, h.v1, h.v2, h.v3};
-    double q[12], pq[12], pn = 0;
+    double pq[12];
     for (int a = 0; a < 4; a++)
-      for (int i = 0; i < 3; i++) {
-        q[a * 3 + i] = x[vs[a] * 3 + i];
-        pq[a * 3 + i] = p[vs[a] * 3 + i];
-        pn = js_max(pn, std::fabs(pq[a * 3 + i]));
-      }
-    if (pn == 0) continue;
-    const double e = 1e-7 / pn;
-    double qp[12], qm[12], gp[12], gm[12];
-    for (int j = 0; j < 12; j++) { qp[j] = q[j] + e * pq[j]; qm[j] = q[j] - e * pq[j]; }
-    hinge_grad_exact(qp, h.restAngle, h.edgeLen, h.areaSum, kb, gp);
-    hinge_grad_exact(qm, h.restAngle, h.edgeLen, h.areaSum, kb, gm);
-    for (int a = 0; a < 4; a++)
-      for (int i = 0; i < 3; i++) out[vs[a] * 3 + i] += (gp[a * 3 + i] - gm[a * 3 + i]) / (2 * e);
+      for (int i = 0; i < 3; i++) pq[a * 3 + i] = p[vs[a] * 3 + i];
+    const double* H = hinH ? hinH + hI * 144 : own;
+    if (!hinH) {
+      double q[12];
+      for (int a = 0; a < 4; a++)
+        for (int i = 0; i < 3; i++) q[a * 3 + i] = x[vs[a] * 3 + i];
+      hinge_hess_exact(q, h.restAngle, h.edgeLen, h.areaSum, kb, own);
+    }
+    for (int r = 0; r < 12; r++) {
+      double sum = 0;
+      for (int c = 0; c < 12; c++) sum += H[r * 12 + c] * pq[c];
+      out[vs[r / 3] * 3 + r % 3] += sum;
+    }
   }
 }
 
@@ -369,6 +434,7 @@ StepStats implicit_step_exact(Scene& scene, double h, const StepperOptions& opts
   Vec cHp(n3), fHp(n3), egrad(n3), cgrad(n3), g(n3), b(n3), Hp(n3), xt(n3);
   SchwarzFactors sf;
   BlockFactors bf;
+  std::vector<double> hinH;
   for (int ni = 0; ni < newtonIters; ni++) {
     itersUsed = ni + 1;
     const FemEval ev = eval_internal_exact(x.data(), mesh, mat, egrad.data());
@@ -389,8 +455,9 @@ StepStats implicit_step_exact(Scene& scene, double h, const StepperOptions& opts
     if (!std::isfinite(gradNorm)) throw std::runtime_error("non-finite gradient");
     if (gradNorm < gradTol) { converged = true; break; }
     for (int i = 0; i < n3; i++) b[i] = -g[i];
+    hinge_hessians(x.data(), mesh, mat, hinH);
     auto hvp = [&](const Vec& p, Vec& out) {
-      internal_hvp_exact(x.data(), p.data(), mesh, mat, Hp.data());
+      internal_hvp_exact(x.data(), p.data(), mesh, mat, Hp.data(), hinH.data());
       for (int i = 0; i < n3; i++) out[i] = M[i / 3] * p[i] * invH2 + Hp[i];
       if (contact) {
         contact->apply_hvp(x.data(), p.data(), cHp.data(), n3);
