@@ -25,6 +25,9 @@
 //   forward(h, dt, steps, checkpointEvery, positions: Float64Array)  // final positions written in place
 //   backward(h, dLdxN: Float64Array, dLdTheta: Float64Array(4), dLdv0: Float64Array)
 //   membraneHvp(h, x: Float64Array, p: Float64Array, out: Float64Array)
+//   setNewtonMode(h, mode: "reference"|"exact", tol: number)
+//   setGraphMode(h, on: boolean)
+//   graphInfo(h) -> {graphSteps, repeats}
 #include <node_api.h>
 
 #include <cstdint>
@@ -399,6 +402,56 @@ bool set_num(napi_env env, napi_value o, const char* k, double val) {
   return ok(env, napi_create_double(env, val, &v), k) && ok(env, napi_set_named_property(env, o, k, v), k);
 }
 
+// Newton mode (no counterpart in the reference): "reference", the default, or
+// "exact" with its relative PCG tolerance (cs_set_newton_mode).
+napi_value SetNewtonMode(napi_env env, napi_callback_info info) {
+  napi_value argv[3];
+  if (!args(env, info, argv, 3)) return nullptr;
+  cs_solver* h;
+  double tol;
+  if (!get_handle(env, argv[0], &h) || !get_double(env, argv[2], &tol)) return nullptr;
+  char mode[16] = {0};
+  size_t len = 0;
+  if (!ok(env, napi_get_value_string_utf8(env, argv[1], mode, sizeof mode, &len), "mode must be a string"))
+    return nullptr;
+  int32_t m;
+  if (std::strcmp(mode, "reference") == 0) m = 0;
+  else if (std::strcmp(mode, "exact") == 0) m = 1;
+  else {
+    napi_throw_range_error(env, nullptr, "mode must be \"reference\" or \"exact\"");
+    return nullptr;
+  }
+  cs_ok(env, h, cs_set_newton_mode(h, m, tol));
+  return nullptr;
+}
+
+// Graph-captured steps on or off (cs_set_graph_mode).
+napi_value SetGraphMode(napi_env env, napi_callback_info info) {
+  napi_value argv[2];
+  if (!args(env, info, argv, 2)) return nullptr;
+  cs_solver* h;
+  bool on = true;
+  if (!get_handle(env, argv[0], &h) || !ok(env, napi_get_value_bool(env, argv[1], &on), "expected a boolean"))
+    return nullptr;
+  cs_ok(env, h, cs_set_graph_mode(h, on ? 1 : 0));
+  return nullptr;
+}
+
+// Steps taken as graph replays and steps repeated host-driven (cs_graph_info).
+napi_value GraphInfo(napi_env env, napi_callback_info info) {
+  napi_value argv[1];
+  if (!args(env, info, argv, 1)) return nullptr;
+  cs_solver* h;
+  if (!get_handle(env, argv[0], &h)) return nullptr;
+  int64_t o[2] = {0, 0};
+  if (!cs_ok(env, h, cs_graph_info(h, o))) return nullptr;
+  napi_value r;
+  if (!ok(env, napi_create_object(env, &r), "graphInfo") || !set_num(env, r, "graphSteps", (double)o[0]) ||
+      !set_num(env, r, "repeats", (double)o[1]))
+    return nullptr;
+  return r;
+}
+
 // StepStats (src/solver/newton.ts:10-18) with ContactDiagnostics
 // (src/collision/types.ts:49-62) under `contact` (null without contact).
 napi_value LastStats(napi_env env, napi_callback_info info) {
@@ -508,6 +561,9 @@ NAPI_MODULE_INIT() {
       {"forward", nullptr, Forward, nullptr, nullptr, nullptr, napi_default, nullptr},
       {"backward", nullptr, Backward, nullptr, nullptr, nullptr, napi_default, nullptr},
       {"membraneHvp", nullptr, MembraneHvp, nullptr, nullptr, nullptr, napi_default, nullptr},
+      {"setNewtonMode", nullptr, SetNewtonMode, nullptr, nullptr, nullptr, napi_default, nullptr},
+      {"setGraphMode", nullptr, SetGraphMode, nullptr, nullptr, nullptr, napi_default, nullptr},
+      {"graphInfo", nullptr, GraphInfo, nullptr, nullptr, nullptr, napi_default, nullptr},
   };
   if (napi_define_properties(env, exports, sizeof fns / sizeof fns[0], fns) != napi_ok) return nullptr;
   return exports;

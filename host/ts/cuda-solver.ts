@@ -63,12 +63,16 @@ interface CudaAddon {
   forward(h: CudaHandle, dt: number, steps: number, checkpointEvery: number, positions: Float64Array): void;
   backward(h: CudaHandle, dLdxN: Float64Array, dLdTheta: Float64Array, dLdv0: Float64Array | null): void;
   membraneHvp(h: CudaHandle, x: Float64Array, p: Float64Array, out: Float64Array): void;
+  setNewtonMode(h: CudaHandle, mode: NewtonMode, tol: number): void;
+  setGraphMode(h: CudaHandle, on: boolean): void;
+  graphInfo(h: CudaHandle): { graphSteps: number; repeats: number };
 }
 
 /** Opaque solver handle owned by the addon. */
 export type CudaHandle = { readonly __brand: "closim_cuda_handle" };
 export type Precision = "fp64" | "mixed";
 export type Preconditioner = "jacobi" | "schwarz" | "mas2";
+export type NewtonMode = "reference" | "exact";
 
 export interface CudaSolverOptions extends StepperOptions {
   /** "fp64": the reference's arithmetic, op for op; "mixed": FP32 linear solve. */
@@ -186,6 +190,27 @@ export class CudaSolver implements ClothSolver {
       lineSearchIters: opts.lineSearchIters ?? DEFAULT_STEPPER.lineSearchIters,
       preconditioner: opts.preconditioner ?? "jacobi",
     });
+  }
+
+  /**
+   * Newton mode (no counterpart in the reference). "reference", the default,
+   * is implicitStep's own linear solve. "exact" solves with the full Hessian to
+   * the relative PCG tolerance `tol`, starts Newton from x0 + h v and treats the
+   * lagged friction as a frozen potential: with a tight gradTol every step
+   * converges, to the same solution in far fewer Newton iterations.
+   */
+  setNewtonMode(mode: NewtonMode, tol = 1e-6): void {
+    cs.setNewtonMode(this.h(), mode, tol);
+  }
+
+  /** Graph-captured steps (on by default) or the host-driven step. */
+  setGraphMode(on: boolean): void {
+    cs.setGraphMode(this.h(), on);
+  }
+
+  /** Steps taken as graph replays, and steps repeated host-driven after a buffer grew. */
+  graphInfo(): { graphSteps: number; repeats: number } {
+    return cs.graphInfo(this.h());
   }
 
   /** membraneHvp(x, p) (src/physics/fem.ts:108-130) on the GPU. */

@@ -235,9 +235,12 @@ int cs_backward(cs_solver* s, const double* dL_dxN, double* dL_dtheta, double* d
  * contact, lagged friction as a frozen potential) to the relative PCG
  * tolerance tol, takes the analytic hinge gradient, and starts Newton from
  * x0 + h v; it keeps the reference's descent safeguard, trust region and
- * Armijo search. The converged step is the same, reached in far fewer
- * iterations, as the converged comparisons and the adjoint's implicit-function
- * theorem need. cs_set_stepper_options' budgets apply to both. */
+ * Armijo search, with the Armijo base energy re-evaluated at every Newton
+ * iterate (its active set and friction potential) and a CCD-valid full step
+ * taken once the gradient norm is below 1e-7, where the energy decrease falls
+ * below the rounding of the energy sum. The converged step is the same,
+ * reached in far fewer iterations, as the converged comparisons and the
+ * adjoint's implicit-function theorem need. cs_set_stepper_options' budgets apply to both. */
 int cs_set_newton_mode(cs_solver* s, int32_t mode, double tol);
 /* Adjoint PCG budget (default 2000 iterations, relative residual 1e-10). */
 int cs_set_adjoint_options(cs_solver* s, int32_t max_iters, double tol);

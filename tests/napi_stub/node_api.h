@@ -22,6 +22,7 @@ napi_status napi_get_value_external(napi_env, napi_value, void**);
 napi_status napi_create_external(napi_env, void*, napi_finalize, void*, napi_value*);
 napi_status napi_get_value_double(napi_env, napi_value, double*);
 napi_status napi_get_value_int32(napi_env, napi_value, int32_t*);
+napi_status napi_get_value_bool(napi_env, napi_value, bool*);
 napi_status napi_get_value_string_utf8(napi_env, napi_value, char*, size_t, size_t*);
 napi_status napi_has_named_property(napi_env, napi_value, const char*, bool*);
 napi_status napi_get_named_property(napi_env, napi_value, const char*, napi_value*);
