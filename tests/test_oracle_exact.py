@@ -12,7 +12,10 @@ the reference quantity it differentiates or replaces:
 - the friction potential against the reference's Coulomb friction force
   (friction.ts:14-23 through contact-assembly.ts:318-341) on floor contacts;
 - the exact step against the reference step where both equations coincide
-  (no bending, no friction): both converge to the same positions.
+  (no bending, no friction): both converge to the same positions;
+- the exact step on frictionless self-contact (VT and EE), where it converges
+  and the reference step does not, and the reason it cannot on cloth-cloth
+  friction: there the reference's friction term is not a potential gradient.
 """
 import math
 
@@ -262,3 +265,80 @@ def test_exact_step_reaches_the_reference_steps_stationary_point():
     assert cb >= len(b) - 2, cb
     err = max(float(np.max(np.abs(x - y)) / np.max(np.abs(y))) for x, y in zip(a, b))
     assert err <= 1e-7, err
+
+
+def _sliding_patches(mu):
+    """Patch B lands on patch A (which rests on a floor) and slides across it:
+    cloth-cloth VT and EE contacts plus floor contacts."""
+    from tests.helpers import offset_mesh, preprocess_merged
+    A = offset_mesh(4, 4, 0.08, 0.08, 0.0, 0.02, 0)
+    B = offset_mesh(4, 4, 0.08, 0.08, 0.03, 0.0215, 0.011)
+    mesh = preprocess_merged([A, B], 0.15)
+    nA = len(A[0]) // 3
+    v = np.zeros(mesh.n * 3)
+    v[0::3] = np.where(np.arange(mesh.n) < nA, 0.1, -0.1)
+    sc = O.Scene(mesh, MAT, v=v)
+    cs = O.ContactSystem(dict(O.DEFAULT_CONTACT, mu=mu), mesh.indices)
+    cs.set_floor(0.0185)
+    sc.set_contact(cs)
+    return sc, cs, mesh
+
+
+def test_exact_step_converges_on_frictionless_self_contact():
+    """VT and EE contacts between two patches: every exact step converges; the
+    reference step at the same budget does not."""
+    conv = {}
+    for exact in (True, False):
+        sc, _, _ = _sliding_patches(0.0)
+        conv[exact] = 0
+        for _ in range(12):
+            st = sc.step(1 / 60, newton_iters=40, pcg_max_iters=2000, grad_tol=1e-8, exact=exact, pcg_tol=1e-6)
+            assert st["vtPairs"] > 0 and st["eePairs"] > 0
+            conv[exact] += st["converged"] > 0
+    assert conv[True] == 12 and conv[False] < 12, conv
+
+
+def test_cloth_cloth_friction_term_is_not_the_potential_gradient():
+    """The reference's lagged friction term (contact-assembly.ts:318-341) on
+    cloth-cloth contacts is not the gradient of the slip potential: it applies
+    an EE contact's force to the second edge with the weights' sign flipped
+    (both edges are pushed the same way), and a VT contact's force reaches the
+    triangle's third vertex, which relativeSlip (contact-assembly.ts:344-367)
+    leaves out. No merit is then consistent with the reference's equations, so
+    exact-Newton mode converges there only without friction (the previous
+    test); floor and one-sided static contacts match (the floor test above)."""
+    rng = np.random.default_rng(23)
+    sc, cs, mesh = _sliding_patches(0.3)
+    x0 = sc.positions
+    cs.begin_step(x0)
+    no_f = O.ContactSystem(dict(O.DEFAULT_CONTACT, mu=0.0), mesh.indices)
+    no_f.set_floor(0.0185)
+    no_f.begin_step(x0)
+    x = x0.copy()
+    x[1::3] -= 0.0003 * (np.arange(mesh.n) >= mesh.n // 2)  # bring B within reach of A
+    x[0::3] += rng.uniform(-2e-4, 2e-4, mesh.n)
+    x[2::3] += rng.uniform(-2e-4, 2e-4, mesh.n)
+    for c in (cs, no_f):
+        c.update_active_set(x)
+    ids, _ = cs.active()
+    kinds = set(ids[:, 0].tolist())
+    assert {0, 1, 2} <= kinds, kinds
+    g_fric = cs.energy_grad(x)[1] - no_f.energy_grad(x)[1]
+    fd = np.zeros(x.size)
+    h = 1e-9
+    for j in range(x.size):
+        xp, xm = x.copy(), x.copy()
+        xp[j] += h
+        xm[j] -= h
+        fd[j] = (cs.friction_potential(x, xp) - cs.friction_potential(x, xm)) / (2 * h)
+    # the floor-only vertices (patch A's vertices in no cloth-cloth contact) agree ...
+    cloth = set()
+    for k, p, a, b, c, d in ids.tolist():
+        if k in (0, 1):
+            cloth.update(q for q in (p, a, b, c, d) if q >= 0)
+    rest = [v for v in range(mesh.n) if v not in cloth]
+    sel = np.array([3 * v + i for v in rest for i in range(3)])
+    assert np.max(np.abs(fd[sel] - g_fric[sel])) <= 1e-6 * np.max(np.abs(g_fric)) + 1e-15
+    # ... the cloth-cloth ones do not
+    csel = np.array([3 * v + i for v in sorted(cloth) for i in range(3)])
+    assert np.max(np.abs(fd[csel] - g_fric[csel])) > 0.1 * np.max(np.abs(g_fric[csel]))
