@@ -240,7 +240,9 @@ int cs_backward(cs_solver* s, const double* dL_dxN, double* dL_dtheta, double* d
  * taken once the gradient norm is below 1e-7, where the energy decrease falls
  * below the rounding of the energy sum. The converged step is the same,
  * reached in far fewer iterations, as the converged comparisons and the
- * adjoint's implicit-function theorem need. cs_set_stepper_options' budgets apply to both. */
+ * adjoint's implicit-function theorem need. The exception is friction between
+ * two cloth sides (VT, EE): the reference's friction term there is not the
+ * gradient of any potential, and the line search can stall as in mode 0. cs_set_stepper_options' budgets apply to both. */
 int cs_set_newton_mode(cs_solver* s, int32_t mode, double tol);
 /* Adjoint PCG budget (default 2000 iterations, relative residual 1e-10). */
 int cs_set_adjoint_options(cs_solver* s, int32_t max_iters, double tol);
