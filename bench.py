@@ -5,7 +5,7 @@ python bench.py --gpus N --steps K --warmup W [--impl cuda|reference]
                 [--skip S]   # untimed steps after the warm-up (default 17: the window spans the landing)
                 [--budget converged|reference]
 
-Default (floor drape, 64 x 64): the mixed-precision path and
+Default (floor drape, 64 x 64, 4,096 vertices): the mixed-precision path and
 the FP64 path run the same steps under a stepper budget where both converge
 (exact-Newton mode: 40 Newton iterations, 3000 PCG iterations, gradTol 1e-8);
 the timed window is steps W+S .. W+S+K (steps 20..119 by default: free fall,
