@@ -1,6 +1,6 @@
 // Oracle (test infrastructure only): a CPU FP64 restatement of the reference
-// CpuSolver hot path of mohdabraralikhan/closim. It is the checker for the
-// CUDA solver and the timed CPU baseline; nothing in the product links it.
+// CpuSolver hot path of mohdabraralikhan/closim. The tests compare the CUDA
+// solver with it, and it is the timed CPU baseline; nothing in the product links it.
 //
 // Every function follows the reference TypeScript line by line, with the same
 // floating-point operation order (compile with -ffp-contract=off so a*b+c is

@@ -1,8 +1,8 @@
 """Pins the oracle (the CPU restatement of the reference CpuSolver) against the
 reference's own known-answer tests, published numbers and invariants.
 
-Each test cites the reference test it restates. The oracle is the checker for
-the CUDA solver, so these run first and on CPU only.
+Each test cites the reference test it restates. The CUDA solver's tests compare
+against the oracle, so these run first and on CPU only.
 """
 import json
 import math
