@@ -14,7 +14,13 @@ would move the positions by less than the converged solve's residual.
 
 Target: relative agreement <= 1e-4 for dL/d(C00, C11, G, k_bend) and for a
 directional derivative along a seeded random initial-velocity direction.
+
+The same gradient is also checked against central differences through the
+oracle's exact-Newton rollout, an implementation independent of the CUDA
+forward (tests/golden/make_adjoint_fd.py writes them as a fixture).
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -97,6 +103,31 @@ def test_adjoint_matches_central_differences():
     rel = abs(ad - fd) / max(abs(fd), 1e-300)
     print(f"dL/dv0 . u: adjoint {ad:.8e}  FD {fd:.8e}  rel {rel:.2e}")
     assert rel <= TOL
+
+
+GOLD_FD = os.path.join(os.path.dirname(__file__), "golden", "adjoint_fd_12.npz")
+
+
+def test_adjoint_matches_central_differences_of_the_oracle():
+    g = np.load(GOLD_FD)
+    cfg = small_fit()
+    assert np.array_equal(cfg["theta0"], g["theta0"])
+    xs, _ = rollout(cfg, cfg["theta_gt"])
+    x0, s = rollout(cfg, cfg["theta0"])
+    n = len(x0) // 3
+    # the forward rollouts themselves match the oracle's
+    fwd = max(float(np.max(np.abs(xs - g["xs"])) / np.max(np.abs(g["xs"]))),
+              float(np.max(np.abs(x0 - g["x0"])) / np.max(np.abs(g["x0"]))))
+    dth, dv0 = s.backward(2 * (x0 - xs) / n)
+    adj = np.array([dth["C00"], dth["C11"], dth["G"], dth["kBend"]])
+    rel = np.abs(adj - g["dL_dtheta"]) / np.abs(g["dL_dtheta"])
+    u = np.random.default_rng(7).standard_normal(3 * n) * 1e-3
+    for pid in cfg["fixed_pins"]:
+        u[pid * 3:pid * 3 + 3] = 0
+    rel_u = abs(float(dv0 @ u) - float(g["dL_dv0_u"])) / abs(float(g["dL_dv0_u"]))
+    print(f"adjoint vs oracle FD: forward {fwd:.2e}; dL/dtheta rel {rel}; dL/dv0.u rel {rel_u:.2e}")
+    assert fwd <= 1e-9, fwd
+    assert float(np.max(rel)) <= TOL and rel_u <= TOL, (rel, rel_u)
 
 
 def test_autograd_function_semantics():
