@@ -38,4 +38,10 @@ void hc_bend_hvp(const double* q, const double* v, const double* meta, double k,
 void hc_membrane_block9(const double* x9, const double* inv4, double s, const double* C4, double* h) {
   cs::membrane_block9<double>(x9, x9 + 3, x9 + 6, inv4[0], inv4[1], inv4[2], inv4[3], s, C4[0], C4[1], C4[2], C4[3], h);
 }
+// Exact-Newton mode: the block with the stress's positive part, and the clamp itself.
+void hc_membrane_block9_psd(const double* x9, const double* inv4, double s, const double* C4, double* h) {
+  cs::membrane_block9<double>(x9, x9 + 3, x9 + 6, inv4[0], inv4[1], inv4[2], inv4[3], s, C4[0], C4[1], C4[2], C4[3], h,
+                              true);
+}
+void hc_psd_stress(double* s3) { cs::psd_stress(s3[0], s3[1], s3[2]); }
 }

@@ -1,6 +1,9 @@
 """The device contact primitives (closim_b200/csrc/contact_math.cuh and
 jsmath.cuh), compiled for the host, agree bit for bit with the oracle on
-random and edge-case inputs. Catches porting slips without a GPU."""
+random and edge-case inputs. Catches porting slips without a GPU. The device
+math of exact-Newton mode (adjoint_math.cuh: hinge gradient and HVP, clamped
+stress, clamped membrane block) agrees with the oracle's exact-mode pieces to
+rounding."""
 import ctypes as C
 import math
 import os
@@ -243,3 +246,76 @@ def test_membrane_block9_matches_oracle(hc):
                               np.array([mat["C00"], mat["C11"], mat["C01"], mat["G"]]), h)
         worst = max(worst, np.max(np.abs(h.reshape(9, 9) - ref)) / np.max(np.abs(ref)))
     assert worst < 1e-12, worst
+
+
+def test_exact_mode_bending_matches_the_oracle(hc):
+    """Exact-Newton mode's hinge gradient and full bending HVP (the FP64
+    path's) against the oracle's exact hinge gradient and Hessian, written
+    independently (hyper-dual numbers): agreement to rounding, near flat and
+    folded up to 2.8 rad, flat and curved rest angles."""
+    p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+    hc.hc_bend_grad.restype = C.c_double
+    hc.hc_bend_grad.argtypes = [p, p, C.c_double, p]
+    hc.hc_bend_hvp.restype = None
+    hc.hc_bend_hvp.argtypes = [p, p, p, C.c_double, p]
+    rng = np.random.default_rng(19)
+    k = 2e-4
+    worst_g = worst_h = 0.0
+    for trial, ang in enumerate([1e-6, 1e-3, 0.05, 0.3, 1.0, 2.0, 2.8] * 6):
+        q = np.array([0, 0, 0, 1, 0, 0, 0.4, 0, 1, 0.6, np.sin(ang), -np.cos(ang)], np.float64)
+        q = q * 0.02 + rng.uniform(-1e-4, 1e-4, 12) * (trial % 2)
+        meta = np.array([np.pi if trial % 3 else 2.6, 0.02, 3e-4])
+        g = np.zeros(12)
+        hc.hc_bend_grad(q, meta, k, g)
+        go = O.hinge_grad_exact(q, meta, k)
+        worst_g = max(worst_g, np.max(np.abs(g - go)) / max(np.max(np.abs(go)), 1e-300))
+        v = rng.uniform(-1, 1, 12)
+        hv = np.zeros(12)
+        hc.hc_bend_hvp(q, v, meta, k, hv)
+        ho = O.hinge_hess_exact(q, meta, k) @ v
+        worst_h = max(worst_h, np.max(np.abs(hv - ho)) / max(np.max(np.abs(ho)), 1e-300))
+    assert worst_g < 1e-9, worst_g
+    assert worst_h < 1e-8, worst_h
+
+
+def test_exact_mode_psd_stress_matches_the_oracle(hc):
+    p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+    hc.hc_psd_stress.restype = None
+    hc.hc_psd_stress.argtypes = [p]
+    rng = np.random.default_rng(29)
+    cases = [rng.normal(size=3) * rng.uniform(1, 1e4) for _ in range(500)]
+    cases += [np.array(c, float) for c in ([3, -2, 0], [-3, 2, 0], [-1, -1, 0], [2, 2, 0], [0, 0, 0], [1, -1, 1e-20])]
+    for c in cases:
+        s = c.copy()
+        hc.hc_psd_stress(s)
+        ref = np.array(O.stress_positive_part(*c))
+        assert np.max(np.abs(s - ref)) <= 1e-13 * max(np.max(np.abs(c)), 1e-300), (c, s, ref)
+
+
+def test_exact_mode_membrane_block_matches_the_oracle(hc):
+    """The Schwarz / FP64 exact-mode membrane block with the clamped stress
+    (membrane_block9, psd) against the oracle's exact-mode membrane HVP on
+    single compressed, sheared and stretched triangles."""
+    p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+    hc.hc_membrane_block9_psd.restype = None
+    hc.hc_membrane_block9_psd.argtypes = [p, p, C.c_double, p, p]
+    rng = np.random.default_rng(31)
+    mat = dict(O.DEFAULT_MATERIAL, C00=5e3, C11=3e3, C01=400.0, G=1e3, bendWarp=0.0, bendWeft=0.0)
+    pos = np.array([0, 0, 0, 0.01, 0, 0, 0.002, 0, 0.012], np.float32)
+    mesh = O.Mesh(pos, np.array([0, 0, 1, 0, 0, 1], np.float32), np.array([0, 1, 2], np.uint32), 0.2)
+    inv = mesh.invDm.astype(np.float64)
+    s = mat["thickness"] * float(mesh.areas[0])
+    C4 = np.array([mat["C00"], mat["C11"], mat["C01"], mat["G"]])
+    worst = 0.0
+    for trial in range(60):
+        A = np.eye(3) + rng.uniform(-0.08, 0.08, (3, 3))
+        A[0, 0] *= (0.9, 1.0, 1.05)[trial % 3]
+        x = (pos.astype(np.float64).reshape(3, 3) @ A.T + rng.uniform(-1, 1, 3)).ravel()
+        H = np.zeros(81)
+        hc.hc_membrane_block9_psd(x, inv, s, C4, H)
+        v = rng.uniform(-1, 1, 9)
+        ho = O.internal_hvp_exact(mesh, mat, x, v)
+        hv = H.reshape(9, 9) @ v
+        worst = max(worst, np.max(np.abs(hv - ho)) / np.max(np.abs(ho)))
+        assert np.min(np.linalg.eigvalsh(H.reshape(9, 9))) >= -1e-9 * np.max(np.abs(H))
+    assert worst < 1e-10, worst
