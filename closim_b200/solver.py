@@ -428,8 +428,14 @@ class CudaSolver:
         return dict(C00=th[0], C11=th[1], G=th[2], kBend=th[3]), dv
 
     def setNewtonMode(self, mode: str = "reference", tol: float = 1e-8) -> None:
-        """'reference': the reference's inexact Newton; 'exact': full FP64
-        Hessian solved to `tol` (converges tightly; for differentiable rollouts)."""
+        """'reference': the reference's inexact Newton. 'exact': the full
+        Hessian (FP64 path; FP32 with Gauss-Newton bending on the mixed path)
+        solved to the relative PCG tolerance `tol`, Newton started from
+        x0 + h v, lagged friction as a frozen potential in the merit, the Armijo
+        base energy re-evaluated at every iterate: with a tight gradTol every
+        step converges (except under cloth-cloth friction, whose reference
+        force is no potential gradient), to the same solution in far fewer
+        Newton iterations. The benchmark and the differentiable rollouts use it."""
         self._check(self._lib.cs_set_newton_mode(self._h, {"reference": 0, "exact": 1}[mode], tol))
 
     def setAdjointOptions(self, maxIters: int = 2000, tol: float = 1e-10) -> None:
