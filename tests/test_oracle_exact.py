@@ -15,7 +15,9 @@ the reference quantity it differentiates or replaces:
   (no bending, no friction): both converge to the same positions;
 - the exact step on frictionless self-contact (VT and EE), where it converges
   and the reference step does not, and the reason it cannot on cloth-cloth
-  friction: there the reference's friction term is not a potential gradient.
+  friction: there the reference's friction term is not a potential gradient;
+- the exact step under friction on one-sided static contacts, where every
+  step converges.
 """
 import math
 
@@ -342,3 +344,28 @@ def test_cloth_cloth_friction_term_is_not_the_potential_gradient():
     # ... the cloth-cloth ones do not
     csel = np.array([3 * v + i for v in sorted(cloth) for i in range(3)])
     assert np.max(np.abs(fd[csel] - g_fric[csel])) > 0.1 * np.max(np.abs(g_fric[csel]))
+
+
+def test_exact_step_converges_on_static_collider_friction():
+    """tests/static-collider.test.ts:34-70's plate drape (mu 0.3): on one-sided
+    static contacts (cloth vertex against static triangle, cloth edge against
+    static edge) the friction potential's gradient is the reference's friction
+    term, and every exact step converges; the reference step at the same
+    budget mostly does not."""
+    from tests.helpers import offset_mesh, preprocess_merged
+    conv = {}
+    for exact in (True, False):
+        g = offset_mesh(4, 4, 0.08, 0.08, 0.01, 0.08, 0.01)
+        mesh = preprocess_merged([g], 0.15)
+        sc = O.Scene(mesh, MAT)
+        spos = np.array([-0.05, 0.03, -0.05, 0.15, 0.03, -0.05, 0.15, 0.03, 0.15, -0.05, 0.03, 0.15], np.float32)
+        cs = O.ContactSystem({"mu": 0.3}, mesh.indices)
+        cs.set_static_mesh(spos, np.array([0, 1, 2, 0, 2, 3], np.uint32))
+        sc.set_contact(cs)
+        conv[exact], vt, ee = 0, 0, 0
+        for _ in range(30):
+            st = sc.step(1 / 60, newton_iters=40, pcg_max_iters=2000, grad_tol=1e-8, exact=exact, pcg_tol=1e-6)
+            conv[exact] += st["converged"] > 0
+            vt, ee = max(vt, st["vtPairs"]), max(ee, st["eePairs"])
+        assert vt > 0 and ee > 0
+    assert conv[True] == 30 and conv[False] < 15, conv
