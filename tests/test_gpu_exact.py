@@ -12,7 +12,9 @@ drape, with and without friction, both GPU paths converge on every step to
 the oracle's positions within 1e-7. At the benchmark's scale and budget (the
 64x64 drape, 120 steps, PCG tolerance 3e-4) the oracle's trajectory is a
 committed fixture (tests/golden/make_exact_drape.py), and both GPU paths match
-it within 1e-7 after the landing and at step 120.
+it within 1e-7 after the landing and at step 120. With friction on one-sided
+static contacts (the reference's static-plate drape) both GPU paths converge
+on every step, as the oracle does, to its positions within 1e-7.
 """
 import os
 
@@ -122,3 +124,51 @@ def test_exact_mode_matches_the_oracle_on_the_64x64_drape(precision):
           f"Newton {newton} (oracle {int(g['newton'].sum())})")
     assert conv == steps, conv
     assert max(errs.values()) <= 1e-7, errs
+
+
+def static_plate(steps):
+    """tests/static-collider.test.ts:34-70's plate drape (mu 0.3): a 5x5 patch
+    falls onto a static two-triangle plate; VT and EE contacts against the
+    static mesh, with friction."""
+    from tests.helpers import merge_parts, offset_mesh
+    pos, uv, idx = merge_parts([offset_mesh(4, 4, 0.08, 0.08, 0.01, 0.08, 0.01)])
+    n = len(pos) // 3
+    spos = np.array([-0.05, 0.03, -0.05, 0.15, 0.03, -0.05, 0.15, 0.03, 0.15, -0.05, 0.03, 0.15], np.float32)
+    sidx = np.array([0, 1, 2, 0, 2, 3], np.uint32)
+    mat = dict(arealDensityKgM2=0.15, thickness=0.001, stretchWarp=20000.0, stretchWeft=20000.0, stretchCoupling=0.0,
+               shear=5000.0, bendWarp=1e-5, bendWeft=1e-5, damping=0.001)
+    return dict(name="static_plate", pos=pos, uv=uv, idx=idx, density=0.15, material=mat, x=pos.astype(np.float64),
+                v=np.zeros(n * 3), gravity=(0.0, -9.81, 0.0), h=1 / 60, steps=steps,
+                options=dict(newtonIters=40, pcgMaxIters=2000, gradTol=1e-8, lineSearchIters=10, precond="jacobi"),
+                fixed_pins=[], moving_pins=[], pin_velocity=(0.0, 0.0, 0.0),
+                contact=dict(dHatM=0.002, kappaJ=50.0, dMinM=1e-4, frictionMu=0.3, frictionEpsM=1e-4, floorY=None,
+                             staticPos=spos, staticIdx=sidx), seed=0)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_exact_mode_static_collider_friction_matches_the_oracle(precision):
+    """Friction on one-sided static contacts is a potential gradient, so every
+    exact step converges, on the GPU as in the oracle's exact mode, to the
+    same positions."""
+    steps = 30
+    cfg = static_plate(steps)
+    osc = oracle_scene(cfg)
+    kw = oracle_step_kwargs(cfg)
+    sc = configs.make_scene(cfg)
+    s = cb.CudaSolver(precision, **cfg["options"])
+    s.initialize(sc)
+    s.setNewtonMode("exact", 1e-6)
+    worst, co, cg, vt, ee = 0.0, 0, 0, 0, 0
+    for _ in range(steps):
+        st = osc.step(cfg["h"], exact=True, pcg_tol=1e-6, drift=True, **kw)
+        s.step(cfg["h"])
+        co += st["converged"] > 0
+        cg += bool(s.lastStats.converged)
+        vt, ee = max(vt, st["vtPairs"]), max(ee, st["eePairs"])
+        xo = osc.positions
+        worst = max(worst, float(np.max(np.abs(sc.positions - xo)) / np.max(np.abs(xo))))
+    print(f"{precision}: static plate, exact mode vs oracle {worst:.3e}; converged GPU {cg}/{steps}, "
+          f"oracle {co}/{steps}; VT {vt}, EE {ee}")
+    assert vt > 0 and ee > 0
+    assert co == steps and cg == steps, (co, cg)
+    assert worst <= 1e-7, worst
