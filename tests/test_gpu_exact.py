@@ -14,7 +14,8 @@ the oracle's positions within 1e-7. At the benchmark's scale and budget (the
 committed fixture (tests/golden/make_exact_drape.py), and both GPU paths match
 it within 1e-7 after the landing and at step 120. With friction on one-sided
 static contacts (the reference's static-plate drape) both GPU paths converge
-on every step, as the oracle does, to its positions within 1e-7.
+on every step, as the oracle does, to its positions within 1e-7; so they do
+on frictionless cloth-cloth self-contact (two sliding patches).
 """
 import os
 
@@ -168,6 +169,49 @@ def test_exact_mode_static_collider_friction_matches_the_oracle(precision):
         xo = osc.positions
         worst = max(worst, float(np.max(np.abs(sc.positions - xo)) / np.max(np.abs(xo))))
     print(f"{precision}: static plate, exact mode vs oracle {worst:.3e}; converged GPU {cg}/{steps}, "
+          f"oracle {co}/{steps}; VT {vt}, EE {ee}")
+    assert vt > 0 and ee > 0
+    assert co == steps and cg == steps, (co, cg)
+    assert worst <= 1e-7, worst
+
+
+def sliding_patches(steps):
+    """Patch B lands on patch A, which rests on a floor, and slides across it:
+    cloth-cloth VT and EE contacts plus floor contacts, without friction (the
+    reference's cloth-cloth friction term is no potential gradient)."""
+    from tests.helpers import merge_parts, offset_mesh
+    A = offset_mesh(4, 4, 0.08, 0.08, 0.0, 0.02, 0)
+    B = offset_mesh(4, 4, 0.08, 0.08, 0.03, 0.0215, 0.011)
+    pos, uv, idx = merge_parts([A, B])
+    n, nA = len(pos) // 3, len(A[0]) // 3
+    v = np.zeros(n * 3)
+    v[0::3] = np.where(np.arange(n) < nA, 0.1, -0.1)
+    cfg = static_plate(steps)
+    cfg.update(name="sliding_patches", pos=pos, uv=uv, idx=idx, x=pos.astype(np.float64), v=v)
+    cfg["contact"] = dict(dHatM=0.002, kappaJ=50.0, dMinM=1e-4, frictionMu=0.0, frictionEpsM=1e-4, floorY=0.0185)
+    return cfg
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_exact_mode_frictionless_self_contact_matches_the_oracle(precision):
+    steps = 12
+    cfg = sliding_patches(steps)
+    osc = oracle_scene(cfg)
+    kw = oracle_step_kwargs(cfg)
+    sc = configs.make_scene(cfg)
+    s = cb.CudaSolver(precision, **cfg["options"])
+    s.initialize(sc)
+    s.setNewtonMode("exact", 1e-6)
+    worst, co, cg, vt, ee = 0.0, 0, 0, 0, 0
+    for _ in range(steps):
+        st = osc.step(cfg["h"], exact=True, pcg_tol=1e-6, drift=True, **kw)
+        s.step(cfg["h"])
+        co += st["converged"] > 0
+        cg += bool(s.lastStats.converged)
+        vt, ee = max(vt, st["vtPairs"]), max(ee, st["eePairs"])
+        xo = osc.positions
+        worst = max(worst, float(np.max(np.abs(sc.positions - xo)) / np.max(np.abs(xo))))
+    print(f"{precision}: sliding patches, exact mode vs oracle {worst:.3e}; converged GPU {cg}/{steps}, "
           f"oracle {co}/{steps}; VT {vt}, EE {ee}")
     assert vt > 0 and ee > 0
     assert co == steps and cg == steps, (co, cg)
