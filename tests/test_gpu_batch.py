@@ -9,6 +9,7 @@
 - A graph-replayed multi-step call equals the same steps issued one by one.
 - Floor contact: sheets dropped onto the floor stay above dMin.
 - The autotuner returns a candidate block size and leaves the state unchanged.
+- At a converging budget each sheet matches the oracle's exact-Newton mode.
 """
 import numpy as np
 import pytest
@@ -99,3 +100,35 @@ def test_autotune_keeps_state():
     assert np.array_equal(bs.allPositions(), x0)
     bs.step(0.01)
     assert np.all(np.isfinite(bs.allPositions()))
+
+
+def test_batch_matches_the_oracle_exact_mode_when_converged():
+    """Each sheet of the batch at a converging budget (gradTol 1e-8) against the
+    oracle's exact-Newton mode, an independent CPU implementation of the same
+    equations (both take the exact hinge gradient): the oracle converges every
+    step and the batch all but at most one per sheet (its Armijo search, the
+    reference's, has no near-convergence rule, so a step can stop just short of
+    the tolerance), and the positions agree."""
+    from tests.helpers import oracle_scene, oracle_step_kwargs
+    sheets = [soft_strip(nx, ny, seed) for nx, ny, seed in [(24, 12, 2), (31, 5, 4)]]
+    budget = dict(newtonIters=40, pcgMaxIters=400, gradTol=1e-8)
+    steps = 20
+    h = sheets[0]["h"]
+    bs = BatchSolver(sheets, options=budget)
+    conv = np.zeros(len(sheets))
+    for _ in range(steps):
+        bs.step(h)
+        conv += [st["converged"] == 1 for st in bs.stats()]
+    for i, cfg in enumerate(sheets):
+        osc = oracle_scene(cfg)
+        kw = dict(oracle_step_kwargs(cfg), newton_iters=40, pcg_max_iters=3000, grad_tol=1e-8)
+        co = 0
+        for k in range(steps):
+            osc.set_pins(configs.pins_at(cfg, k))
+            co += osc.step(h, exact=True, pcg_tol=1e-6, drift=True, **kw)["converged"] > 0
+        xo = osc.positions
+        err = float(np.max(np.abs(bs.positions(i) - xo)) / np.max(np.abs(xo)))
+        print(f"sheet {i}: batch vs oracle exact mode {err:.3e}; converged batch {int(conv[i])}/{steps}, "
+              f"oracle {co}/{steps}")
+        assert co == steps and conv[i] >= steps - 1, (conv[i], co)
+        assert err <= 1e-7, err
