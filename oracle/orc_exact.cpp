@@ -11,7 +11,9 @@
 //   - the lagged Coulomb friction of friction.ts:14-23 as the potential
 //     D = mu lambda sqrt(|P u|^2 + eps^2) of the relative slip u
 //     (contact-assembly.ts:344-367), with lambda and the normal n frozen at the
-//     Newton iterate; its gradient is the reference's friction force.
+//     Newton iterate; its gradient is the reference's friction force on floor
+//     and one-sided static contacts (on cloth-cloth contacts the reference's
+//     force is the gradient of no potential).
 #include <cmath>
 #include <functional>
 #include <stdexcept>
